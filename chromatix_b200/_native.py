@@ -1,0 +1,236 @@
+"""ctypes binding of the sm_100a shared library (``include/cx_b200.h``).
+
+The library is the only compute path: if it is missing or cannot be loaded
+every operation raises -- there is no CPU or eager fallback.  torch is used
+for device memory, streams and host<->device copies only.
+"""
+
+from __future__ import annotations
+
+import ctypes
+import os
+import threading
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "_lib", "libcx_b200.so")
+
+c_double = ctypes.c_double
+c_int32 = ctypes.c_int32
+c_void_p = ctypes.c_void_p
+c_size_t = ctypes.c_size_t
+
+CX_OK = 0
+CX_PREC_ACCURATE = 0
+CX_PREC_REF32 = 1
+CX_KERNEL_TRANSFER = 0
+CX_KERNEL_ASM = 1
+CX_KERNEL_EXPLICIT = 2
+
+_STATUS = {
+    0: "CX_OK",
+    1: "CX_ERR_INVALID",
+    2: "CX_ERR_UNSUPPORTED",
+    3: "CX_ERR_CUDA",
+    4: "CX_ERR_WORKSPACE",
+    5: "CX_ERR_NOT_CONVERGED",
+}
+
+
+class CxError(RuntimeError):
+    """A non-zero ``cx_status`` from the native library."""
+
+    def __init__(self, status: int, msg: str):
+        super().__init__(f"{_STATUS.get(status, status)}: {msg}")
+        self.status = status
+
+
+class cx_plane(ctypes.Structure):
+    _fields_ = [
+        ("z", c_double),
+        ("wavelength", c_double),
+        ("dy", c_double),
+        ("dx", c_double),
+        ("shift_y", c_double),
+        ("shift_x", c_double),
+        ("bl_y0", c_double),
+        ("bl_x0", c_double),
+        ("bl_hy", c_double),
+        ("bl_hx", c_double),
+        ("in_plane", c_int32),
+        ("h_plane", c_int32),
+    ]
+
+
+PLANE_DTYPE = np.dtype(
+    [
+        ("z", "<f8"),
+        ("wavelength", "<f8"),
+        ("dy", "<f8"),
+        ("dx", "<f8"),
+        ("shift_y", "<f8"),
+        ("shift_x", "<f8"),
+        ("bl_y0", "<f8"),
+        ("bl_x0", "<f8"),
+        ("bl_hy", "<f8"),
+        ("bl_hx", "<f8"),
+        ("in_plane", "<i4"),
+        ("h_plane", "<i4"),
+    ]
+)
+assert PLANE_DTYPE.itemsize == ctypes.sizeof(cx_plane)
+
+
+class cx_prop2d_desc(ctypes.Structure):
+    _fields_ = [
+        ("ny", c_int32),
+        ("nx", c_int32),
+        ("pad_y", c_int32),
+        ("pad_x", c_int32),
+        ("n_wv", c_int32),
+        ("n_in_planes", c_int32),
+        ("n_out_planes", c_int32),
+        ("mode_same", c_int32),
+        ("kernel", c_int32),
+        ("precision", c_int32),
+        ("remove_evanescent", c_int32),
+        ("bandlimit", c_int32),
+        ("n_medium", c_double),
+        ("ky0", c_double),
+        ("kx0", c_double),
+    ]
+
+
+class cx_psf_desc(ctypes.Structure):
+    _fields_ = [
+        ("ny", c_int32),
+        ("nx", c_int32),
+        ("n_z", c_int32),
+        ("n_wv", c_int32),
+        ("precision", c_int32),
+        ("has_phase", c_int32),
+        ("spectrally_modulate", c_int32),
+        ("normalize_power", c_int32),
+        ("f_obj", c_double),
+        ("n_medium", c_double),
+        ("NA", c_double),
+        ("power", c_double),
+        ("amplitude", c_double),
+        ("offset_y", c_double),
+        ("offset_x", c_double),
+        ("f_lens", c_double),
+        ("lens_NA", c_double),
+    ]
+
+
+class cx_psf_spectrum(ctypes.Structure):
+    _fields_ = [
+        ("wavelength", ctypes.POINTER(c_double)),
+        ("density", ctypes.POINTER(c_double)),
+        ("dy", ctypes.POINTER(c_double)),
+        ("dx", ctypes.POINTER(c_double)),
+    ]
+
+
+# name -> (restype, argtypes)
+_SIGS = {
+    "cx_version": (c_int32, []),
+    "cx_last_error": (ctypes.c_char_p, []),
+    "cx_fft_size_supported": (c_int32, [c_int32]),
+    "cx_fft1d": (c_int32, [c_void_p, c_void_p, c_int32, ctypes.c_int64, c_int32, c_void_p]),
+    "cx_intensity": (c_int32, [c_void_p, ctypes.c_int64, c_int32, c_void_p, c_void_p, c_void_p]),
+    "cx_prop2d_workspace_size": (c_int32, [ctypes.POINTER(cx_prop2d_desc), ctypes.POINTER(c_size_t)]),
+    "cx_prop2d": (
+        c_int32,
+        [ctypes.POINTER(cx_prop2d_desc), c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_size_t, c_void_p],
+    ),
+    "cx_fill_propagator": (c_int32, [ctypes.POINTER(cx_prop2d_desc), c_void_p, c_void_p, c_void_p]),
+    "cx_psf_workspace_size": (c_int32, [ctypes.POINTER(cx_psf_desc), ctypes.POINTER(c_size_t)]),
+    "cx_psf_4f": (
+        c_int32,
+        [
+            ctypes.POINTER(cx_psf_desc),
+            ctypes.POINTER(cx_psf_spectrum),
+            c_void_p,
+            c_void_p,
+            c_void_p,
+            c_void_p,
+            c_size_t,
+            c_void_p,
+        ],
+    ),
+}
+
+_lib = None
+_lock = threading.Lock()
+
+
+def lib():
+    """Load (once) and return the native library; raises if it is missing."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    with _lock:
+        if _lib is not None:
+            return _lib
+        if not os.path.exists(LIB_PATH):
+            raise RuntimeError(
+                f"chromatix_b200 native library not found at {LIB_PATH}; "
+                "build it with `python -m chromatix_b200.build` (no CPU fallback exists)"
+            )
+        L = ctypes.CDLL(LIB_PATH)
+        for name, (res, args) in _SIGS.items():
+            fn = getattr(L, name)
+            fn.restype = res
+            fn.argtypes = args
+        _lib = L
+    return _lib
+
+
+def check(status: int) -> None:
+    if status != CX_OK:
+        msg = lib().cx_last_error()
+        raise CxError(status, msg.decode() if msg else "")
+
+
+def exported_symbols():
+    """Names declared in include/cx_b200.h that the loaded library must export."""
+    return sorted(_SIGS)
+
+
+# ---------------------------------------------------------------------------
+# torch plumbing
+# ---------------------------------------------------------------------------
+
+
+def torch_mod():
+    import torch
+
+    return torch
+
+
+def stream_handle(device=None) -> int:
+    torch = torch_mod()
+    return torch.cuda.current_stream(device).cuda_stream
+
+
+def ptr(t) -> int:
+    return 0 if t is None else int(t.data_ptr())
+
+
+def workspace(nbytes: int, device):
+    torch = torch_mod()
+    return torch.empty(max(int(nbytes), 256), dtype=torch.uint8, device=device)
+
+
+def to_device_bytes(arr: np.ndarray, device):
+    """Copy a numpy (structured) array to device memory as raw bytes."""
+    torch = torch_mod()
+    b = np.ascontiguousarray(arr).view(np.uint8).reshape(-1)
+    return torch.from_numpy(b.copy()).to(device, non_blocking=False)
+
+
+def require_cuda(t, what="tensor"):
+    if not t.is_cuda:
+        raise ValueError(f"{what} must live on a CUDA device (the library has no CPU path)")

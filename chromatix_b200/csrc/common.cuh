@@ -1,0 +1,51 @@
+// Common device helpers for the chromatix_b200 kernels (sm_100a).
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "../../include/cx_b200.h"
+
+namespace cx {
+
+__device__ __forceinline__ float2 cadd(float2 a, float2 b) { return make_float2(a.x + b.x, a.y + b.y); }
+__device__ __forceinline__ float2 csub(float2 a, float2 b) { return make_float2(a.x - b.x, a.y - b.y); }
+__device__ __forceinline__ float2 cmul(float2 a, float2 b) {
+  return make_float2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
+}
+__device__ __forceinline__ float2 cconj(float2 a) { return make_float2(a.x, -a.y); }
+__device__ __forceinline__ float2 cscale(float2 a, float s) { return make_float2(a.x * s, a.y * s); }
+// multiply by -i (forward) or +i (inverse)
+template <bool INV>
+__device__ __forceinline__ float2 mul_mi(float2 a) {
+  return INV ? make_float2(-a.y, a.x) : make_float2(a.y, -a.x);
+}
+__device__ __forceinline__ float cabs2(float2 a) { return a.x * a.x + a.y * a.y; }
+
+// fftfreq numerator of FFT bin k for length n (numpy/jax convention).
+__host__ __device__ __forceinline__ int freq_index(int k, int n) { return k < (n + 1) / 2 ? k : k - n; }
+
+// Reduce an FP64 phase to [-pi, pi] before the FP32 sin/cos.
+__device__ __forceinline__ float reduce_phase(double ph) {
+  const double inv2pi = 0.15915494309189533576888376337251;
+  const double twopi = 6.283185307179586476925286766559;
+  return (float)(ph - twopi * rint(ph * inv2pi));
+}
+
+// exp(i ph) for an FP64 phase: exact reduction to [-pi, pi] in FP64, then the
+// hardware sin/cos, whose absolute error on [-pi, pi] is at most 2^-21.41
+// (< 4e-7) -- far inside the 1e-5 relative-L2 budget of the accurate mode.
+__device__ __forceinline__ float2 expi_reduced(double ph) {
+  float s, c;
+  __sincosf(reduce_phase(ph), &s, &c);
+  return make_float2(c, s);
+}
+
+// Cast helpers that block FMA contraction, for the float32 reference-order
+// evaluation mode.
+__device__ __forceinline__ float fm(float a, float b) { return __fmul_rn(a, b); }
+__device__ __forceinline__ float fa(float a, float b) { return __fadd_rn(a, b); }
+__device__ __forceinline__ float fs(float a, float b) { return __fsub_rn(a, b); }
+__device__ __forceinline__ float fd(float a, float b) { return __fdiv_rn(a, b); }
+
+}  // namespace cx

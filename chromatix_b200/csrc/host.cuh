@@ -1,0 +1,168 @@
+// Host-side helpers shared by the kernel translation units.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdarg>
+#include <cstdio>
+
+#include "../../include/cx_b200.h"
+#include "fft_engine.cuh"
+
+namespace cx {
+
+// thread-local error message (defined in capi.cu)
+void set_error(const char* fmt, ...);
+
+#define CX_CUDA_TRY(call)                                                                  \
+  do {                                                                                     \
+    cudaError_t e_ = (call);                                                               \
+    if (e_ != cudaSuccess) {                                                               \
+      ::cx::set_error("%s failed: %s (%s:%d)", #call, cudaGetErrorString(e_), __FILE__, __LINE__); \
+      return CX_ERR_CUDA;                                                                  \
+    }                                                                                      \
+  } while (0)
+
+#define CX_LAUNCH_CHECK()                                                                  \
+  do {                                                                                     \
+    cudaError_t e_ = cudaGetLastError();                                                   \
+    if (e_ != cudaSuccess) {                                                               \
+      ::cx::set_error("kernel launch failed: %s (%s:%d)", cudaGetErrorString(e_), __FILE__, __LINE__); \
+      return CX_ERR_CUDA;                                                                  \
+    }                                                                                      \
+  } while (0)
+
+// FFT lengths compiled into the fast path.
+#define CX_FOR_EACH_SIZE(X)                                                                          \
+  X(2) X(3) X(4) X(5) X(6) X(8) X(10) X(12) X(16) X(20) X(24) X(32) X(40) X(48) X(64) X(80) X(96)   \
+  X(128) X(160) X(192) X(256) X(320) X(384) X(512) X(640) X(768) X(1024) X(1280) X(1536) X(2048)    \
+  X(2560) X(3072) X(4096)
+
+inline bool size_supported(int n) {
+  switch (n) {
+#define CX_CASE_(N) case N:
+    CX_FOR_EACH_SIZE(CX_CASE_)
+#undef CX_CASE_
+    return true;
+    default:
+      return false;
+  }
+}
+
+int sm_count();  // of the current device (capi.cu)
+
+// Row kernels: about 384 threads, one team per vector (at most 15 multi-warp
+// teams: named barrier ids 1..15).
+template <int N>
+struct RowCfg {
+  static constexpr int LPV = Plan<N>::LPV;
+  static constexpr int T0 = 384 / LPV > 0 ? 384 / LPV : 1;
+  static constexpr int TEAMS = (LPV > 32 && T0 > 15) ? 15 : T0;
+  static constexpr int THREADS = TEAMS * LPV;
+  static constexpr int MINB = THREADS <= 384 ? 2 : 1;  // register budget: two CTAs per SM
+  static constexpr int TW = tw_len(N);
+  static constexpr size_t SMEM = sizeof(float2) * ((size_t)TW + (size_t)TEAMS * Plan<N>::LEN);
+};
+
+// Column stride (float2) of a V-column tile: a warp transposing a tile
+// touches V columns x (32/V) rows, so the stride must put those 32 elements
+// in distinct bank pairs: stride = 16/V (mod 16) for V <= 16, odd above.
+__host__ __device__ constexpr int col_len(int N, int V) {
+  int l = pad_idx(N - 1) + 1;
+  if (V >= 16) return (l % 2 == 0) ? l + 1 : l;
+  const int want = 16 / V;
+  while (l % 16 != want) ++l;
+  return l;
+}
+
+// Column-tile kernels: V adjacent columns per CTA, one team per column.
+template <int N>
+struct ColCfg {
+  static constexpr int LPV = Plan<N>::LPV;
+  static constexpr int V0 = LPV < 32 ? (256 / LPV > 16 ? 256 / LPV : 16) : (LPV <= 64 ? 8 : 4);
+  static constexpr int TW = tw_len(N);
+  static constexpr size_t smem_for(int v) { return sizeof(float2) * ((size_t)TW + (size_t)v * col_len(N, v)); }
+  static constexpr int V = smem_for(V0) <= 200 * 1024 ? V0 : (smem_for(V0 / 2) <= 200 * 1024 ? V0 / 2 : V0 / 4);
+  static constexpr int LEN = col_len(N, V);
+  static constexpr int THREADS = V * LPV;
+  static constexpr int MINB = THREADS <= 384 ? 2 : 1;
+  static constexpr size_t SMEM = smem_for(V);
+};
+
+// Copy rows [r0, r1) x columns [x0, x0 + V) of a row-major complex matrix
+// (leading dimension ld) into a column tile: tile[c * LEN + pad_idx(dst(r))].
+// Each thread issues four independent loads (two columns per 16-byte load
+// when the row segments are 16-byte aligned) before storing them, so the
+// copy is not serialised on global-memory latency.
+template <int V, int LEN, class DstRow>
+__device__ __forceinline__ void load_col_tile(float2* tile, const float2* __restrict__ src, size_t ld, int x0,
+                                              int ncols, int r0, int r1, DstRow dst) {
+  const int nr = r1 - r0;
+  if (nr <= 0) return;
+  const bool vec = (V % 2 == 0) && (ld % 2 == 0) && (x0 % 2 == 0);
+  if (vec) {
+    constexpr int PR = V / 2;
+    const int total = nr * PR;
+    for (int base = threadIdx.x; base < total; base += 4 * blockDim.x) {
+      float4 v[4];
+#pragma unroll
+      for (int u = 0; u < 4; ++u) {
+        const int idx = base + u * blockDim.x;
+        const int i = idx / PR, c = (idx % PR) * 2;
+        v[u] = make_float4(0.f, 0.f, 0.f, 0.f);
+        if (idx < total && x0 + c + 1 < ncols + 1) {
+          if (x0 + c + 1 < ncols)
+            v[u] = *reinterpret_cast<const float4*>(src + (size_t)(r0 + i) * ld + x0 + c);
+          else if (x0 + c < ncols) {
+            const float2 t = src[(size_t)(r0 + i) * ld + x0 + c];
+            v[u] = make_float4(t.x, t.y, 0.f, 0.f);
+          }
+        }
+      }
+#pragma unroll
+      for (int u = 0; u < 4; ++u) {
+        const int idx = base + u * blockDim.x;
+        if (idx < total) {
+          const int i = idx / PR, c = (idx % PR) * 2;
+          const int d = pad_idx(dst(r0 + i));
+          tile[c * LEN + d] = make_float2(v[u].x, v[u].y);
+          tile[(c + 1) * LEN + d] = make_float2(v[u].z, v[u].w);
+        }
+      }
+    }
+  } else {
+    const int total = nr * V;
+    for (int base = threadIdx.x; base < total; base += 4 * blockDim.x) {
+      float2 v[4];
+#pragma unroll
+      for (int u = 0; u < 4; ++u) {
+        const int idx = base + u * blockDim.x;
+        const int i = idx / V, c = idx % V;
+        v[u] = (idx < total && x0 + c < ncols) ? src[(size_t)(r0 + i) * ld + x0 + c] : make_float2(0.f, 0.f);
+      }
+#pragma unroll
+      for (int u = 0; u < 4; ++u) {
+        const int idx = base + u * blockDim.x;
+        if (idx < total) tile[(idx % V) * LEN + pad_idx(dst(r0 + idx / V))] = v[u];
+      }
+    }
+  }
+}
+
+template <class K>
+inline int persistent_grid(K kernel, int threads, size_t smem, long work_items_ctas) {
+  int occ = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kernel, threads, smem) != cudaSuccess || occ < 1) occ = 1;
+  long g = (long)sm_count() * occ;
+  if (work_items_ctas < g) g = work_items_ctas;
+  if (g < 1) g = 1;
+  return (int)g;
+}
+
+template <class K>
+inline cudaError_t set_smem(K kernel, size_t smem) {
+  if (smem > 48 * 1024) return cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  return cudaSuccess;
+}
+
+}  // namespace cx

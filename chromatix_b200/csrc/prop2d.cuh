@@ -1,0 +1,213 @@
+// Fourier-multiplier propagation: transfer / angular-spectrum / explicit kernel.
+//
+// Reference: functional/propagation.py:168-352 (transfer_propagate,
+// asm_propagate), 355-394 (kernel_propagate FFT branch), 466-580
+// (compute_transfer_propagator, compute_asm_propagator).
+//
+// Three passes over the padded (py, px) grid:
+//   A  row FFT of the ny input rows, zero padding done in the loader
+//      (rows outside the data are never materialised);
+//   B  per V-column tile: column FFT -> x H(ky, kx) evaluated on the fly ->
+//      column IFFT -> 1/(py px), only the output rows are written back;
+//   C  row IFFT of the output rows, crop done in the store.
+#pragma once
+#include "host.cuh"
+
+namespace cx {
+
+struct Prop2DArgs {
+  int ny, nx, py, px, pad_y, pad_x, W;
+  int n_in_planes, n_out_planes;
+  int out_y0, out_ny, out_x0, out_nx;
+  int kernel, precision, remove_evanescent, bandlimit;
+  double n_med, ky0, kx0;
+  const cx_plane* planes;
+  const float2* H;
+};
+
+// --------------------------------------------------------------------------
+// the propagator H(ky, kx) in FFT bin order (already "ifftshifted")
+// --------------------------------------------------------------------------
+__device__ __forceinline__ float2 prop_kernel_accurate(int ky, int kx, const Prop2DArgs& a, const cx_plane& pl) {
+  const double pi = 3.141592653589793238462643383279502884;
+  const double fy = (double)freq_index(ky, a.py) / ((double)a.py * pl.dy);
+  const double fx = (double)freq_index(kx, a.px) / ((double)a.px * pl.dx);
+  const double gy = fy - a.ky0, gx = fx - a.kx0;
+  const double s = gy * gy + gx * gx;
+  if (a.kernel == CX_KERNEL_TRANSFER) {
+    // phase = -pi lam / n z |f - kykx|^2  (propagation.py:493-496)
+    return expi_reduced(-pi * pl.wavelength / a.n_med * pl.z * s);
+  }
+  if (a.bandlimit && (fabs(fy - pl.bl_y0) > pl.bl_hy || fabs(fx - pl.bl_x0) > pl.bl_hx)) return make_float2(0.f, 0.f);
+  const double q = pl.wavelength / a.n_med;
+  const double kern = 1.0 - q * q * s;
+  const double K = 2.0 * pi * fabs(pl.z) * a.n_med / pl.wavelength;
+  const double sh = 2.0 * pi * (fy * pl.shift_y + fx * pl.shift_x);
+  double amp = 1.0, ph;
+  if (kern >= 0.0 || a.remove_evanescent) {
+    ph = K * sqrt(kern > 0.0 ? kern : 0.0) + sh;
+  } else {
+    amp = exp(-K * sqrt(-kern));
+    ph = sh;
+  }
+  if (pl.z < 0.0) ph = -ph;  // conj(exp(i phase)) keeps the decay (propagation.py:556)
+  float2 e = expi_reduced(ph);
+  return make_float2((float)amp * e.x, (float)amp * e.y);
+}
+
+// float32 evaluation in the reference's operation order (no FMA contraction)
+__device__ __forceinline__ float2 prop_kernel_ref32(int ky, int kx, const Prop2DArgs& a, const cx_plane& pl) {
+  const float PI = 3.14159265358979323846f, TWO_PI = 6.28318530717958647692f;
+  const float dyf = (float)pl.dy, dxf = (float)pl.dx;
+  const float fy = fm(fd((float)freq_index(ky, a.py), (float)a.py), fd(1.f, dyf));
+  const float fx = fm(fd((float)freq_index(kx, a.px), (float)a.px), fd(1.f, dxf));
+  const float gy = fs(fy, (float)a.ky0), gx = fs(fx, (float)a.kx0);
+  const float s = fa(fm(gy, gy), fm(gx, gx));
+  const float lam = (float)pl.wavelength, n = (float)a.n_med, z = (float)pl.z;
+  if (a.kernel == CX_KERNEL_TRANSFER) {
+    const float ph = fm(fm(fd(fm(-PI, lam), n), z), s);
+    float sn, cs;
+    sincosf(ph, &sn, &cs);
+    return make_float2(cs, sn);
+  }
+  if (a.bandlimit && (fabsf(fs(fy, (float)pl.bl_y0)) > (float)pl.bl_hy || fabsf(fs(fx, (float)pl.bl_x0)) > (float)pl.bl_hx))
+    return make_float2(0.f, 0.f);
+  const float q = fd(lam, n);
+  const float kern = fs(1.f, fm(fm(q, q), s));
+  const float A = fd(fm(fabsf(z), n), lam);
+  const float c = fm(TWO_PI, A);
+  const float sh = fm(TWO_PI, fa(fm(fy, (float)pl.shift_y), fm(fx, (float)pl.shift_x)));
+  float amp = 1.f, ph;
+  if (kern >= 0.f || a.remove_evanescent) {
+    ph = fa(fm(c, __fsqrt_rn(kern > 0.f ? kern : 0.f)), sh);
+  } else {
+    amp = expf(-fm(c, __fsqrt_rn(-kern)));
+    ph = sh;
+  }
+  float sn, cs;
+  sincosf(ph, &sn, &cs);
+  if (z < 0.f) sn = -sn;
+  return make_float2(amp * cs, amp * sn);
+}
+
+__device__ __forceinline__ float2 prop_kernel(int ky, int kx, const Prop2DArgs& a, const cx_plane& pl) {
+  if (a.kernel == CX_KERNEL_EXPLICIT)
+    return a.H[((size_t)pl.h_plane * a.py + ky) * a.px + kx];
+  return a.precision == CX_PREC_REF32 ? prop_kernel_ref32(ky, kx, a, pl) : prop_kernel_accurate(ky, kx, a, pl);
+}
+
+// --------------------------------------------------------------------------
+// pass A: forward row FFT with zero padding in the loader
+// --------------------------------------------------------------------------
+template <int NX>
+__global__ void __launch_bounds__(RowCfg<NX>::THREADS, RowCfg<NX>::MINB) k_prop_rows_fwd(const float2* __restrict__ u,
+                                                                      float2* __restrict__ T, Prop2DArgs a) {
+  using C = RowCfg<NX>;
+  extern __shared__ float2 sm[];
+  float2* tw = sm;
+  init_twiddles<NX>(tw, threadIdx.x, blockDim.x);
+  __syncthreads();
+  const int team = threadIdx.x / C::LPV, lane = threadIdx.x % C::LPV;
+  float2* s = sm + C::TW + team * Plan<NX>::LEN;
+  const long total = (long)a.n_in_planes * a.ny;
+  for (long base = (long)blockIdx.x * C::TEAMS; base < total; base += (long)gridDim.x * C::TEAMS) {
+    const long item = base + team;
+    const bool valid = item < total;
+    const int p = valid ? (int)(item / a.ny) : 0;
+    const int y = valid ? (int)(item % a.ny) : 0;
+    const int b = p / a.W, w = p % a.W;
+    const float2* src = u + ((size_t)b * a.ny + y) * a.nx * a.W + w;
+    float2* dst = T + ((size_t)p * a.ny + y) * a.px;
+    auto load = [&](int n) -> float2 {
+      const int x = n - a.pad_x;
+      return (valid && x >= 0 && x < a.nx) ? src[(size_t)x * a.W] : make_float2(0.f, 0.f);
+    };
+    auto store = [&](int k, float2 v, int) {
+      if (valid) dst[k] = v;
+    };
+    team_fft<NX, false>(s, tw, lane, team, load, store);
+  }
+}
+
+// --------------------------------------------------------------------------
+// pass B: column FFT -> x H -> column IFFT on V-column tiles
+// --------------------------------------------------------------------------
+template <int NY>
+__global__ void __launch_bounds__(ColCfg<NY>::THREADS, ColCfg<NY>::MINB) k_prop_cols(const float2* __restrict__ T,
+                                                                  float2* __restrict__ T2, Prop2DArgs a) {
+  using C = ColCfg<NY>;
+  constexpr int V = C::V, LEN = C::LEN;
+  extern __shared__ float2 sm[];
+  float2* tw = sm;
+  float2* tile = sm + C::TW;
+  init_twiddles<NY>(tw, threadIdx.x, blockDim.x);
+  const int team = threadIdx.x / C::LPV, lane = threadIdx.x % C::LPV;
+  float2* s = tile + team * LEN;
+  const int tiles_x = (a.px + V - 1) / V;
+  const long total = (long)tiles_x * a.n_out_planes;
+  const float scale = 1.0f / ((float)a.py * (float)a.px);
+  for (long t = blockIdx.x; t < total; t += gridDim.x) {
+    const int q = (int)(t / tiles_x);
+    const int x0 = (int)(t % tiles_x) * V;
+    const cx_plane pl = a.planes[q];
+    const int p_in = pl.in_plane;
+    __syncthreads();
+    // cooperative, coalesced load of the ny data rows of this column tile
+    load_col_tile<V, LEN>(tile, T + (size_t)p_in * a.ny * a.px, a.px, x0, a.px, 0, a.ny,
+                          [&](int r) { return r + a.pad_y; });
+    __syncthreads();
+    const int kx = x0 + team;
+    const bool valid = kx < a.px;
+    auto load1 = [&](int n) -> float2 {
+      return (n >= a.pad_y && n < a.pad_y + a.ny) ? s[pad_idx(n)] : make_float2(0.f, 0.f);
+    };
+    auto store1 = [&](int k, float2 v, int) { s[pad_idx(k)] = valid ? cmul(v, prop_kernel(k, kx, a, pl)) : v; };
+    team_fft<NY, false>(s, tw, lane, team, load1, store1);
+    team_sync<C::LPV>(team);
+    auto load2 = [&](int n) -> float2 { return s[pad_idx(n)]; };
+    auto store2 = [&](int k, float2 v, int) { s[pad_idx(k)] = cscale(v, scale); };
+    team_fft<NY, true>(s, tw, lane, team, load2, store2);
+    __syncthreads();
+    for (int idx = threadIdx.x; idx < a.out_ny * V; idx += blockDim.x) {
+      const int r = idx / V, c = idx % V, x = x0 + c;
+      if (x < a.px) T2[((size_t)q * a.out_ny + r) * a.px + x] = tile[c * LEN + pad_idx(a.out_y0 + r)];
+    }
+  }
+}
+
+// --------------------------------------------------------------------------
+// pass C: inverse row FFT of the output rows, crop in the store
+// --------------------------------------------------------------------------
+template <int NX>
+__global__ void __launch_bounds__(RowCfg<NX>::THREADS, RowCfg<NX>::MINB) k_prop_rows_inv(const float2* __restrict__ T2,
+                                                                      float2* __restrict__ out, Prop2DArgs a) {
+  using C = RowCfg<NX>;
+  extern __shared__ float2 sm[];
+  float2* tw = sm;
+  init_twiddles<NX>(tw, threadIdx.x, blockDim.x);
+  __syncthreads();
+  const int team = threadIdx.x / C::LPV, lane = threadIdx.x % C::LPV;
+  float2* s = sm + C::TW + team * Plan<NX>::LEN;
+  const long total = (long)a.n_out_planes * a.out_ny;
+  for (long base = (long)blockIdx.x * C::TEAMS; base < total; base += (long)gridDim.x * C::TEAMS) {
+    const long item = base + team;
+    const bool valid = item < total;
+    const int q = valid ? (int)(item / a.out_ny) : 0;
+    const int r = valid ? (int)(item % a.out_ny) : 0;
+    const int b = q / a.W, w = q % a.W;
+    const float2* src = T2 + ((size_t)q * a.out_ny + r) * a.px;
+    float2* dst = out + ((size_t)b * a.out_ny + r) * a.out_nx * a.W + w;
+    auto load = [&](int n) -> float2 { return valid ? src[n] : make_float2(0.f, 0.f); };
+    auto store = [&](int k, float2 v, int) {
+      const int x = k - a.out_x0;
+      if (valid && x >= 0 && x < a.out_nx) dst[(size_t)x * a.W] = v;
+    };
+    team_fft<NX, true>(s, tw, lane, team, load, store);
+  }
+}
+
+// dispatchers (defined in prop2d_rows.cu / prop2d_cols.cu)
+cx_status dispatch_rows_fwd(int n, const float2* u, float2* T, const Prop2DArgs& a, cudaStream_t st);
+cx_status dispatch_cols(int n, const float2* T, float2* T2, const Prop2DArgs& a, cudaStream_t st);
+cx_status dispatch_rows_inv(int n, const float2* T2, float2* out, const Prop2DArgs& a, cudaStream_t st);
+}  // namespace cx

@@ -1,0 +1,277 @@
+// C API of the fused batched 4f PSF (kernels in psf.cuh).
+#include <cmath>
+#include <cstdlib>
+
+#include "psf.cuh"
+
+namespace cx {
+
+// ---------------------------------------------------------------------------
+// pass 0: pupil pixel counts (one counter per wavelength, zeroed by the host)
+// ---------------------------------------------------------------------------
+// One thread per (wavelength, row): the pupil is a disc, so the pixels of a
+// row that pass the (exact, per-pixel) pupil predicate form one contiguous
+// run around the centre column; its ends are found by bisection with the
+// same predicate the kernels use.  Also records the exact range of rows that
+// hold pupil pixels: srange[w] = max(ny - y), srange[8 + w] = max(y + 1)
+// (zero-initialised, so an empty pupil gives the empty range [ny, 0)).
+__global__ void k_psf_count(PsfArgs a, unsigned long long* counts, int* srange) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= a.W * a.ny) return;
+  const int w = i / a.ny, y = i % a.ny;
+  const PsfWv& p = a.wv[w];
+  const int xc = a.nx / 2;  // grid value 0 (x = nx/2): the widest point of the chord
+  if (!in_pupil(a, p, y, xc)) return;
+  // last inside column to the right of xc, first inside column to the left
+  int lo = xc, hi = a.nx;  // in_pupil(lo) true, columns >= hi outside
+  while (hi - lo > 1) {
+    const int m = (lo + hi) / 2;
+    if (in_pupil(a, p, y, m)) lo = m; else hi = m;
+  }
+  const int right = lo;
+  lo = -1;
+  hi = xc;  // columns <= lo outside, in_pupil(hi) true
+  while (hi - lo > 1) {
+    const int m = (lo + hi) / 2;
+    if (in_pupil(a, p, y, m)) hi = m; else lo = m;
+  }
+  const int left = hi;
+  atomicAdd(counts + w, (unsigned long long)(right - left + 1));
+  atomicMax(srange + w, a.ny - y);
+  atomicMax(srange + 8 + w, y + 1);
+}
+
+// ---------------------------------------------------------------------------
+// materialised source field (objective_point_source [-> phase_change]) for
+// callers that need u itself: out (zc, ny, nx, W) complex64, without the lens
+// normalisation
+// ---------------------------------------------------------------------------
+__global__ void k_psf_source(PsfArgs a, float2* __restrict__ out) {
+  const long per = (long)a.ny * a.nx;
+  const long total = per * a.nz * a.W;
+  const double PI = 3.141592653589793238462643383279502884;
+  for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < total; i += (long)gridDim.x * blockDim.x) {
+    const int w = (int)(i % a.W);
+    const long pix = (i / a.W) % per;
+    const int iz = (int)(i / ((long)a.W * per));
+    const int y = (int)(pix / a.nx), x = (int)(pix % a.nx);
+    const PsfWv& p = a.wv[w];
+    float2 v = make_float2(0.f, 0.f);
+    if (in_pupil(a, p, y, x)) {
+      const float2 cst = psf_const(a, w, a.counts);
+      const double z = a.z[iz];
+      if (a.precision == CX_PREC_REF32) {
+        const float gyf = fm((float)p.dy, (float)y - (float)a.ny * 0.5f);
+        const float gxf = fm((float)p.dx, (float)x - (float)a.nx * 0.5f);
+        const float dyo = fs(gyf, (float)a.offy), dxo = fs(gxf, (float)a.offx);
+        const float r2 = fa(fm(dyo, dyo), fm(dxo, dxo));
+        const float phs = fd(fm(fm(-3.14159265358979f, fd((float)z, (float)a.f_obj)), r2), p.L2f);
+        float s1, c1;
+        sincosf(phs, &s1, &c1);
+        v = cmul(cst, make_float2(c1, s1));
+        if (a.has_phase) {
+          float s2, c2;
+          sincosf(fm(a.phase[pix], p.modf), &s2, &c2);
+          v = cmul(v, make_float2(c2, s2));
+        }
+      } else {
+        const double gyo = p.dy * ((double)y - (double)a.ny * 0.5) - a.offy;
+        const double gxo = p.dx * ((double)x - (double)a.nx * 0.5) - a.offx;
+        double ph = -PI * (z / a.f_obj) / p.L2 * (gyo * gyo + gxo * gxo);
+        if (a.has_phase) ph += (double)a.phase[pix] * p.mod;
+        v = cmul(cst, expi_reduced(ph));
+      }
+    }
+    out[i] = v;
+  }
+}
+
+// rows of the grid that can hold pupil pixels for wavelength w (a
+// conservative superset, one row of margin: the kernels re-test every row)
+static void psf_rows(const cx_psf_desc* d, const cx_psf_spectrum* spec, int w, int* ylo, int* nrows) {
+  const double lam0 = spec->wavelength[0];
+  const double D = 2.0 * d->f_obj * d->NA / d->n_medium;
+  double r = (lam0 / spec->wavelength[w]) * D / 2.0;
+  if (d->lens_NA > 0.0) {
+    const double rl = (lam0 / spec->wavelength[w]) * (2.0 * d->f_lens * d->lens_NA / d->n_medium) / 2.0;
+    r = rl < r ? rl : r;
+  }
+  const double h = r / spec->dy[w];
+  long lo = (long)floor(0.5 * d->ny - h) - 1, hi = (long)ceil(0.5 * d->ny + h) + 1;
+  if (lo < 0) lo = 0;
+  if (hi > d->ny - 1) hi = d->ny - 1;
+  if (hi < lo) hi = lo;
+  *ylo = (int)lo;
+  *nrows = (int)(hi - lo + 1);
+}
+
+// Row spectra of one z-chunk are written by pass A and read back by pass B;
+// the chunk is sized to stay L2-resident in between (CX_PSF_L2_MB, default
+// 64 MiB of the 126 MB L2).
+static size_t psf_chunk_budget() {
+  static size_t cached = 0;
+  if (!cached) {
+    const char* e = getenv("CX_PSF_L2_MB");
+    const long mb = e ? atol(e) : 64;
+    cached = (size_t)(mb > 0 ? mb : 64) << 20;
+  }
+  return cached;
+}
+
+static cx_status psf_check(const cx_psf_desc* d) {
+  if (!d || d->ny <= 0 || d->nx <= 0 || d->n_z <= 0 || d->n_wv <= 0 || d->n_wv > PSF_MAX_WV) {
+    set_error("invalid PSF descriptor (1 <= n_wv <= %d)", PSF_MAX_WV);
+    return CX_ERR_INVALID;
+  }
+  if (!size_supported(d->ny) || !size_supported(d->nx)) {
+    set_error("PSF grid %dx%d: FFT length not supported", d->ny, d->nx);
+    return CX_ERR_UNSUPPORTED;
+  }
+  if (!(d->f_lens > 0.0)) {
+    set_error("cx_psf_4f needs a forward lens (f_lens > 0); use cx_optical_fft for inverse lenses");
+    return CX_ERR_INVALID;
+  }
+  return CX_OK;
+}
+
+static PsfArgs psf_make_args(const cx_psf_desc* d, const cx_psf_spectrum* spec, bool with_lens) {
+  PsfArgs a{};
+  a.ny = d->ny;
+  a.nx = d->nx;
+  a.nz = d->n_z;
+  a.W = d->n_wv;
+  a.precision = d->precision;
+  a.has_phase = d->has_phase;
+  a.normalize = d->normalize_power;
+  a.f_obj = d->f_obj;
+  a.n = d->n_medium;
+  a.amp = d->amplitude;
+  a.offy = d->offset_y;
+  a.offx = d->offset_x;
+  a.power = d->power;
+  const double lam0 = spec->wavelength[0];
+  const double D = 2.0 * d->f_obj * d->NA / d->n_medium;                                   // sources.py:205
+  const double DL = d->lens_NA > 0.0 ? 2.0 * d->f_lens * d->lens_NA / d->n_medium : -1.0;  // lenses.py:90
+  for (int w = 0; w < a.W; ++w) {
+    PsfWv& p = a.wv[w];
+    p.lam = spec->wavelength[w];
+    p.dens = spec->density[w];
+    p.dy = spec->dy[w];
+    p.dx = spec->dx[w];
+    p.L2 = p.lam * d->f_obj / d->n_medium;
+    const double r = (lam0 / p.lam) * D / 2.0;
+    p.R2 = r * r;
+    const double rl = (lam0 / p.lam) * DL / 2.0;
+    p.RL2 = DL > 0.0 ? rl * rl : -1.0;
+    p.mod = d->spectrally_modulate ? lam0 / p.lam : 1.0;
+    // optical_fft forward normalisation -1j * dy dx / L_sq, L_sq = lam f / n (convenience.py:33,43)
+    if (with_lens) {
+      const double Lsq = p.lam * d->f_lens / d->n_medium;
+      p.lens_re = 0.0;
+      p.lens_im = -(p.dy * p.dx) / Lsq;
+    } else {
+      p.lens_re = 1.0;
+      p.lens_im = 0.0;
+    }
+    // float32 reference-order values
+    const float Lf = sqrtf((float)p.lam * (float)d->f_obj / (float)d->n_medium);
+    p.L2f = Lf * Lf;
+    const float rf = (float)lam0 / (float)p.lam * (float)D / 2.0f;
+    p.R2f = rf * rf;
+    const float rlf = (float)lam0 / (float)p.lam * (float)DL / 2.0f;
+    p.RL2f = DL > 0.0 ? rlf * rlf : -1.0f;
+    p.modf = (float)p.mod;
+  }
+  return a;
+}
+
+// workspace: 256 bytes of pupil counters, then one chunk of row spectra
+// (sized for the worst case rowsum = n_wv * ny, independent of the spectrum)
+static size_t psf_ws(const cx_psf_desc* d) {
+  const size_t worst_z = (size_t)d->n_wv * d->ny * d->nx * sizeof(float2);
+  const size_t t = psf_chunk_budget() > worst_z ? psf_chunk_budget() : worst_z;
+  return 256 + ((t + 255) & ~(size_t)255);
+}
+
+}  // namespace cx
+
+using namespace cx;
+
+extern "C" cx_status cx_psf_workspace_size(const cx_psf_desc* d, size_t* bytes) {
+  cx_status s = psf_check(d);
+  if (s != CX_OK) return s;
+  if (!bytes) return CX_ERR_INVALID;
+  *bytes = psf_ws(d);
+  return CX_OK;
+}
+
+extern "C" cx_status cx_psf_4f(const cx_psf_desc* d, const cx_psf_spectrum* spec, const double* z_dev,
+                               const float* phase, float* intensity_out, void* workspace, size_t workspace_bytes,
+                               cx_stream_t stream) {
+  cx_status s = psf_check(d);
+  if (s != CX_OK) return s;
+  if (!spec || !spec->wavelength || !spec->density || !spec->dy || !spec->dx || !z_dev || !intensity_out ||
+      !workspace || (d->has_phase && !phase)) {
+    set_error("null pointer argument");
+    return CX_ERR_INVALID;
+  }
+  if (workspace_bytes < psf_ws(d)) {
+    set_error("workspace too small: %zu < %zu", workspace_bytes, psf_ws(d));
+    return CX_ERR_WORKSPACE;
+  }
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  PsfArgs a = psf_make_args(d, spec, /*with_lens=*/true);
+  a.z = z_dev;
+  a.phase = phase;
+  a.out = intensity_out;
+  unsigned long long* counts = static_cast<unsigned long long*>(workspace);
+  int* srange = reinterpret_cast<int*>(static_cast<char*>(workspace) + 64);
+  a.counts = counts;
+  a.srange = srange;
+  a.T = reinterpret_cast<float2*>(static_cast<char*>(workspace) + 256);
+  CX_CUDA_TRY(cudaMemsetAsync(workspace, 0, 256, st));
+  k_psf_count<<<(a.W * a.ny + 127) / 128, 128, 0, st>>>(a, counts, srange);
+  CX_LAUNCH_CHECK();
+  a.rowsum = 0;
+  for (int w = 0; w < a.W; ++w) {
+    psf_rows(d, spec, w, &a.ylo[w], &a.nrows[w]);
+    a.prefix[w] = a.rowsum;
+    a.rowsum += a.nrows[w];
+  }
+  // z planes per chunk: as many compact planes as the workspace holds
+  const size_t zbytes = sizeof(float2) * (size_t)a.rowsum * a.nx;
+  int zc = (int)((psf_ws(d) - 256) / zbytes);
+  if (zc < 1) zc = 1;
+  if (zc > a.nz) zc = a.nz;
+  for (int z0 = 0; z0 < a.nz; z0 += zc) {
+    a.z0 = z0;
+    a.zc = (a.nz - z0) < zc ? (a.nz - z0) : zc;
+    if ((s = psf_dispatch_rows(a.nx, a, st)) != CX_OK) return s;
+    if ((s = psf_dispatch_cols(a.ny, a, st)) != CX_OK) return s;
+  }
+  return CX_OK;
+}
+
+extern "C" cx_status cx_psf_source(const cx_psf_desc* d, const cx_psf_spectrum* spec, const double* z_dev,
+                                   const float* phase, void* u_out, void* workspace, size_t workspace_bytes,
+                                   cx_stream_t stream) {
+  if (!d || d->ny <= 0 || d->nx <= 0 || d->n_z <= 0 || d->n_wv <= 0 || d->n_wv > PSF_MAX_WV || !spec || !z_dev ||
+      !u_out || !workspace || workspace_bytes < 256 || (d->has_phase && !phase)) {
+    set_error("invalid point-source arguments");
+    return CX_ERR_INVALID;
+  }
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  PsfArgs a = psf_make_args(d, spec, /*with_lens=*/false);
+  a.z = z_dev;
+  a.phase = phase;
+  unsigned long long* counts = static_cast<unsigned long long*>(workspace);
+  int* srange = reinterpret_cast<int*>(static_cast<char*>(workspace) + 64);
+  a.counts = counts;
+  a.srange = srange;
+  CX_CUDA_TRY(cudaMemsetAsync(workspace, 0, 256, st));
+  k_psf_count<<<(a.W * a.ny + 127) / 128, 128, 0, st>>>(a, counts, srange);
+  CX_LAUNCH_CHECK();
+  k_psf_source<<<sm_count() * 8, 256, 0, st>>>(a, static_cast<float2*>(u_out));
+  CX_LAUNCH_CHECK();
+  return CX_OK;
+}

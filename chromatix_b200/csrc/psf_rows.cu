@@ -1,0 +1,30 @@
+// Row pass of the fused PSF (see psf.cuh).
+#include "psf.cuh"
+
+namespace cx {
+
+template <int NX>
+static cx_status launch_psf_rows(const PsfArgs& a, cudaStream_t st) {
+  using C = RowCfg<NX>;
+  auto k = k_psf_rows<NX>;
+  CX_CUDA_TRY(set_smem(k, C::SMEM));
+  const long items = ((long)a.zc * a.rowsum + C::TEAMS - 1) / C::TEAMS;
+  const int grid = persistent_grid(k, C::THREADS, C::SMEM, items);
+  k<<<grid, C::THREADS, C::SMEM, st>>>(a);
+  CX_LAUNCH_CHECK();
+  return CX_OK;
+}
+
+cx_status psf_dispatch_rows(int n, const PsfArgs& a, cudaStream_t st) {
+  switch (n) {
+#define CX_CASE_(N) \
+  case N:           \
+    return launch_psf_rows<N>(a, st);
+    CX_FOR_EACH_SIZE(CX_CASE_)
+#undef CX_CASE_
+  }
+  set_error("FFT length %d is not supported", n);
+  return CX_ERR_UNSUPPORTED;
+}
+
+}  // namespace cx

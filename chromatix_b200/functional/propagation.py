@@ -1,0 +1,336 @@
+"""Free-space propagation with the same signatures as ``chromatix.functional``.
+
+Reference: functional/propagation.py.  The Fourier-multiplier propagators
+(transfer, angular spectrum / exact, explicit kernel) run as one fused
+three-pass CUDA pipeline (``cx_prop2d``): zero padding in the first FFT's
+loader, the transfer function evaluated on the fly between the column FFT and
+IFFT, the crop in the last FFT's store.
+"""
+
+from __future__ import annotations
+
+from typing import Literal
+
+import numpy as np
+
+from .. import _native as nat
+from .. import config
+from ..core.field import Field, shift_grid
+
+__all__ = [
+    "transform_propagate",
+    "transform_propagate_sas",
+    "transfer_propagate",
+    "asm_propagate",
+    "kernel_propagate",
+    "compute_transfer_propagator",
+    "compute_asm_propagator",
+    "compute_padding_transform",
+    "compute_padding_transfer",
+    "compute_padding_exact",
+]
+
+_BOUNDARIES = ("tukey", "super_gaussian")
+
+
+def _pad_tuple(pad_width):
+    if isinstance(pad_width, (int, np.integer)):
+        return int(pad_width), int(pad_width)
+    py, px = pad_width
+    return int(py), int(px)
+
+
+def _z_array(z):
+    z = np.asarray(z, dtype=np.float64)
+    if z.size > 1:
+        return z.reshape(-1), (z.size,)
+    return z.reshape(-1)[:1], ()
+
+
+def _bandlimit_rect(z, lam, shift_yx, dy, dx, py, px, prec: str):
+    """Matsushima band-limit rectangle (functional/propagation.py:557-579)."""
+    dt = np.float32 if prec == "ref32" else np.float64
+    s = np.asarray(shift_yx, dtype=dt)
+    ext = np.array([dy * py, dx * px], dtype=dt)
+    df = dt(1) / ext
+    z = dt(z)
+    lam = dt(lam)
+    with np.errstate(divide="ignore"):
+        klp = ((s + 1 / (2 * df)) ** (-2) * z**2 + 1) ** (-0.5) / lam
+        kln = ((s - 1 / (2 * df)) ** (-2) * z**2 + 1) ** (-0.5) / lam
+    k0 = 0.5 * (np.sign(s + ext) * klp + np.sign(s - ext) * kln)
+    kw = np.sign(s + ext) * klp - np.sign(s - ext) * kln
+    return k0.astype(np.float64), (kw / 2).astype(np.float64)
+
+
+def _plan_planes(field: Field, zs, zshape, py, px, shift_yx=(0.0, 0.0), bandlimit=False, prec="accurate",
+                 h_index=None, batch_shape=None):
+    """Per-output-plane launch parameters.
+
+    Output batch = broadcast(field batch, z batch) as in the reference
+    (z broadcast to the innermost batch, utils/shapes.py:52-58).
+    """
+    B = field.batch_shape if batch_shape is None else tuple(batch_shape)
+    out_batch = np.broadcast_shapes(B, zshape)
+    nb_in = int(np.prod(B)) if B else 1
+    nb_out = int(np.prod(out_batch)) if out_batch else 1
+    in_idx = np.broadcast_to(np.arange(nb_in).reshape(B if B else ()), out_batch).reshape(-1)
+    if zshape:
+        z_idx = np.broadcast_to(np.arange(zs.size).reshape(zshape), out_batch).reshape(-1)
+    else:
+        z_idx = np.zeros(nb_out, dtype=np.int64)
+    W = field.n_wv
+    dxw = field.dx_wv
+    wl = field.spectrum.wavelength
+    planes = np.zeros(nb_out * W, dtype=nat.PLANE_DTYPE)
+    sy, sx = np.asarray(shift_yx, dtype=np.float64).reshape(2)
+    for ob in range(nb_out):
+        for w in range(W):
+            q = ob * W + w
+            z = float(zs[z_idx[ob]])
+            p = planes[q]
+            planes[q]["z"] = z
+            planes[q]["wavelength"] = wl[w]
+            planes[q]["dy"] = dxw[w, 0]
+            planes[q]["dx"] = dxw[w, 1]
+            planes[q]["shift_y"] = sy
+            planes[q]["shift_x"] = sx
+            planes[q]["in_plane"] = int(in_idx[ob]) * W + w
+            planes[q]["h_plane"] = int(h_index[q]) if h_index is not None else 0
+            if bandlimit:
+                k0, km = _bandlimit_rect(z, wl[w], (sy, sx), dxw[w, 0], dxw[w, 1], py, px, prec)
+                planes[q]["bl_y0"], planes[q]["bl_x0"] = k0
+                planes[q]["bl_hy"], planes[q]["bl_hx"] = km
+            del p
+    return planes, out_batch, nb_in, nb_out
+
+
+def _run_prop2d(field: Field, kernel: int, zs, zshape, n, pad_width, kykx=(0.0, 0.0), shift_yx=(0.0, 0.0),
+                remove_evanescent=False, bandlimit=False, mode="full", H=None, h_index=None, precision=None):
+    torch = nat.torch_mod()
+    nat.require_cuda(field.u, "Field.u")
+    prec = precision or config.get_precision()
+    py_, px_ = _pad_tuple(pad_width)
+    ny, nx = field.spatial_shape
+    py, px = ny + 2 * py_, nx + 2 * px_
+    planes, out_batch, nb_in, nb_out = _plan_planes(field, zs, zshape, py, px, shift_yx, bandlimit, prec, h_index)
+    W = field.n_wv
+    d = nat.cx_prop2d_desc()
+    d.ny, d.nx, d.pad_y, d.pad_x = ny, nx, py_, px_
+    d.n_wv = W
+    d.n_in_planes = nb_in * W
+    d.n_out_planes = nb_out * W
+    d.mode_same = 1 if mode == "same" else 0
+    d.kernel = kernel
+    d.precision = config.precision_code(prec)
+    d.remove_evanescent = int(bool(remove_evanescent))
+    d.bandlimit = int(bool(bandlimit))
+    d.n_medium = float(n)
+    ky0, kx0 = np.asarray(kykx, dtype=np.float64).reshape(2)
+    d.ky0, d.kx0 = float(ky0), float(kx0)
+    L = nat.lib()
+    ws_bytes = nat.c_size_t(0)
+    nat.check(L.cx_prop2d_workspace_size(d, ws_bytes))
+    dev = field.device
+    u_in = field.u.contiguous()
+    oy, ox = (ny, nx) if mode == "same" else (py, px)
+    out_shape = tuple(out_batch) + (oy, ox) + ((W,) if field.chromatic else ())
+    u_out = torch.empty(out_shape, dtype=torch.complex64, device=dev)
+    ws = nat.workspace(ws_bytes.value, dev)
+    planes_dev = nat.to_device_bytes(planes, dev)
+    nat.check(L.cx_prop2d(d, nat.ptr(planes_dev), nat.ptr(u_in), nat.ptr(u_out), nat.ptr(H), nat.ptr(ws),
+                          ws_bytes.value, nat.stream_handle(dev)))
+    return u_out
+
+
+def _check_mode(mode):
+    if mode not in ("full", "same"):
+        raise ValueError(f"mode must be 'full' or 'same', got {mode!r}")
+
+
+def _check_boundary(absorbing_boundary):
+    # kernel_propagate applies the pupil to the pre-propagation field object and
+    # then returns field.replace(u=u): the boundary never reaches the output
+    # (functional/propagation.py:460-463).  Validated, then (faithfully) unused.
+    assert absorbing_boundary is None or absorbing_boundary in _BOUNDARIES, (
+        f"The absorbing_boundary must be None or in {_BOUNDARIES}."
+    )
+
+
+def transfer_propagate(field: Field, z, n, pad_width, cval: float = 0, absorbing_boundary=None,
+                       absorbing_boundary_width: float = 0.65, kykx=(0.0, 0.0), shift_yx=(0.0, 0.0),
+                       output_dx=None, output_shape=None, use_czt: bool = True,
+                       mode: Literal["full", "same"] = "full", *, precision=None) -> Field:
+    """Fresnel transfer propagation (functional/propagation.py:168-252)."""
+    _check_mode(mode)
+    _check_boundary(absorbing_boundary)
+    if output_dx is not None or output_shape is not None:
+        from .rescaled import rescaled_propagate
+
+        return rescaled_propagate(field, nat.CX_KERNEL_TRANSFER, z, n, pad_width, kykx=kykx, shift_yx=shift_yx,
+                                  output_dx=output_dx, output_shape=output_shape, use_czt=use_czt, mode=mode,
+                                  cval=cval, precision=precision)
+    if cval != 0:
+        raise NotImplementedError("non-zero cval padding is not supported by the fused loader")
+    zs, _ = _z_array(z)
+    # transfer_propagate broadcasts z only when it has more than one entry
+    zshape = (zs.size,) if np.asarray(z).size > 1 else ()
+    u = _run_prop2d(field, nat.CX_KERNEL_TRANSFER, zs, zshape, n, pad_width, kykx=kykx, mode=mode,
+                    precision=precision)
+    out = shift_grid(field.replace(u=u), shift_yx)
+    return out
+
+
+def asm_propagate(field: Field, z, n, pad_width, cval: float = 0, absorbing_boundary=None,
+                  absorbing_boundary_width: float = 0.65, kykx=(0.0, 0.0), remove_evanescent: bool = False,
+                  bandlimit: bool = False, shift_yx=(0.0, 0.0), output_dx=None, output_shape=None,
+                  use_czt: bool = True, mode: Literal["full", "same"] = "full", *, precision=None) -> Field:
+    """Angular-spectrum propagation; ``remove_evanescent=True`` is the "exact"
+    method (functional/propagation.py:255-352)."""
+    _check_mode(mode)
+    _check_boundary(absorbing_boundary)
+    if output_dx is not None or output_shape is not None:
+        from .rescaled import rescaled_propagate
+
+        return rescaled_propagate(field, nat.CX_KERNEL_ASM, z, n, pad_width, kykx=kykx, shift_yx=shift_yx,
+                                  output_dx=output_dx, output_shape=output_shape, use_czt=use_czt, mode=mode,
+                                  remove_evanescent=remove_evanescent, bandlimit=bandlimit, cval=cval,
+                                  precision=precision)
+    if cval != 0:
+        raise NotImplementedError("non-zero cval padding is not supported by the fused loader")
+    zs, zshape = _z_array(z)
+    u = _run_prop2d(field, nat.CX_KERNEL_ASM, zs, zshape, n, pad_width, kykx=kykx, shift_yx=shift_yx,
+                    remove_evanescent=remove_evanescent, bandlimit=bandlimit, mode=mode, precision=precision)
+    return shift_grid(field.replace(u=u), shift_yx)
+
+
+def _planar_propagator(field: Field, propagator):
+    """Explicit propagator -> planar (HP, py, px) device tensor + plane index map."""
+    torch = nat.torch_mod()
+    H = propagator if isinstance(propagator, torch.Tensor) else torch.as_tensor(np.asarray(propagator))
+    H = H.to(device=field.device, dtype=torch.complex64)
+    ny, nx = field.spatial_shape
+    W = field.n_wv
+    if field.chromatic:
+        if H.ndim >= 3 and H.shape[-1] in (1, W) and tuple(H.shape[-3:-1]) == (ny, nx):
+            H = H.movedim(-1, -3)  # (..., wv, py, px)
+            if H.shape[-3] == 1 and W > 1:
+                H = H.expand(*H.shape[:-3], W, ny, nx)
+        elif tuple(H.shape[-2:]) == (ny, nx):
+            H = H.unsqueeze(-3).expand(*H.shape[:-2], W, ny, nx)
+        else:
+            raise ValueError(f"propagator shape {tuple(H.shape)} does not match field {field.shape}")
+        hb = tuple(H.shape[:-3])
+    else:
+        if tuple(H.shape[-2:]) != (ny, nx):
+            raise ValueError(f"propagator shape {tuple(H.shape)} does not match field {field.shape}")
+        hb = tuple(H.shape[:-2])
+    H = H.reshape(-1, ny, nx).contiguous()
+    return H, hb
+
+
+def kernel_propagate(field: Field, propagator, absorbing_boundary=None, absorbing_boundary_width: float = 0.65,
+                     output_dx=None, output_shape=None, shift_yx=(0.0, 0.0), use_czt: bool = False,
+                     *, precision=None) -> Field:
+    """``ifft2(fft2(u) * propagator)`` (functional/propagation.py:355-394, FFT branch)."""
+    _check_boundary(absorbing_boundary)
+    if output_dx is not None or output_shape is not None or use_czt:
+        raise NotImplementedError("kernel_propagate with an explicit propagator supports the FFT branch only; "
+                                  "use asm_propagate/transfer_propagate with output_dx/output_shape")
+    H, hb = _planar_propagator(field, propagator)
+    W = field.n_wv
+    B = field.batch_shape
+    out_batch = np.broadcast_shapes(B, hb)
+    nb_out = int(np.prod(out_batch)) if out_batch else 1
+    nh = int(np.prod(hb)) if hb else 1
+    hidx = np.broadcast_to(np.arange(nh).reshape(hb if hb else ()), out_batch).reshape(-1)
+    h_index = np.repeat(hidx * W, W) + np.tile(np.arange(W), nb_out)
+    # reuse the batch-broadcast plane planner with a pseudo z batch of hb
+    zs = np.zeros(max(nh, 1))
+    zshape = hb
+    u = _run_prop2d(field, nat.CX_KERNEL_EXPLICIT, zs, zshape, 1.0, 0, mode="full", H=H, h_index=h_index,
+                    precision=precision)
+    return shift_grid(field.replace(u=u), shift_yx)
+
+
+def _fill_propagator(field: Field, kernel: int, z, n, kykx, shift_yx=(0.0, 0.0), bandlimit=False,
+                     remove_evanescent=False, precision=None, zshape_rule="asm"):
+    torch = nat.torch_mod()
+    prec = precision or config.get_precision()
+    zs, zshape = _z_array(z)
+    ny, nx = field.spatial_shape
+    W = field.n_wv
+    # one plane per (z, wv): the propagator does not depend on the field batch
+    planes, out_batch, _, nb_out = _plan_planes(field, zs, zshape, ny, nx, shift_yx, bandlimit, prec,
+                                                batch_shape=())
+    d = nat.cx_prop2d_desc()
+    d.ny, d.nx, d.pad_y, d.pad_x = ny, nx, 0, 0
+    d.n_wv = W
+    d.n_in_planes = W
+    d.n_out_planes = nb_out * W
+    d.kernel = kernel
+    d.precision = config.precision_code(prec)
+    d.remove_evanescent = int(bool(remove_evanescent))
+    d.bandlimit = int(bool(bandlimit))
+    d.n_medium = float(n)
+    ky0, kx0 = np.asarray(kykx, dtype=np.float64).reshape(2)
+    d.ky0, d.kx0 = float(ky0), float(kx0)
+    H = torch.empty((nb_out * W, ny, nx), dtype=torch.complex64, device=field.device)
+    planes_dev = nat.to_device_bytes(planes, field.device)
+    nat.check(nat.lib().cx_fill_propagator(d, nat.ptr(planes_dev), nat.ptr(H), nat.stream_handle(field.device)))
+    H = H.reshape(tuple(out_batch) + (W, ny, nx))
+    if field.chromatic:
+        return H.movedim(-3, -1).contiguous()
+    return H.reshape(tuple(out_batch) + (ny, nx))
+
+
+def compute_transfer_propagator(field: Field, z, n, kykx=(0.0, 0.0), *, precision=None):
+    """Fresnel transfer kernel, ifftshifted (functional/propagation.py:466-496)."""
+    return _fill_propagator(field, nat.CX_KERNEL_TRANSFER, z, n, kykx, precision=precision)
+
+
+def compute_asm_propagator(field: Field, z, n, kykx=(0.0, 0.0), bandlimit: bool = False, shift_yx=(0.0, 0.0),
+                           remove_evanescent: bool = False, *, precision=None):
+    """Angular-spectrum kernel, ifftshifted (functional/propagation.py:499-580)."""
+    return _fill_propagator(field, nat.CX_KERNEL_ASM, z, n, kykx, shift_yx, bandlimit, remove_evanescent,
+                            precision=precision)
+
+
+def compute_padding_transform(height: int, wavelength: float, dx: float, z: float) -> int:
+    """functional/propagation.py:583-605."""
+    D = height * dx
+    Nf = np.max((D / 2) ** 2 / (wavelength * z))
+    M = height
+    Q = 2 * np.maximum(1.0, M / (4 * Nf))
+    N = (np.ceil((Q * M) / 2) * 2).astype(int)
+    return int(N - M)
+
+
+compute_padding_transfer = compute_padding_transform  # functional/propagation.py:608-630 (same rule)
+
+
+def compute_padding_exact(height: int, wavelength: float, dx: float, z: float) -> int:
+    """functional/propagation.py:633-656."""
+    D = height * dx
+    Nf = np.max((D / 2) ** 2 / (wavelength * z))
+    M = height
+    Q = 2 * np.maximum(1.0, M / (4 * Nf))
+    scale = np.max((wavelength / (2 * dx)))
+    Q = Q / np.sqrt(1 - scale**2)
+    N = (np.ceil((Q * M) / 2) * 2).astype(int)
+    return int(N - M)
+
+
+def transform_propagate(field: Field, z, n, pad_width, cval: float = 0, skip_initial_phase: bool = False,
+                        skip_final_phase: bool = False, *, precision=None) -> Field:
+    """Single-FFT Fresnel propagation (functional/propagation.py:34-82)."""
+    from .convenience import _optical_fft_chirped
+
+    return _optical_fft_chirped(field, z, n, pad_width, cval, skip_initial_phase, skip_final_phase,
+                                precision=precision)
+
+
+def transform_propagate_sas(field: Field, z, n, cval: float = 0, skip_initial_phase: bool = False,
+                            skip_final_phase: bool = False, *, precision=None) -> Field:
+    """Scalable angular spectrum (functional/propagation.py:106-165)."""
+    raise NotImplementedError("transform_propagate_sas is not part of this build yet")

@@ -1,0 +1,206 @@
+/*
+ * cx_b200.h -- C ABI of the B200-native Chromatix propagation kernels.
+ *
+ * The reference (chromatix 0.5.0) is pure Python/JAX and has no native
+ * interface; these entry points are what a jax.ffi / XLA FFI custom call for
+ * each hot-path function binds.  Each declaration names the reference
+ * function it replaces (paths relative to the chromatix repository root).
+ *
+ * Conventions
+ *  - All field buffers are complex64 (interleaved float re, im), device
+ *    memory owned by the caller, laid out like the reference's Field.u:
+ *    (batch..., y, x) for a monochromatic field, (batch..., y, x, wv) for a
+ *    chromatic one (wv innermost, stride n_wv).
+ *  - Per-plane parameters (z, wavelength, spacing, ...) are an array of
+ *    cx_plane in DEVICE memory, one entry per output (batch, wavelength)
+ *    plane, so the same launch can be replayed from a CUDA graph with new
+ *    values.
+ *  - Scratch space is a caller-provided workspace of the size reported by
+ *    the matching *_workspace_size call.  No entry point allocates device
+ *    memory, synchronises the stream, or traps: errors come back as a
+ *    cx_status and a thread-local message (cx_last_error).
+ *  - Every call is asynchronous on the given stream.
+ */
+#ifndef CX_B200_H
+#define CX_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef void* cx_stream_t; /* a cudaStream_t */
+
+typedef enum {
+  CX_OK = 0,
+  CX_ERR_INVALID = 1,     /* bad argument (shape, pointer, parameter) */
+  CX_ERR_UNSUPPORTED = 2, /* size/feature not compiled in */
+  CX_ERR_CUDA = 3,        /* a CUDA runtime call failed */
+  CX_ERR_WORKSPACE = 4,   /* workspace too small */
+  CX_ERR_NOT_CONVERGED = 5
+} cx_status;
+
+typedef enum {
+  CX_PREC_ACCURATE = 0, /* FP64 phase arguments reduced mod 2pi, FP32 FFT */
+  CX_PREC_REF32 = 1     /* FP32 in the reference's operation order */
+} cx_precision;
+
+typedef enum {
+  CX_KERNEL_TRANSFER = 0, /* Fresnel transfer function (propagation.py:466-496) */
+  CX_KERNEL_ASM = 1,      /* angular spectrum (propagation.py:499-580) */
+  CX_KERNEL_EXPLICIT = 2  /* caller-supplied propagator array (propagation.py:355-393) */
+} cx_kernel_kind;
+
+/* One output plane of a batched propagation. */
+typedef struct {
+  double z;          /* propagation distance */
+  double wavelength; /* vacuum wavelength */
+  double dy, dx;     /* sample spacing of the padded input grid */
+  double shift_y, shift_x;   /* ASM output-plane shift (propagation.py:551) */
+  double bl_y0, bl_x0;       /* band-limit rectangle centre (propagation.py:566) */
+  double bl_hy, bl_hx;       /* band-limit rectangle half width (propagation.py:574) */
+  int32_t in_plane;  /* input plane (batch * n_wv + wv) this output reads */
+  int32_t h_plane;   /* plane of the explicit propagator array (CX_KERNEL_EXPLICIT) */
+} cx_plane;
+
+/* Fourier-multiplier propagation: pad -> FFT2 -> x H -> IFFT2 -> crop. */
+typedef struct {
+  int32_t ny, nx;          /* input spatial shape */
+  int32_t pad_y, pad_x;    /* zero padding on each side */
+  int32_t n_wv;            /* interleaved wavelengths (1: monochromatic layout) */
+  int32_t n_in_planes;     /* input batch * n_wv */
+  int32_t n_out_planes;    /* output batch * n_wv (entries in the cx_plane array) */
+  int32_t mode_same;       /* 1: crop the output back to ny x nx */
+  int32_t kernel;          /* cx_kernel_kind */
+  int32_t precision;       /* cx_precision */
+  int32_t remove_evanescent;
+  int32_t bandlimit;
+  double n_medium;
+  double ky0, kx0;         /* kykx tilt subtracted from the frequency grid */
+} cx_prop2d_desc;
+
+/* Workspace bytes for cx_prop2d. */
+cx_status cx_prop2d_workspace_size(const cx_prop2d_desc* d, size_t* bytes);
+
+/* transfer_propagate / asm_propagate / kernel_propagate (FFT branch)
+ * (functional/propagation.py:168-252, 255-352, 355-394).
+ * u_out: (n_out_planes/n_wv, oy, ox, n_wv) with (oy, ox) = (ny, nx) when
+ * mode_same else (ny + 2 pad_y, nx + 2 pad_x).  H (CX_KERNEL_EXPLICIT only):
+ * planar (h_planes, py, px) complex64 in FFT (ifftshifted) order. */
+cx_status cx_prop2d(const cx_prop2d_desc* d, const cx_plane* planes_dev, const void* u_in, void* u_out,
+                    const void* H, void* workspace, size_t workspace_bytes, cx_stream_t stream);
+
+/* compute_transfer_propagator / compute_asm_propagator
+ * (functional/propagation.py:466-496, 499-580): writes the ifftshifted
+ * propagator, planar (n_out_planes, py, px) complex64, py/px = padded size. */
+cx_status cx_fill_propagator(const cx_prop2d_desc* d, const cx_plane* planes_dev, void* H_out,
+                             cx_stream_t stream);
+
+/* ---------------------------------------------------------------------------
+ * Batched 4f widefield PSF:
+ *   objective_point_source (functional/sources.py:122-209)
+ *   -> phase_change (functional/phase_masks.py:29-68)
+ *   -> ff_lens (functional/lenses.py:64-95 via convenience.py:9-59)
+ *   -> Field.intensity (core/field.py:735-740)
+ * fused: the source, pupil, power normalisation, phase mask and lens
+ * normalisation are evaluated inside the FFT loader; the fftshifts are index
+ * remaps; the spectral sum of |u|^2 is the FFT epilogue.
+ * ------------------------------------------------------------------------- */
+typedef struct {
+  int32_t ny, nx;        /* grid */
+  int32_t n_z;           /* defocus planes */
+  int32_t n_wv;          /* wavelengths */
+  int32_t precision;     /* cx_precision */
+  int32_t has_phase;     /* phase mask present */
+  int32_t spectrally_modulate;
+  int32_t normalize_power; /* objective_point_source(power=...) not None */
+  double f_obj, n_medium, NA, power;
+  double amplitude;      /* scalar source amplitude */
+  double offset_y, offset_x;
+  double f_lens;         /* ff_lens focal length (negative: inverse lens) */
+  double lens_NA;        /* ff_lens pupil NA, <= 0: none */
+} cx_psf_desc;
+
+/* Per-wavelength parameters of the PSF (host memory, n_wv entries each). */
+typedef struct {
+  const double* wavelength; /* n_wv */
+  const double* density;    /* n_wv, normalised spectral density */
+  const double* dy;         /* n_wv source spacing y */
+  const double* dx;         /* n_wv source spacing x */
+} cx_psf_spectrum;
+
+cx_status cx_psf_workspace_size(const cx_psf_desc* d, size_t* bytes);
+
+/* z_dev: n_z defocus distances (device, double).  phase: (ny, nx) float32 or
+ * NULL.  intensity_out: (n_z, ny, nx) float32. */
+cx_status cx_psf_4f(const cx_psf_desc* d, const cx_psf_spectrum* spec, const double* z_dev, const float* phase,
+                    float* intensity_out, void* workspace, size_t workspace_bytes, cx_stream_t stream);
+
+/* objective_point_source [-> phase_change] materialised
+ * (functional/sources.py:122-209, functional/phase_masks.py:29-68):
+ * u_out (n_z, ny, nx, n_wv) complex64, power-normalised; f_lens / lens_NA are
+ * ignored.  workspace: >= 256 bytes. */
+cx_status cx_psf_source(const cx_psf_desc* d, const cx_psf_spectrum* spec, const double* z_dev, const float* phase,
+                        void* u_out, void* workspace, size_t workspace_bytes, cx_stream_t stream);
+
+/* ---------------------------------------------------------------------------
+ * Centred optical FFT with fused chirps
+ *   optical_fft        functional/convenience.py:9-59 (+ utils/fft.py:8-20)
+ *   ff_lens / df_lens  functional/lenses.py:64-95, 159-198
+ *   transform_propagate functional/propagation.py:34-82
+ * out = crop( post * chirp_out * C( FFT2_shifted( pre * C(pad(u) * chirp_in * pupil) ) ) )
+ * with C = complex conjugation when `conj` is set (the z < 0 branch of
+ * optical_fft), FFT2_shifted = fftshift(fft2(ifftshift(.))) done by index
+ * remapping, chirp_* = exp(i c |r|^2) on the input / output grid.
+ * ------------------------------------------------------------------------- */
+typedef struct {
+  double pre_re, pre_im;   /* complex factor on the (conjugated) input */
+  double post_re, post_im; /* complex factor on the (conjugated) output */
+  double chirp_in;         /* input phase coefficient c_in (0: none) */
+  double chirp_out;        /* output phase coefficient c_out (0: none) */
+  double dy_in, dx_in;     /* input grid spacing (padded grid) */
+  double dy_out, dx_out;   /* output grid spacing */
+  double oy, ox;           /* grid origin */
+  double pupil_r2;         /* circular input pupil radius^2 (< 0: none) */
+  int32_t in_plane;        /* input plane (batch * n_wv + wv) */
+  int32_t conj;            /* 1: conjugate input and output (inverse transform) */
+} cx_fft_plane;
+
+typedef struct {
+  int32_t ny, nx;          /* input spatial shape */
+  int32_t pad_y, pad_x;    /* zero padding on each side before the transform */
+  int32_t crop_y, crop_x;  /* crop on each side after the transform */
+  int32_t n_wv;            /* interleaved wavelengths of input and output */
+  int32_t n_in_planes, n_out_planes;
+  int32_t precision;       /* cx_precision */
+} cx_optfft_desc;
+
+cx_status cx_optfft_workspace_size(const cx_optfft_desc* d, size_t* bytes);
+/* planes_dev: n_out_planes cx_fft_plane in device memory.  u_out:
+ * (n_out_planes/n_wv, ny + 2 pad_y - 2 crop_y, nx + 2 pad_x - 2 crop_x, n_wv). */
+cx_status cx_optical_fft(const cx_optfft_desc* d, const cx_fft_plane* planes_dev, const void* u_in, void* u_out,
+                         void* workspace, size_t workspace_bytes, cx_stream_t stream);
+
+/* Field.intensity (core/field.py:656-665, 735-740): out[b, y, x] =
+ * sum_wv density[wv] |u[b, y, x, wv]|^2.  density_dev: n_wv doubles. */
+cx_status cx_intensity(const void* u, int64_t n_pix, int32_t n_wv, const double* density_dev, float* out,
+                       cx_stream_t stream);
+
+/* ---------------------------------------------------------------------------
+ * misc
+ * ------------------------------------------------------------------------- */
+const char* cx_last_error(void);
+int32_t cx_version(void);
+/* 1 if an FFT length is compiled in (fast path), else 0. */
+int32_t cx_fft_size_supported(int32_t n);
+/* Batched complex FFT along the last axis (test/utility entry):
+ * in/out (batch, n) complex64, inverse=1 applies exp(+i..) and 1/n. */
+cx_status cx_fft1d(const void* in, void* out, int32_t n, int64_t batch, int32_t inverse, cx_stream_t stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* CX_B200_H */

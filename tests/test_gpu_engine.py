@@ -1,0 +1,41 @@
+"""The FFT engine on the GPU vs numpy, for every compiled length (cx_fft1d)."""
+
+import numpy as np
+import pytest
+
+from tests.helpers import to_np
+
+SIZES = [2, 3, 4, 5, 6, 8, 10, 12, 16, 20, 24, 32, 40, 48, 64, 80, 96, 128, 160, 192, 256, 320, 384, 512, 640,
+         768, 1024, 1280, 1536, 2048, 2560, 3072, 4096]
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("n", SIZES)
+def test_fft1d_matches_numpy(n):
+    import torch
+
+    from chromatix_b200 import _native as nat
+
+    rng = np.random.default_rng(n)
+    batch = 37
+    x = (rng.standard_normal((batch, n)) + 1j * rng.standard_normal((batch, n))).astype(np.complex64)
+    xd = torch.as_tensor(x, device="cuda")
+    y = torch.empty_like(xd)
+    L = nat.lib()
+    for inv in (0, 1):
+        nat.check(L.cx_fft1d(nat.ptr(xd), nat.ptr(y), n, batch, inv, nat.stream_handle()))
+        torch.cuda.synchronize()
+        ref = np.fft.ifft(x.astype(np.complex128), axis=-1) if inv else np.fft.fft(x.astype(np.complex128), axis=-1)
+        err = np.linalg.norm(to_np(y) - ref) / np.linalg.norm(ref)
+        assert err < 2e-6, (n, inv, err)
+
+
+@pytest.mark.gpu
+def test_fft1d_unsupported_length_is_an_error():
+    import torch
+
+    from chromatix_b200 import _native as nat
+
+    x = torch.zeros(7 * 11, dtype=torch.complex64, device="cuda")
+    with pytest.raises(nat.CxError):
+        nat.check(nat.lib().cx_fft1d(nat.ptr(x), nat.ptr(x), 77, 1, 0, nat.stream_handle()))
