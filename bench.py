@@ -1,0 +1,413 @@
+"""Benchmark: batched 4f widefield PSF on B200 (one JSON line on rank 0).
+
+Workload (the configuration the headline metric is quoted on):
+  objective_point_source on a 1280 x 1280 grid, f_obj = 8 mm, f_tube = 200 mm,
+  NA = 0.6, n = 1.33, 64 defocus planes z ~ U[-5, 5] um x 3 wavelengths
+  {0.45, 0.532, 0.63} um with equal spectral density, phase mask ~ U[0, 2 pi)
+  float32, then ff_lens and the spectral intensity sum -> (64, 1280, 1280)
+  float32.  Spacing per wavelength f_tube * lambda / (n * 1280 * 6.5 um)
+  (a 6.5 um camera pitch).  Synthetic, seeded inputs.
+
+One "step" = one full PSF stack.  ``value`` counts propagated pixels
+(64 * 3 * 1280^2 per step) per second with inputs resident in HBM; ``e2e``
+is the same metric through the public API from pinned host buffers (phase
+mask and z in, intensity stack out, copies inside the timed region).
+
+Multi-GPU: the stacks are independent, so N GPUs run N replicas (weak
+scaling, no collective in the data path); timing is the max over ranks.
+
+``--impl reference`` times the CPU oracle (numpy/scipy float32 restatement of
+the reference's operation order, all host cores) on a bounded sample of the
+same workload.
+"""
+
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+NZ, NWV, N = 64, 3, 1280
+WAVELENGTHS = np.array([0.45, 0.532, 0.63])
+F_OBJ, F_TUBE, N_MED, NA, CAM = 8000.0, 200000.0, 1.33, 0.6, 6.5
+METRIC = "Mpx/s propagated vs plain FP32 @<=1e-5 rel err"
+UNIT = "Mpx/s"
+CONFIG = {
+    "workload": "batched 4f widefield PSF: objective_point_source 1280x1280, 64 z x 3 wavelengths, "
+                "phase mask, ff_lens, spectral intensity (complex64 fields, float32 output)",
+    "grid": [N, N], "n_z": NZ, "wavelengths_um": WAVELENGTHS.tolist(), "f_obj_um": F_OBJ, "f_tube_um": F_TUBE,
+    "NA": NA, "n": N_MED, "camera_pitch_um": CAM,
+}
+PX_PER_STEP = NZ * NWV * N * N
+
+
+def inputs(seed=0):
+    rng = np.random.default_rng(seed)
+    z = np.sort(rng.uniform(-5.0, 5.0, NZ))
+    phase = rng.uniform(0, 2 * np.pi, (N, N)).astype(np.float32)
+    dx = F_TUBE * WAVELENGTHS / (N_MED * N * CAM)
+    return z, phase, dx
+
+
+# ---------------------------------------------------------------------------
+# clocks
+# ---------------------------------------------------------------------------
+class ClockSampler:
+    """nvidia-smi sampling of SM clocks and throttle reasons during the timed region."""
+
+    FIELDS = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
+              "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+              "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), "--query-gpu=" + self.FIELDS,
+                                          "--format=csv,noheader,nounits", "-lms", "50"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except Exception:
+            self.proc = None
+        time.sleep(0.3)
+        return self
+
+    def __exit__(self, *a):
+        if self.proc is not None:
+            time.sleep(0.1)
+            self.proc.terminate()
+            try:
+                out, _ = self.proc.communicate(timeout=5)
+            except Exception:
+                self.proc.kill()
+                out = ""
+            self.lines = [ln for ln in (out or "").splitlines() if ln.strip()]
+
+    def summary(self):
+        samples = [[p.strip() for p in ln.split(",")] for ln in self.lines]
+        samples = [s for s in samples if len(s) >= 7]
+        if not samples:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+
+        def f(x):
+            try:
+                return float(x)
+            except ValueError:
+                return None
+
+        sm = [f(s[0]) for s in samples if f(s[0]) is not None]
+        mx = [f(s[1]) for s in samples if f(s[1]) is not None]
+        pw = [f(s[2]) for s in samples if f(s[2]) is not None]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for s in samples for i in range(4) if s[3 + i].lower() == "active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "power_w_max": max(pw) if pw else None, "reasons": reasons, "samples": len(samples)}
+
+
+# ---------------------------------------------------------------------------
+# GPU arm
+# ---------------------------------------------------------------------------
+def gpu_arm(args):
+    import torch
+
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120), device_id=dev)
+
+    import chromatix_b200 as cx
+    import chromatix_b200.functional as cf
+    from chromatix_b200 import _native as nat
+
+    z, phase, dx = inputs(seed=rank)
+    phase_d = torch.as_tensor(phase, device=dev)
+    spec = (WAVELENGTHS, np.ones(NWV))
+
+    def step_device():
+        f = cf.objective_point_source((N, N), dx, spec, z, F_OBJ, N_MED, NA, device=dev)
+        f = cf.phase_change(f, phase_d)
+        f = cf.ff_lens(f, F_TUBE, N_MED)
+        return f.intensity
+
+    # pinned host buffers for the end-to-end arm
+    phase_h = torch.from_numpy(phase).pin_memory()
+    z_h = torch.from_numpy(z.copy()).pin_memory()
+    out_h = torch.empty((NZ, N, N), dtype=torch.float32).pin_memory()
+
+    def step_e2e():
+        ph = phase_h.to(dev, non_blocking=True)
+        zz = z_h.to(dev, non_blocking=True)
+        f = cf.objective_point_source((N, N), dx, spec, zz, F_OBJ, N_MED, NA, device=dev)
+        f = cf.ff_lens(cf.phase_change(f, ph), F_TUBE, N_MED)
+        out_h.copy_(f.intensity, non_blocking=True)
+        return out_h
+
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)  # > 126 MB L2
+
+    def timed(fn, steps, warmup):
+        for _ in range(warmup):
+            fn()
+        torch.cuda.synchronize(dev)
+        if dist:
+            dist.barrier()
+        st = torch.cuda.current_stream(dev)
+        total = 0.0
+        for _ in range(steps):
+            flush.fill_(1.0)  # evict L2 between steps (outside the timed events)
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(st)
+            fn()
+            e1.record(st)
+            e1.synchronize()
+            total += e0.elapsed_time(e1)
+        torch.cuda.synchronize(dev)
+        if dist:
+            dist.barrier()
+        return total / steps  # ms per step (this rank)
+
+    with ClockSampler(local) as clk:
+        ms = timed(step_device, args.steps, args.warmup)
+    ms_e2e = timed(step_e2e, max(2, args.steps // 2), 2)
+
+    # dominant kernel (column pass) launch time, measured live with CUDA events
+    # on the launching stream: one chunk of the same workload
+    kern = dominant_kernel_time(dev, z, phase_d, dx)
+
+    if dist:
+        t = torch.tensor([ms, ms_e2e], device=dev, dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms, ms_e2e = float(t[0]), float(t[1])
+    value = PX_PER_STEP * world / (ms * 1e-3) / 1e6
+    e2e_value = PX_PER_STEP * world / (ms_e2e * 1e-3) / 1e6
+
+    if rank == 0:
+        import json as _json
+
+        peaks = {}
+        try:
+            peaks = _json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+        except Exception:
+            pass
+        hbm = float(peaks.get("hbm_gbs", 6650.0))
+        peak_src = "measured" if "hbm_gbs" in peaks else "fallback"
+        # algorithmic bytes of one column-pass launch: its share of the compulsory
+        # outputs (intensity of the chunk's z planes); the phase mask read is
+        # attributed to the row pass
+        alg_bytes = kern["zc"] * N * N * 4
+        achieved = alg_bytes / (kern["ms"] * 1e-3) / 1e9
+        traffic = None
+        tp = os.path.join(ROOT, "profiles", "psf_cols_1280.traffic.json")
+        if os.path.exists(tp):
+            try:
+                tj = _json.load(open(tp))
+                traffic = tj["dram_bytes_per_z"] * kern["zc"]
+            except Exception:
+                traffic = None
+        # FP32 work of the pipeline (5 N log2 N per complex FFT of N points)
+        rows_ffts = NZ * kern["rowsum"]
+        cols_ffts = NZ * NWV * N
+        flops = 5 * N * np.log2(N) * (rows_ffts + cols_ffts)
+        gpu_launches = kern["launches_per_step"] * args.steps
+        line = {
+            "metric": METRIC, "value": round(value, 1), "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": round(ms, 4), "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "c64/f32 (FP64 phase arguments)", "data": "synthetic (seeded)",
+            "config": dict(CONFIG, l2="flushed between timed steps (256 MB write)",
+                           parallelism=f"replicas x{world}" if world > 1 else "single GPU"),
+            "e2e": {"value": round(e2e_value, 1), "unit": UNIT, "ms_per_step": round(ms_e2e, 4),
+                    "h2d_bytes_per_step": int(phase.nbytes + z.nbytes),
+                    "d2h_bytes_per_step": int(NZ * N * N * 4)},
+            "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": hbm, "unit": "GB/s",
+                         "frac": round(achieved / hbm, 4), "traffic": traffic,
+                         "kernel": "k_psf_cols<1280> (column FFT + spectral intensity)",
+                         "kernel_ms": round(kern["ms"], 5), "peak_source": peak_src},
+            "compute": {"fp32_fft_gflop_per_step": round(flops / 1e9, 2),
+                        "achieved_tflops": round(flops / (ms * 1e-3) / 1e12, 2)},
+            "gpu_launches": gpu_launches,
+            "clocks": clk.summary(),
+        }
+        if not args.no_cpu_baseline and world == 1:
+            line["cpu_baseline"] = cpu_baseline(args.cpu_sample_z)
+        if args.accuracy:
+            line["rel_err_vs_fp64"] = accuracy_check(dev)
+        print(json.dumps(line), flush=True)
+    if dist:
+        dist.destroy_process_group()
+
+
+def dominant_kernel_time(dev, z, phase_d, dx):
+    """Average duration of the column-pass launch, CUDA events on the stream
+    the library launches on (a launch sequence of one chunk)."""
+    import torch
+
+    import chromatix_b200.functional as cf
+
+    # time a full step's sequence and the row-pass-only sequence of the same
+    # chunking through the C ABI, by running the one-chunk workload
+    from chromatix_b200 import _native as nat
+
+    f = cf.ff_lens(cf.phase_change(cf.objective_point_source((N, N), dx, (WAVELENGTHS, np.ones(NWV)), z,
+                                                             F_OBJ, N_MED, NA, device=dev), phase_d), F_TUBE, N_MED)
+    d = f._desc()
+    spec, keep = f._spec()
+    L = nat.lib()
+    info = (nat.c_int32 * 4)()
+    L.cx_psf_plan_info.restype = nat.c_int32
+    L.cx_psf_plan_info.argtypes = [nat.ctypes.POINTER(nat.cx_psf_desc), nat.ctypes.POINTER(nat.cx_psf_spectrum),
+                                   nat.ctypes.POINTER(nat.c_int32)]
+    nat.check(L.cx_psf_plan_info(d, spec, info))
+    zc, rowsum, nchunks = int(info[0]), int(info[1]), int(info[2])
+    ws_b = nat.c_size_t(0)
+    nat.check(L.cx_psf_workspace_size(d, ws_b))
+    ws = nat.workspace(ws_b.value, dev)
+    zd = torch.as_tensor(z, device=dev)
+    out = torch.empty((NZ, N, N), dtype=torch.float32, device=dev)
+    L.cx_psf_4f_stage.restype = nat.c_int32
+    L.cx_psf_4f_stage.argtypes = [nat.ctypes.POINTER(nat.cx_psf_desc), nat.ctypes.POINTER(nat.cx_psf_spectrum),
+                                  nat.c_void_p, nat.c_void_p, nat.c_void_p, nat.c_void_p, nat.c_size_t,
+                                  nat.c_int32, nat.c_int32, nat.c_void_p]
+    st = torch.cuda.current_stream(dev)
+    sh = st.cuda_stream
+    # prepare counters once (stage -1), then time column-pass launches of chunk 0
+    nat.check(L.cx_psf_4f_stage(d, spec, nat.ptr(zd), nat.ptr(phase_d), nat.ptr(out), nat.ptr(ws), ws_b.value, -1,
+                                0, sh))
+    nat.check(L.cx_psf_4f_stage(d, spec, nat.ptr(zd), nat.ptr(phase_d), nat.ptr(out), nat.ptr(ws), ws_b.value, 0, 0,
+                                sh))
+    reps = 20
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    for _ in range(3):
+        nat.check(L.cx_psf_4f_stage(d, spec, nat.ptr(zd), nat.ptr(phase_d), nat.ptr(out), nat.ptr(ws), ws_b.value,
+                                    1, 0, sh))
+    e0.record(st)
+    for _ in range(reps):
+        nat.check(L.cx_psf_4f_stage(d, spec, nat.ptr(zd), nat.ptr(phase_d), nat.ptr(out), nat.ptr(ws), ws_b.value,
+                                    1, 0, sh))
+    e1.record(st)
+    e1.synchronize()
+    del keep
+    return {"ms": e0.elapsed_time(e1) / reps, "zc": zc, "rowsum": rowsum, "launches_per_step": 1 + 2 * nchunks}
+
+
+def accuracy_check(dev):
+    """Relative L2 error of the CUDA PSF vs the FP64 oracle on 2 defocus planes."""
+    import torch
+
+    import chromatix_b200.functional as cf
+    from oracle import chromatix_oracle as O
+
+    z, phase, dx = inputs(seed=0)
+    zz = z[[0, NZ - 1]]
+    spec = (WAVELENGTHS, np.ones(NWV))
+    f = cf.ff_lens(cf.phase_change(cf.objective_point_source((N, N), dx, spec, zz, F_OBJ, N_MED, NA, device=dev),
+                                   torch.as_tensor(phase, device=dev)), F_TUBE, N_MED)
+    I = f.intensity.cpu().numpy()
+    O.set_fft_workers(os.cpu_count())
+    o = O.ff_lens(O.phase_change(O.objective_point_source((N, N), dx, spec, zz, F_OBJ, N_MED, NA), phase),
+                  F_TUBE, N_MED)
+    return float(O.rel_l2(I, o.intensity))
+
+
+# ---------------------------------------------------------------------------
+# CPU baseline / reference arm: the oracle (float32 reference order)
+# ---------------------------------------------------------------------------
+def cpu_baseline(n_z_sample: int = 2):
+    from oracle import chromatix_oracle as O
+
+    cores = os.cpu_count() or 1
+    O.set_fft_workers(cores)
+    z, phase, dx = inputs(seed=0)
+    zz = z[:n_z_sample]
+    spec = (WAVELENGTHS, np.ones(NWV))
+    t0 = time.perf_counter()
+    f = O.objective_point_source((N, N), dx, spec, zz, F_OBJ, N_MED, NA, prec=O.REF32)
+    f = O.ff_lens(O.phase_change(f, phase), F_TUBE, N_MED)
+    _ = f.intensity
+    dt = time.perf_counter() - t0
+    px = n_z_sample * NWV * N * N
+    return {"value": round(px / dt / 1e6, 2), "unit": UNIT, "cores": cores, "kind": "port",
+            "sample": f"{n_z_sample} of {NZ} defocus planes x 3 wavelengths at 1280^2 (numpy/scipy float32 "
+                      f"restatement, scipy.fft workers={cores}), {dt:.2f} s"}
+
+
+def reference_arm(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    from oracle import chromatix_oracle as O
+
+    cores = os.cpu_count() or 1
+    O.set_fft_workers(cores)
+    z, phase, dx = inputs(seed=0)
+    spec = (WAVELENGTHS, np.ones(NWV))
+    nzs = args.cpu_sample_z
+
+    def step():
+        f = O.objective_point_source((N, N), dx, spec, z[:nzs], F_OBJ, N_MED, NA, prec=O.REF32)
+        return O.ff_lens(O.phase_change(f, phase), F_TUBE, N_MED).intensity
+
+    for _ in range(args.warmup if args.warmup < 2 else 1):
+        step()
+    ts = []
+    for _ in range(args.steps):
+        t0 = time.perf_counter()
+        step()
+        ts.append(time.perf_counter() - t0)
+    dt = float(np.mean(ts))
+    px = nzs * NWV * N * N
+    value = px / dt / 1e6
+    line = {
+        "metric": METRIC, "value": round(value, 2), "unit": UNIT, "n_gpus": int(os.environ.get("WORLD_SIZE", "1")),
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(dt * 1e3, 2), "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "c64/f32", "data": "synthetic (seeded)",
+        "config": dict(CONFIG, note=f"each step is a bounded sample: {nzs} of {NZ} defocus planes"),
+        "impl": "reference",
+        "cpu_baseline": {"value": round(value, 2), "unit": UNIT, "cores": cores, "kind": "port",
+                         "sample": f"{nzs} of {NZ} defocus planes x 3 wavelengths at 1280^2 per step "
+                                   "(numpy/scipy float32 restatement of the reference; jax is not installed)"},
+        "e2e": {"value": round(value, 2), "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=100)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--cpu-sample-z", type=int, default=2)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--accuracy", action="store_true", help="also report the error vs the FP64 oracle")
+    args = ap.parse_args()
+    if args.warmup < 3 and args.impl == "ours":
+        args.warmup = 3
+    if args.impl == "reference":
+        reference_arm(args)
+    else:
+        gpu_arm(args)
+
+
+if __name__ == "__main__":
+    main()

@@ -205,9 +205,13 @@ extern "C" cx_status cx_psf_workspace_size(const cx_psf_desc* d, size_t* bytes) 
   return CX_OK;
 }
 
-extern "C" cx_status cx_psf_4f(const cx_psf_desc* d, const cx_psf_spectrum* spec, const double* z_dev,
-                               const float* phase, float* intensity_out, void* workspace, size_t workspace_bytes,
-                               cx_stream_t stream) {
+namespace cx {
+
+// shared set-up of cx_psf_4f / cx_psf_4f_stage: arguments, compact-row
+// geometry and the z-chunk size
+static cx_status psf_setup(const cx_psf_desc* d, const cx_psf_spectrum* spec, const double* z_dev, const float* phase,
+                           float* intensity_out, void* workspace, size_t workspace_bytes, PsfArgs* out_args,
+                           int* zc_out) {
   cx_status s = psf_check(d);
   if (s != CX_OK) return s;
   if (!spec || !spec->wavelength || !spec->density || !spec->dy || !spec->dx || !z_dev || !intensity_out ||
@@ -219,19 +223,13 @@ extern "C" cx_status cx_psf_4f(const cx_psf_desc* d, const cx_psf_spectrum* spec
     set_error("workspace too small: %zu < %zu", workspace_bytes, psf_ws(d));
     return CX_ERR_WORKSPACE;
   }
-  cudaStream_t st = static_cast<cudaStream_t>(stream);
   PsfArgs a = psf_make_args(d, spec, /*with_lens=*/true);
   a.z = z_dev;
   a.phase = phase;
   a.out = intensity_out;
-  unsigned long long* counts = static_cast<unsigned long long*>(workspace);
-  int* srange = reinterpret_cast<int*>(static_cast<char*>(workspace) + 64);
-  a.counts = counts;
-  a.srange = srange;
+  a.counts = static_cast<unsigned long long*>(workspace);
+  a.srange = reinterpret_cast<int*>(static_cast<char*>(workspace) + 64);
   a.T = reinterpret_cast<float2*>(static_cast<char*>(workspace) + 256);
-  CX_CUDA_TRY(cudaMemsetAsync(workspace, 0, 256, st));
-  k_psf_count<<<(a.W * a.ny + 127) / 128, 128, 0, st>>>(a, counts, srange);
-  CX_LAUNCH_CHECK();
   a.rowsum = 0;
   for (int w = 0; w < a.W; ++w) {
     psf_rows(d, spec, w, &a.ylo[w], &a.nrows[w]);
@@ -243,6 +241,32 @@ extern "C" cx_status cx_psf_4f(const cx_psf_desc* d, const cx_psf_spectrum* spec
   int zc = (int)((psf_ws(d) - 256) / zbytes);
   if (zc < 1) zc = 1;
   if (zc > a.nz) zc = a.nz;
+  *out_args = a;
+  *zc_out = zc;
+  return CX_OK;
+}
+
+static cx_status psf_prepare(const PsfArgs& a, void* workspace, cudaStream_t st) {
+  CX_CUDA_TRY(cudaMemsetAsync(workspace, 0, 256, st));
+  k_psf_count<<<(a.W * a.ny + 127) / 128, 128, 0, st>>>(a, const_cast<unsigned long long*>(a.counts),
+                                                         const_cast<int*>(a.srange));
+  CX_LAUNCH_CHECK();
+  return CX_OK;
+}
+
+}  // namespace cx
+
+using namespace cx;
+
+extern "C" cx_status cx_psf_4f(const cx_psf_desc* d, const cx_psf_spectrum* spec, const double* z_dev,
+                               const float* phase, float* intensity_out, void* workspace, size_t workspace_bytes,
+                               cx_stream_t stream) {
+  PsfArgs a;
+  int zc = 1;
+  cx_status s = psf_setup(d, spec, z_dev, phase, intensity_out, workspace, workspace_bytes, &a, &zc);
+  if (s != CX_OK) return s;
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  if ((s = psf_prepare(a, workspace, st)) != CX_OK) return s;
   for (int z0 = 0; z0 < a.nz; z0 += zc) {
     a.z0 = z0;
     a.zc = (a.nz - z0) < zc ? (a.nz - z0) : zc;
@@ -250,6 +274,45 @@ extern "C" cx_status cx_psf_4f(const cx_psf_desc* d, const cx_psf_spectrum* spec
     if ((s = psf_dispatch_cols(a.ny, a, st)) != CX_OK) return s;
   }
   return CX_OK;
+}
+
+extern "C" cx_status cx_psf_plan_info(const cx_psf_desc* d, const cx_psf_spectrum* spec, int32_t* info) {
+  if (!info) return CX_ERR_INVALID;
+  cx_status s = psf_check(d);
+  if (s != CX_OK) return s;
+  int rowsum = 0;
+  for (int w = 0; w < d->n_wv; ++w) {
+    int lo, nr;
+    psf_rows(d, spec, w, &lo, &nr);
+    rowsum += nr;
+  }
+  const size_t zbytes = sizeof(float2) * (size_t)rowsum * d->nx;
+  int zc = (int)((psf_ws(d) - 256) / zbytes);
+  if (zc < 1) zc = 1;
+  if (zc > d->n_z) zc = d->n_z;
+  info[0] = zc;
+  info[1] = rowsum;
+  info[2] = (d->n_z + zc - 1) / zc;
+  info[3] = 0;
+  return CX_OK;
+}
+
+extern "C" cx_status cx_psf_4f_stage(const cx_psf_desc* d, const cx_psf_spectrum* spec, const double* z_dev,
+                                     const float* phase, float* intensity_out, void* workspace,
+                                     size_t workspace_bytes, int32_t stage, int32_t chunk, cx_stream_t stream) {
+  PsfArgs a;
+  int zc = 1;
+  cx_status s = psf_setup(d, spec, z_dev, phase, intensity_out, workspace, workspace_bytes, &a, &zc);
+  if (s != CX_OK) return s;
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  if (stage < 0) return psf_prepare(a, workspace, st);
+  a.z0 = chunk * zc;
+  if (a.z0 < 0 || a.z0 >= a.nz) {
+    set_error("chunk %d out of range", chunk);
+    return CX_ERR_INVALID;
+  }
+  a.zc = (a.nz - a.z0) < zc ? (a.nz - a.z0) : zc;
+  return stage == 0 ? psf_dispatch_rows(a.nx, a, st) : psf_dispatch_cols(a.ny, a, st);
 }
 
 extern "C" cx_status cx_psf_source(const cx_psf_desc* d, const cx_psf_spectrum* spec, const double* z_dev,

@@ -55,7 +55,7 @@ class LazySourceField(Field):
     @property
     def shape(self):
         r = self._recipe
-        zb = (r["z"].size,) if r["zbatch"] else ()
+        zb = (r["nz"],) if r["zbatch"] else ()
         return zb + tuple(r["shape"]) + ((self.spectrum.size,) if self.chromatic else ())
 
     @property
@@ -103,7 +103,7 @@ class LazySourceField(Field):
         d = nat.cx_psf_desc()
         ny, nx = r["shape"]
         d.ny, d.nx = ny, nx
-        d.n_z = int(r["z"].size)
+        d.n_z = int(r["nz"])
         d.n_wv = self.spectrum.size
         d.precision = config.precision_code(r["precision"])
         d.has_phase = 1 if r.get("phase") is not None else 0
@@ -137,7 +137,10 @@ class LazySourceField(Field):
 
     def _z_dev(self):
         torch = nat.torch_mod()
-        return torch.as_tensor(np.ascontiguousarray(self._recipe["z"], dtype=np.float64), device=self._device)
+        r = self._recipe
+        if r.get("z_dev") is not None:
+            return r["z_dev"]
+        return torch.as_tensor(np.ascontiguousarray(r["z"], dtype=np.float64), device=self._device)
 
     def _source_field(self) -> Field:
         """Materialise the source (+ phase) stage."""
@@ -148,7 +151,7 @@ class LazySourceField(Field):
         spec, keep = self._spec()
         ny, nx = r["shape"]
         W = self.spectrum.size
-        u = torch.empty((int(r["z"].size), ny, nx, W), dtype=torch.complex64, device=self._device)
+        u = torch.empty((int(r["nz"]), ny, nx, W), dtype=torch.complex64, device=self._device)
         ws = nat.workspace(256, self._device)
         zd = self._z_dev()
         ph = r.get("phase")
@@ -185,7 +188,7 @@ class LazySourceField(Field):
         ws_b = nat.c_size_t(0)
         nat.check(L.cx_psf_workspace_size(d, ws_b))
         ny, nx = r["shape"]
-        out = torch.empty((int(r["z"].size), ny, nx), dtype=torch.float32, device=self._device)
+        out = torch.empty((int(r["nz"]), ny, nx), dtype=torch.float32, device=self._device)
         ws = nat.workspace(ws_b.value, self._device)
         zd = self._z_dev()
         ph = r.get("phase")
@@ -210,14 +213,23 @@ def objective_point_source(shape, dx, spectrum, z, f, n, NA, power=1.0, amplitud
     ``2 f NA / n`` and power normalisation.  Evaluated lazily (see module doc)."""
     if not scalar:
         raise NotImplementedError("vectorial fields are not part of this build")
+    torch = nat.torch_mod()
     spec = Spectrum.build(spectrum)
     amp = np.asarray(amplitude, dtype=np.float64)
     if amp.size != 1:
         raise AssertionError("scalar fields take a scalar amplitude")
-    z = np.squeeze(np.atleast_1d(np.asarray(z, dtype=np.float64)))
-    zbatch = z.size > 1
+    z_dev = None
+    if isinstance(z, torch.Tensor):
+        # device-resident z (e.g. a traced/batched argument): read in place
+        z_dev = z.detach().reshape(-1).to(device=device, dtype=torch.float64).contiguous()
+        nz = int(z_dev.numel())
+        z = None
+    else:
+        z = np.atleast_1d(np.squeeze(np.atleast_1d(np.asarray(z, dtype=np.float64))))
+        nz = int(z.size)
+    zbatch = nz > 1
     chromatic = not isinstance(spec, MonoSpectrum)
-    recipe = dict(shape=(int(shape[0]), int(shape[1])), z=np.atleast_1d(z).astype(np.float64), zbatch=zbatch,
+    recipe = dict(shape=(int(shape[0]), int(shape[1])), z=z, z_dev=z_dev, nz=nz, zbatch=zbatch,
                   f=float(f), n=float(n), NA=float(NA), power=None if power is None else float(power),
                   amplitude=float(amp.reshape(())), offset=tuple(float(o) for o in np.broadcast_to(offset, (2,))),
                   src_dx=np.asarray(dx, dtype=np.float64), phase=None, stage="source",

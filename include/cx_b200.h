@@ -138,6 +138,17 @@ cx_status cx_psf_workspace_size(const cx_psf_desc* d, size_t* bytes);
 cx_status cx_psf_4f(const cx_psf_desc* d, const cx_psf_spectrum* spec, const double* z_dev, const float* phase,
                     float* intensity_out, void* workspace, size_t workspace_bytes, cx_stream_t stream);
 
+/* Chunking of cx_psf_4f: info[0] = z planes per chunk, info[1] = stored rows
+ * per plane stack (pupil rows of all wavelengths), info[2] = number of chunks. */
+cx_status cx_psf_plan_info(const cx_psf_desc* d, const cx_psf_spectrum* spec, int32_t* info);
+
+/* One stage of cx_psf_4f, for measuring kernels in isolation: stage -1 =
+ * pupil counts (must run first), 0 = row pass of `chunk`, 1 = column pass of
+ * `chunk`.  Same arguments as cx_psf_4f. */
+cx_status cx_psf_4f_stage(const cx_psf_desc* d, const cx_psf_spectrum* spec, const double* z_dev, const float* phase,
+                          float* intensity_out, void* workspace, size_t workspace_bytes, int32_t stage,
+                          int32_t chunk, cx_stream_t stream);
+
 /* objective_point_source [-> phase_change] materialised
  * (functional/sources.py:122-209, functional/phase_masks.py:29-68):
  * u_out (n_z, ny, nx, n_wv) complex64, power-normalised; f_lens / lens_NA are
