@@ -1,5 +1,7 @@
 // C ABI plumbing: error strings, device info, batched 1D FFT, intensity.
+#include <map>
 #include <mutex>
+#include <utility>
 
 #include "host.cuh"
 
@@ -12,6 +14,13 @@ void set_error(const char* fmt, ...) {
   va_start(ap, fmt);
   vsnprintf(g_err, sizeof(g_err), fmt, ap);
   va_end(ap);
+}
+
+KernelFacts& kernel_facts_slot(const void* kernel, int device) {
+  static std::mutex mu;
+  static std::map<std::pair<const void*, int>, KernelFacts> reg;  // node-based: references stay valid
+  std::lock_guard<std::mutex> lock(mu);
+  return reg[std::make_pair(kernel, device)];
 }
 
 int sm_count() {
@@ -31,11 +40,11 @@ int sm_count() {
 // ---------------------------------------------------------------------------
 template <int N, bool INV>
 __global__ void __launch_bounds__(RowCfg<N>::THREADS, RowCfg<N>::MINB) k_fft1d(const float2* __restrict__ in, float2* __restrict__ out,
-                                                             long batch) {
+                                                             long batch, const float2* __restrict__ twg) {
   using C = RowCfg<N>;
   extern __shared__ float2 sm[];
   float2* tw = sm;
-  init_twiddles<N>(tw, threadIdx.x, blockDim.x);
+  load_twiddles<N>(tw, twg, threadIdx.x, blockDim.x);
   __syncthreads();
   const int team = threadIdx.x / C::LPV, lane = threadIdx.x % C::LPV;
   float2* s = sm + C::TW + team * Plan<N>::LEN;
@@ -54,17 +63,18 @@ __global__ void __launch_bounds__(RowCfg<N>::THREADS, RowCfg<N>::MINB) k_fft1d(c
 }
 
 template <int N>
-static cx_status launch_fft1d(const float2* in, float2* out, long batch, bool inv, cudaStream_t st) {
+static cx_status launch_fft1d(const float2* in, float2* out, long batch, bool inv, const float2* twg,
+                              cudaStream_t st) {
   using C = RowCfg<N>;
   const long items = (batch + C::TEAMS - 1) / C::TEAMS;
   if (inv) {
     auto k = k_fft1d<N, true>;
     CX_CUDA_TRY(set_smem(k, C::SMEM));
-    k<<<persistent_grid(k, C::THREADS, C::SMEM, items), C::THREADS, C::SMEM, st>>>(in, out, batch);
+    k<<<persistent_grid(k, C::THREADS, C::SMEM, items), C::THREADS, C::SMEM, st>>>(in, out, batch, twg);
   } else {
     auto k = k_fft1d<N, false>;
     CX_CUDA_TRY(set_smem(k, C::SMEM));
-    k<<<persistent_grid(k, C::THREADS, C::SMEM, items), C::THREADS, C::SMEM, st>>>(in, out, batch);
+    k<<<persistent_grid(k, C::THREADS, C::SMEM, items), C::THREADS, C::SMEM, st>>>(in, out, batch, twg);
   }
   CX_LAUNCH_CHECK();
   return CX_OK;
@@ -105,13 +115,16 @@ extern "C" cx_status cx_fft1d(const void* in, void* out, int32_t n, int64_t batc
     return CX_ERR_INVALID;
   }
   if (batch == 0) return CX_OK;
+  const float2* twg = nullptr;
+  cx_status s = ensure_twiddles(&twg);
+  if (s != CX_OK) return s;
   const float2* i = static_cast<const float2*>(in);
   float2* o = static_cast<float2*>(out);
   cudaStream_t st = static_cast<cudaStream_t>(stream);
   switch (n) {
 #define CX_CASE_(N) \
   case N:           \
-    return launch_fft1d<N>(i, o, batch, inverse != 0, st);
+    return launch_fft1d<N>(i, o, batch, inverse != 0, twg, st);
     CX_FOR_EACH_SIZE(CX_CASE_)
 #undef CX_CASE_
   }

@@ -314,13 +314,38 @@ __device__ __forceinline__ void team_sync(int team) {
 // table length: tw[m] = w^m for m < N, then tw[N + m] = w^(4m) for m < N/8
 __host__ __device__ constexpr int tw_len(int N) { return N + N / 8 + 1; }
 
+// exp(-2 pi i e / N), e in [0, N): for N divisible by 8 only the first octant
+// is evaluated (FP64 sincospi) and the rest follows by exact symmetries
+template <int N>
+__device__ __forceinline__ float2 twiddle_value(int e) {
+  if constexpr (N % 8 == 0) {
+    constexpr int Q = N / 4, O = N / 8;
+    const int q = e / Q, r = e - q * Q;  // e = q N/4 + r, 0 <= r < N/4
+    const bool hi = r > O;               // second octant of the quadrant: mirror
+    const int m = hi ? Q - r : r;        // 0 <= m <= N/8
+    double sd, cd;
+    sincospi(2.0 * (double)m / (double)N, &sd, &cd);
+    // angle t = 2 pi r / N ; (cos t, sin t)
+    float c = hi ? (float)sd : (float)cd;
+    float sn = hi ? (float)cd : (float)sd;
+    // rotate by q quarter turns: exp(i (t + q pi/2))
+    float cr = c, sr = sn;
+    if (q == 1) { cr = -sn; sr = c; }
+    if (q == 2) { cr = -c; sr = -sn; }
+    if (q == 3) { cr = sn; sr = -c; }
+    return make_float2(cr, -sr);  // exp(-i angle)
+  } else {
+    double sd, cd;
+    sincospi(-2.0 * (double)e / (double)N, &sd, &cd);
+    return make_float2((float)cd, (float)sd);
+  }
+}
+
 template <int N>
 __device__ __forceinline__ void init_twiddles(float2* tw, int tid, int nthreads) {
   for (int m = tid; m < tw_len(N); m += nthreads) {
     const int e = m < N ? m : (4 * (m - N)) % N;
-    double s, c;
-    sincospi(-2.0 * (double)e / (double)N, &s, &c);
-    tw[m] = make_float2((float)c, (float)s);
+    tw[m] = twiddle_value<N>(e);
   }
 }
 
@@ -457,6 +482,43 @@ struct Stage<N, LPV, INV, 16, NS> {
 template <int N, bool INV, class Load, class Store>
 __device__ __forceinline__ void team_fft(float2* s, const float2* tw, int lane, int team, Load& load, Store& store) {
   Stage<N, Plan<N>::LPV, INV, 0, 1>::run(s, tw, lane, team, load, store);
+}
+
+// Same transform with the load and/or store functor applied in a compact,
+// coalesced loop through the team's shared buffer (lane-strided indices)
+// instead of once per butterfly value inside the unrolled first / last
+// stage.  Costs one extra shared-memory pass per staged side but emits the
+// functor's code once: for heavy functors (FP64 phase evaluation, sin/cos,
+// transmittances) this keeps the kernel within the instruction cache.
+// Staged store functors receive slot = 0.
+template <int N, bool INV, bool STAGE_LOAD, bool STAGE_STORE, class Load, class Store>
+__device__ __forceinline__ void team_fft_ex(float2* s, const float2* tw, int lane, int team, Load& load,
+                                            Store& store) {
+  constexpr int LPV = Plan<N>::LPV;
+  auto sld = [&](int n) -> float2 { return s[pad_idx(n)]; };
+  auto sst = [&](int k, float2 v, int) { s[pad_idx(k)] = v; };
+  if constexpr (STAGE_LOAD) {
+    team_sync<LPV>(team);  // the previous use of the buffer is complete
+#pragma unroll 4
+    for (int n = lane; n < N; n += LPV) s[pad_idx(n)] = load(n);
+    team_sync<LPV>(team);
+    if constexpr (STAGE_STORE) {
+      Stage<N, LPV, INV, 0, 1>::run(s, tw, lane, team, sld, sst);
+    } else {
+      Stage<N, LPV, INV, 0, 1>::run(s, tw, lane, team, sld, store);
+    }
+  } else {
+    if constexpr (STAGE_STORE) {
+      Stage<N, LPV, INV, 0, 1>::run(s, tw, lane, team, load, sst);
+    } else {
+      Stage<N, LPV, INV, 0, 1>::run(s, tw, lane, team, load, store);
+    }
+  }
+  if constexpr (STAGE_STORE) {
+    team_sync<LPV>(team);
+#pragma unroll 2
+    for (int k = lane; k < N; k += LPV) store(k, s[pad_idx(k)], 0);
+  }
 }
 
 }  // namespace cx

@@ -32,11 +32,11 @@ void set_error(const char* fmt, ...);
     }                                                                                      \
   } while (0)
 
-// FFT lengths compiled into the fast path.
+// FFT lengths compiled into the fast path: 2^a, 3 * 2^a, 5 * 2^a, 7 * 2^a up to 4096.
 #define CX_FOR_EACH_SIZE(X)                                                                          \
-  X(2) X(3) X(4) X(5) X(6) X(8) X(10) X(12) X(16) X(20) X(24) X(32) X(40) X(48) X(64) X(80) X(96)   \
-  X(128) X(160) X(192) X(256) X(320) X(384) X(512) X(640) X(768) X(1024) X(1280) X(1536) X(2048)    \
-  X(2560) X(3072) X(4096)
+  X(2) X(3) X(4) X(5) X(6) X(7) X(8) X(10) X(12) X(14) X(16) X(20) X(24) X(28) X(32) X(40) X(48)    \
+  X(56) X(64) X(80) X(96) X(112) X(128) X(160) X(192) X(224) X(256) X(320) X(384) X(448) X(512)    \
+  X(640) X(768) X(896) X(1024) X(1280) X(1536) X(1792) X(2048) X(2560) X(3072) X(3584) X(4096)
 
 inline bool size_supported(int n) {
   switch (n) {
@@ -49,17 +49,59 @@ inline bool size_supported(int n) {
   }
 }
 
+// Offsets of the per-length twiddle tables inside one device array (lengths in
+// CX_FOR_EACH_SIZE order, tw_len(N) entries each).
+#define CX_SIZE_LIST_(N) N,
+constexpr int kSizes[] = {CX_FOR_EACH_SIZE(CX_SIZE_LIST_)};
+#undef CX_SIZE_LIST_
+constexpr int kNumSizes = sizeof(kSizes) / sizeof(int);
+constexpr int tw_offset(int N) {
+  int off = 0;
+  for (int i = 0; i < kNumSizes; ++i) {
+    if (kSizes[i] == N) return off;
+    off += tw_len(kSizes[i]);
+  }
+  return -1;
+}
+constexpr int tw_total() {
+  int t = 0;
+  for (int i = 0; i < kNumSizes; ++i) t += tw_len(kSizes[i]);
+  return t;
+}
+constexpr int kTwTotal = tw_total();
+
+// Device twiddle tables (twiddles.cu): ensure_twiddles() uploads them (host
+// FP64 values rounded to float) once per device, synchronously, and returns
+// their device address; kernels receive it in their argument structs.
+cx_status ensure_twiddles(const float2** table);
+
+template <int N>
+__device__ __forceinline__ void load_twiddles(float2* tw, const float2* __restrict__ table, int tid, int nthreads) {
+  constexpr int off = tw_offset(N);
+  static_assert(off >= 0, "length not in CX_FOR_EACH_SIZE");
+  const float2* src = table + off;
+  for (int m = tid; m < tw_len(N); m += nthreads) tw[m] = src[m];
+}
+
 int sm_count();  // of the current device (capi.cu)
 
-// Row kernels: about 384 threads, one team per vector (at most 15 multi-warp
-// teams: named barrier ids 1..15).
+// Register budget of the row / column kernels: about 80 registers per thread
+// (min blocks per SM derived from the CTA size).
+__host__ __device__ constexpr int minb_for(int threads) {
+  const int b = 65536 / (threads * 80);
+  return b < 1 ? 1 : b;
+}
+
+// Row kernels: about 192 threads (small CTAs: a 1024^2 pass is 1024 rows, so
+// small CTAs keep all SMs busy), one team per vector, at most 15 multi-warp
+// teams (named barrier ids 1..15).
 template <int N>
 struct RowCfg {
   static constexpr int LPV = Plan<N>::LPV;
-  static constexpr int T0 = 384 / LPV > 0 ? 384 / LPV : 1;
+  static constexpr int T0 = 192 / LPV > 0 ? 192 / LPV : 1;
   static constexpr int TEAMS = (LPV > 32 && T0 > 15) ? 15 : T0;
   static constexpr int THREADS = TEAMS * LPV;
-  static constexpr int MINB = THREADS <= 384 ? 2 : 1;  // register budget: two CTAs per SM
+  static constexpr int MINB = minb_for(THREADS);
   static constexpr int TW = tw_len(N);
   static constexpr size_t SMEM = sizeof(float2) * ((size_t)TW + (size_t)TEAMS * Plan<N>::LEN);
 };
@@ -79,13 +121,13 @@ __host__ __device__ constexpr int col_len(int N, int V) {
 template <int N>
 struct ColCfg {
   static constexpr int LPV = Plan<N>::LPV;
-  static constexpr int V0 = LPV < 32 ? (256 / LPV > 16 ? 256 / LPV : 16) : (LPV <= 64 ? 8 : 4);
+  static constexpr int V0 = LPV < 32 ? (256 / LPV > 16 ? 256 / LPV : 16) : 4;
   static constexpr int TW = tw_len(N);
   static constexpr size_t smem_for(int v) { return sizeof(float2) * ((size_t)TW + (size_t)v * col_len(N, v)); }
   static constexpr int V = smem_for(V0) <= 200 * 1024 ? V0 : (smem_for(V0 / 2) <= 200 * 1024 ? V0 / 2 : V0 / 4);
   static constexpr int LEN = col_len(N, V);
   static constexpr int THREADS = V * LPV;
-  static constexpr int MINB = THREADS <= 384 ? 2 : 1;
+  static constexpr int MINB = minb_for(THREADS);
   static constexpr size_t SMEM = smem_for(V);
 };
 
@@ -149,11 +191,37 @@ __device__ __forceinline__ void load_col_tile(float2* tile, const float2* __rest
   }
 }
 
+// Per-kernel launch facts, computed once per (kernel, device): the
+// shared-memory opt-in and the resident CTAs per SM.  Kept off the per-launch
+// path, which otherwise pays a driver query on every launch.
+struct KernelFacts {
+  int occ = 0;  // CTAs per SM (0 = not yet known)
+  cudaError_t err = cudaSuccess;
+};
+
+// registry keyed by (kernel address, device); defined in capi.cu
+KernelFacts& kernel_facts_slot(const void* kernel, int device);
+
+template <class K>
+inline KernelFacts& kernel_facts(K kernel, int threads, size_t smem) {
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess) dev = 0;
+  KernelFacts& f = kernel_facts_slot(reinterpret_cast<const void*>(kernel), dev);
+  if (f.occ == 0) {
+    if (smem > 48 * 1024) f.err = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    int occ = 0;
+    if (f.err == cudaSuccess &&
+        (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kernel, threads, smem) != cudaSuccess || occ < 1))
+      occ = 1;
+    f.occ = occ;
+  }
+  return f;
+}
+
 template <class K>
 inline int persistent_grid(K kernel, int threads, size_t smem, long work_items_ctas) {
-  int occ = 0;
-  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kernel, threads, smem) != cudaSuccess || occ < 1) occ = 1;
-  long g = (long)sm_count() * occ;
+  KernelFacts& f = kernel_facts(kernel, threads, smem);
+  long g = (long)sm_count() * f.occ;
   if (work_items_ctas < g) g = work_items_ctas;
   if (g < 1) g = 1;
   return (int)g;
@@ -161,8 +229,9 @@ inline int persistent_grid(K kernel, int threads, size_t smem, long work_items_c
 
 template <class K>
 inline cudaError_t set_smem(K kernel, size_t smem) {
-  if (smem > 48 * 1024) return cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-  return cudaSuccess;
+  (void)kernel;
+  (void)smem;
+  return cudaSuccess;  // done once by kernel_facts (called by persistent_grid before every launch)
 }
 
 }  // namespace cx

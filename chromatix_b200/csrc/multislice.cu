@@ -1,0 +1,295 @@
+// C API of the multislice forward / adjoint (kernels in multislice.cuh and
+// the prop2d column pass).
+#include <cmath>
+
+#include "multislice.cuh"
+
+namespace cx {
+
+struct MsPlan {
+  int py, px, D, K, nseg;
+  Prop2DArgs col;  // column pass template (plane pointer set per launch)
+};
+
+static cx_status ms_plan(const cx_ms_desc* d, MsPlan* p) {
+  if (!d || d->ny <= 0 || d->nx <= 0 || d->pad < 0 || d->n_slices <= 0 || !(d->wavelength > 0.0) ||
+      !(d->dy > 0.0) || !(d->dx > 0.0) || d->precision < 0 || d->precision > 1) {
+    set_error("invalid multislice descriptor");
+    return CX_ERR_INVALID;
+  }
+  p->py = d->ny + 2 * d->pad;
+  p->px = d->nx + 2 * d->pad;
+  if (!size_supported(p->py) || !size_supported(p->px)) {
+    set_error("padded grid %dx%d: FFT length not supported", p->py, p->px);
+    return CX_ERR_UNSUPPORTED;
+  }
+  p->D = d->n_slices;
+  int K = d->checkpoint_every;
+  if (K <= 0) K = (int)std::ceil(std::sqrt((double)p->D));
+  if (K > p->D) K = p->D;
+  p->K = K;
+  p->nseg = (p->D + K - 1) / K;
+  Prop2DArgs& a = p->col;
+  a.ny = p->py;
+  a.nx = p->px;
+  a.py = p->py;
+  a.px = p->px;
+  a.pad_y = 0;
+  a.pad_x = 0;
+  a.W = 1;
+  a.n_in_planes = 1;
+  a.n_out_planes = 1;
+  a.out_y0 = 0;
+  a.out_ny = p->py;
+  a.out_x0 = 0;
+  a.out_nx = p->px;
+  a.kernel = CX_KERNEL_ASM;
+  a.precision = d->precision;
+  a.remove_evanescent = d->remove_evanescent;
+  a.bandlimit = d->bandlimit;
+  a.n_med = d->n_medium;
+  a.ky0 = d->ky0;
+  a.kx0 = d->kx0;
+  a.na_f2 = -1.0;
+  a.planes = nullptr;
+  a.H = nullptr;
+  return ensure_twiddles(&a.twg);
+}
+
+static size_t al(size_t b) { return (b + 255) & ~(size_t)255; }
+
+// workspace: [planes (4 x cx_plane)] [F state] ([G state] [K records] for the adjoint)
+static size_t ms_ws(const MsPlan& p, bool grad) {
+  const size_t field = sizeof(float2) * (size_t)p.py * p.px;
+  size_t b = al(4 * sizeof(cx_plane)) + al(field);
+  if (grad) b += al(field) + (size_t)p.K * al(field);
+  return b;
+}
+
+static MsArgs ms_args(const cx_ms_desc* d, const MsPlan& p) {
+  MsArgs a{};
+  a.ny = d->ny;
+  a.nx = d->nx;
+  a.pad_y = d->pad;
+  a.pad_x = d->pad;
+  a.py = p.py;
+  a.px = p.px;
+  a.precision = d->precision;
+  a.lam = d->wavelength;
+  a.dz = d->dz;
+  a.kdz_f = (float)(6.283185307179586476925286766559 * d->dz / d->wavelength);
+  a.twg = p.col.twg;
+  return a;
+}
+
+// planes: 0 slice (+dz), 1 slice adjoint (-dz), 2 defocus (-dist), 3 defocus adjoint (+dist)
+static cx_status ms_upload_planes(const cx_ms_desc* d, const MsPlan& p, cx_plane* dev, cudaStream_t st) {
+  cx_plane h[4];
+  const double zs[4] = {d->dz, -d->dz, -d->reverse_distance, d->reverse_distance};
+  for (int i = 0; i < 4; ++i) {
+    cx_plane& q = h[i];
+    q = cx_plane{};
+    q.z = zs[i];
+    q.wavelength = d->wavelength;
+    q.dy = d->dy;
+    q.dx = d->dx;
+    q.in_plane = 0;
+    q.h_plane = 0;
+    // Matsushima band limit for the slice propagator (propagation.py:557-579, shift 0)
+    if (d->bandlimit && i < 2) {
+      const double ext[2] = {d->dy * p.py, d->dx * p.px};
+      double k0[2], km[2];
+      for (int a = 0; a < 2; ++a) {
+        const double df = 1.0 / ext[a];
+        const double klp = std::pow(std::pow(1.0 / (2 * df), -2.0) * q.z * q.z + 1.0, -0.5) / d->wavelength;
+        const double kln = std::pow(std::pow(-1.0 / (2 * df), -2.0) * q.z * q.z + 1.0, -0.5) / d->wavelength;
+        k0[a] = 0.5 * (klp - kln);
+        km[a] = (klp + kln) / 2.0;
+      }
+      q.bl_y0 = k0[0];
+      q.bl_x0 = k0[1];
+      q.bl_hy = km[0];
+      q.bl_hx = km[1];
+    }
+  }
+  CX_CUDA_TRY(cudaMemcpyAsync(dev, h, sizeof(h), cudaMemcpyHostToDevice, st));
+  return CX_OK;
+}
+
+// slice_prop: the per-slice propagator (band limit / evanescent options of the
+// call); otherwise the plain ASM defocus kernel (samples.py:268-270)
+static cx_status col_pass(const MsPlan& p, const cx_plane* plane, float2* buf, double na_f2, bool slice_prop,
+                          cudaStream_t st) {
+  Prop2DArgs a = p.col;
+  a.planes = plane;
+  a.na_f2 = na_f2;
+  if (!slice_prop) {
+    a.bandlimit = 0;
+    a.remove_evanescent = 0;
+  }
+  return dispatch_cols(p.py, buf, buf, a, st);
+}
+
+static double na_mask(const cx_ms_desc* d) {
+  if (!(d->NA > 0.0)) return -1.0;
+  const double r = d->NA / d->wavelength;
+  return r * r;
+}
+
+}  // namespace cx
+
+using namespace cx;
+
+extern "C" cx_status cx_multislice_workspace_size(const cx_ms_desc* d, int32_t need_grad, size_t* bytes) {
+  MsPlan p;
+  cx_status s = ms_plan(d, &p);
+  if (s != CX_OK) return s;
+  if (!bytes) return CX_ERR_INVALID;
+  *bytes = ms_ws(p, need_grad != 0);
+  return CX_OK;
+}
+
+extern "C" int32_t cx_multislice_num_checkpoints(const cx_ms_desc* d) {
+  MsPlan p;
+  if (ms_plan(d, &p) != CX_OK) return -1;
+  return p.nseg;
+}
+
+extern "C" cx_status cx_multislice_forward(const cx_ms_desc* d, const void* u_in, const float* dn, const float* ab,
+                                           void* u_out, void* checkpoints, void* workspace, size_t workspace_bytes,
+                                           cx_stream_t stream) {
+  MsPlan p;
+  cx_status s = ms_plan(d, &p);
+  if (s != CX_OK) return s;
+  if (!u_in || !dn || !ab || !u_out || !workspace) {
+    set_error("null pointer argument");
+    return CX_ERR_INVALID;
+  }
+  if (workspace_bytes < ms_ws(p, false)) {
+    set_error("workspace too small: %zu < %zu", workspace_bytes, ms_ws(p, false));
+    return CX_ERR_WORKSPACE;
+  }
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  char* w = static_cast<char*>(workspace);
+  cx_plane* planes = reinterpret_cast<cx_plane*>(w);
+  float2* F = reinterpret_cast<float2*>(w + al(4 * sizeof(cx_plane)));
+  float2* ck = static_cast<float2*>(checkpoints);
+  const size_t field = (size_t)p.py * p.px;
+  if ((s = ms_upload_planes(d, p, planes, st)) != CX_OK) return s;
+  MsArgs a = ms_args(d, p);
+  a.dn = dn;
+  a.ab = ab;
+  a.buf = F;
+  // u_0 = pad(u_in) -> FFT_x (recorded as checkpoint 0)
+  a.mode = MS_LOAD;
+  a.src = static_cast<const float2*>(u_in);
+  a.sy = d->ny;
+  a.sx = d->nx;
+  a.oy = d->pad;
+  a.ox = d->pad;
+  a.record = ck ? 1 : 0;
+  a.rec = ck;
+  if ((s = ms_dispatch_rows(p.px, a, st)) != CX_OK) return s;
+  if ((s = col_pass(p, planes + 0, F, -1.0, true, st)) != CX_OK) return s;
+  a.mode = MS_FWD;
+  for (int i = 1; i <= p.D; ++i) {
+    a.slice = i - 1;  // u_i = t_{i-1} P(u_{i-1})
+    a.record = (ck && i < p.D && i % p.K == 0) ? 1 : 0;
+    a.rec = a.record ? ck + (size_t)(i / p.K) * field : nullptr;
+    if ((s = ms_dispatch_rows(p.px, a, st)) != CX_OK) return s;
+    if (i < p.D && (s = col_pass(p, planes + 0, F, -1.0, true, st)) != CX_OK) return s;
+  }
+  // defocus back to the chosen plane, NA mask, crop (samples.py:265-282)
+  if ((s = col_pass(p, planes + 2, F, na_mask(d), false, st)) != CX_OK) return s;
+  a.mode = MS_FINAL;
+  a.record = 0;
+  a.dst = static_cast<float2*>(u_out);
+  return ms_dispatch_rows(p.px, a, st);
+}
+
+extern "C" cx_status cx_multislice_backward(const cx_ms_desc* d, const float* dn, const float* ab,
+                                            const void* checkpoints, const void* grad_out, float* grad_dn,
+                                            float* grad_ab, void* grad_u_in, void* workspace, size_t workspace_bytes,
+                                            cx_stream_t stream) {
+  MsPlan p;
+  cx_status s = ms_plan(d, &p);
+  if (s != CX_OK) return s;
+  if (!dn || !ab || !checkpoints || !grad_out || !grad_dn || !grad_ab || !workspace) {
+    set_error("null pointer argument");
+    return CX_ERR_INVALID;
+  }
+  if (workspace_bytes < ms_ws(p, true)) {
+    set_error("workspace too small: %zu < %zu", workspace_bytes, ms_ws(p, true));
+    return CX_ERR_WORKSPACE;
+  }
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  const size_t field = (size_t)p.py * p.px;
+  char* w = static_cast<char*>(workspace);
+  cx_plane* planes = reinterpret_cast<cx_plane*>(w);
+  w += al(4 * sizeof(cx_plane));
+  float2* F = reinterpret_cast<float2*>(w);
+  w += al(sizeof(float2) * field);
+  float2* G = reinterpret_cast<float2*>(w);
+  w += al(sizeof(float2) * field);
+  float2* seg = reinterpret_cast<float2*>(w);
+  const size_t seg_stride = al(sizeof(float2) * field) / sizeof(float2);
+  const float2* ck = static_cast<const float2*>(checkpoints);
+  if ((s = ms_upload_planes(d, p, planes, st)) != CX_OK) return s;
+
+  MsArgs g = ms_args(d, p);
+  g.dn = dn;
+  g.ab = ab;
+  g.buf = G;
+  // g_D = Q^H pad(g_out)
+  g.mode = MS_LOAD;
+  g.src = static_cast<const float2*>(grad_out);
+  g.sy = d->ny;
+  g.sx = d->nx;
+  g.oy = d->pad;
+  g.ox = d->pad;
+  g.record = 0;
+  if ((s = ms_dispatch_rows(p.px, g, st)) != CX_OK) return s;
+  if ((s = col_pass(p, planes + 3, G, na_mask(d), false, st)) != CX_OK) return s;
+
+  MsArgs f = ms_args(d, p);
+  f.dn = dn;
+  f.ab = ab;
+  f.buf = F;
+  for (int sgi = p.nseg - 1; sgi >= 0; --sgi) {
+    const int i0 = sgi * p.K, i1 = (i0 + p.K < p.D) ? i0 + p.K : p.D;
+    // recompute u_{i0+1} .. u_{i1} from the checkpoint u_{i0}
+    f.mode = MS_LOAD;
+    f.src = ck + (size_t)sgi * field;
+    f.sy = p.py;
+    f.sx = p.px;
+    f.oy = 0;
+    f.ox = 0;
+    f.record = 0;
+    if ((s = ms_dispatch_rows(p.px, f, st)) != CX_OK) return s;
+    if ((s = col_pass(p, planes + 0, F, -1.0, true, st)) != CX_OK) return s;
+    f.mode = MS_FWD;
+    for (int i = i0 + 1; i <= i1; ++i) {
+      f.slice = i - 1;
+      f.record = 1;
+      f.rec = seg + (size_t)(i - i0 - 1) * seg_stride;
+      if ((s = ms_dispatch_rows(p.px, f, st)) != CX_OK) return s;
+      if (i < i1 && (s = col_pass(p, planes + 0, F, -1.0, true, st)) != CX_OK) return s;
+    }
+    // adjoint through slices i1-1 .. i0
+    g.mode = MS_BWD;
+    for (int i = i1 - 1; i >= i0; --i) {
+      g.slice = i;
+      g.rec_u = seg + (size_t)(i - i0) * seg_stride;
+      g.gdn = grad_dn + (size_t)i * d->ny * d->nx;
+      g.gab = grad_ab + (size_t)i * d->ny * d->nx;
+      if ((s = ms_dispatch_rows(p.px, g, st)) != CX_OK) return s;
+      if ((s = col_pass(p, planes + 1, G, -1.0, true, st)) != CX_OK) return s;
+    }
+  }
+  if (grad_u_in) {
+    g.mode = MS_FINAL;
+    g.dst = static_cast<float2*>(grad_u_in);
+    return ms_dispatch_rows(p.px, g, st);
+  }
+  return CX_OK;
+}

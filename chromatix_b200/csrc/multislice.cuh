@@ -1,0 +1,154 @@
+// Thick-sample multislice: row passes of the forward and adjoint slice loop.
+//
+// Reference: functional/samples.py:137-282 (multislice_thick_sample) with
+// thin_sample (samples.py:85-134) and the ASM kernel (propagation.py:499-580).
+//
+// The field state lives in one (py, px) buffer that alternates between the
+// spatial domain and the "row spectrum" domain (FFT along x done).  One slice
+// step is two passes:
+//   row pass:    IFFT_x -> u_{i+1} = t_i * v (optionally recorded) -> FFT_x
+//   column pass: FFT_y -> x H(dz) -> IFFT_y -> 1/(py px)    (prop2d column kernel)
+// so the thin-sample product of slice i and both row transforms share one
+// read and one write of the field.  The adjoint runs the same loop backwards:
+//   row pass:    IFFT_x -> g_{i+1}; dL/d dn_i = k dz Im(g conj u_{i+1}),
+//                dL/d abs_i = -k dz Re(g conj u_{i+1}); g *= conj(t_i) -> FFT_x
+//   column pass: FFT_y -> x conj(H) = H(-dz) -> IFFT_y
+// with g = dL/dRe(u) + i dL/dIm(u).  The forward fields u_{i+1} come from a
+// recomputation of each checkpoint segment.
+#pragma once
+
+#include "prop2d.cuh"
+
+namespace cx {
+
+enum MsMode { MS_LOAD = 0, MS_FWD = 1, MS_BWD = 2, MS_FINAL = 3 };
+
+struct MsArgs {
+  int ny, nx, pad_y, pad_x, py, px;
+  int mode, precision, slice, record;
+  double lam, dz;
+  float kdz_f;          // 2 pi dz / lam rounded once to float
+  int sy, sx, oy, ox;   // MS_LOAD source: (sy, sx) matrix placed at offset (oy, ox) of the padded grid
+  const float* dn;      // (D, ny, nx) refractive-index change (unpadded)
+  const float* ab;      // (D, ny, nx) absorption (unpadded)
+  const float2* src;    // MS_LOAD source
+  float2* buf;          // (py, px) state
+  float2* rec;          // record target (py, px), spatial domain
+  const float2* rec_u;  // MS_BWD: u_{i+1} (py, px), spatial domain
+  float* gdn;           // MS_BWD: dL/d dn_i  (ny, nx)
+  float* gab;           // MS_BWD: dL/d abs_i (ny, nx)
+  float2* dst;          // MS_FINAL: (ny, nx) crop of the padded grid
+  const float2* twg;  // device twiddle tables (ensure_twiddles)
+};
+
+// thin-sample transmittance t = exp(i 2 pi dz / lam (dn + i abs))
+__device__ __forceinline__ float2 ms_transmittance(const MsArgs& a, float dn, float ab) {
+  if (a.precision == CX_PREC_REF32) {
+    // 1j * 2 * pi (folded) * (dn + 1j abs) * thickness / lam, complex64 ops in order
+    const float TWO_PI = 6.28318530717958647692f;
+    const float th = (float)a.dz, lam = (float)a.lam;
+    const float re = fd(fm(-fm(TWO_PI, ab), th), lam);
+    const float im = fd(fm(fm(TWO_PI, dn), th), lam);
+    float s, c;
+    sincosf(im, &s, &c);
+    const float m = expf(re);
+    return make_float2(m * c, m * s);
+  }
+  // k dz is formed in FP64 (kdz_f); the slice phase k dz dn is a few tenths of
+  // a radian for physical dn, so FP32 with the accurate sincosf suffices
+  const float m = __expf(-a.kdz_f * ab);
+  float s, c;
+  sincosf(a.kdz_f * dn, &s, &c);
+  return make_float2(m * c, m * s);
+}
+
+template <int NX, int MODE>
+__global__ void __launch_bounds__(RowCfg<NX>::THREADS, RowCfg<NX>::MINB) k_ms_rows(MsArgs a) {
+  using C = RowCfg<NX>;
+  extern __shared__ float2 sm[];
+  float2* tw = sm;
+  load_twiddles<NX>(tw, a.twg, threadIdx.x, blockDim.x);
+  __syncthreads();
+  const int team = threadIdx.x / C::LPV, lane = threadIdx.x % C::LPV;
+  float2* s = sm + C::TW + team * Plan<NX>::LEN;
+  // MS_FINAL only produces the cropped rows
+  const int r0 = MODE == MS_FINAL ? a.pad_y : 0;
+  const int nrows = MODE == MS_FINAL ? a.ny : a.py;
+  const long total = nrows;
+  const size_t plane_d = (size_t)a.slice * a.ny * a.nx;
+  const double kdz = 6.283185307179586476925286766559 * a.dz / a.lam;
+  for (long base = (long)blockIdx.x * C::TEAMS; base < total; base += (long)gridDim.x * C::TEAMS) {
+    const long item = base + team;
+    if (item >= total) continue;
+    const int y = r0 + (int)item;
+    const int yd = y - a.pad_y;
+    const bool yin = yd >= 0 && yd < a.ny;
+    float2* row = a.buf + (size_t)y * a.px;
+    if constexpr (MODE == MS_LOAD) {
+      const int ys = y - a.oy;
+      const bool rin = ys >= 0 && ys < a.sy;
+      const float2* srow = a.src + (size_t)(rin ? ys : 0) * a.sx;
+      float2* rrow = a.rec ? a.rec + (size_t)y * a.px : nullptr;
+      auto load = [&](int n) -> float2 {
+        const int xs = n - a.ox;
+        const float2 v = (rin && xs >= 0 && xs < a.sx) ? srow[xs] : make_float2(0.f, 0.f);
+        if (a.record) rrow[n] = v;
+        return v;
+      };
+      auto store = [&](int k, float2 v, int) { row[k] = v; };
+      team_fft<NX, false>(s, tw, lane, team, load, store);
+      continue;
+    }
+    // inverse FFT along x of the row spectrum
+    auto load_row = [&](int n) -> float2 { return row[n]; };
+    if constexpr (MODE == MS_FINAL) {
+      float2* drow = a.dst + (size_t)yd * a.nx;
+      auto store = [&](int k, float2 v, int) {
+        const int xd = k - a.pad_x;
+        if (xd >= 0 && xd < a.nx) drow[xd] = v;
+      };
+      team_fft<NX, true>(s, tw, lane, team, load_row, store);
+      continue;
+    }
+    if constexpr (MODE == MS_FWD || MODE == MS_BWD) {
+    if constexpr (MODE == MS_FWD) {
+      float2* rrow = a.record ? a.rec + (size_t)y * a.px : nullptr;
+      auto store1 = [&](int k, float2 v, int) {
+        const int xd = k - a.pad_x;
+        if (yin && xd >= 0 && xd < a.nx) {
+          const size_t idx = plane_d + (size_t)yd * a.nx + xd;
+          v = cmul(v, ms_transmittance(a, a.dn[idx], a.ab[idx]));
+        }
+        if (a.record) rrow[k] = v;
+        s[pad_idx(k)] = v;
+      };
+      team_fft_ex<NX, true, false, true>(s, tw, lane, team, load_row, store1);
+    } else {  // MS_BWD
+      const float2* urow = a.rec_u + (size_t)y * a.px;
+      auto store1 = [&](int k, float2 g, int) {
+        const int xd = k - a.pad_x;
+        if (yin && xd >= 0 && xd < a.nx) {
+          const size_t idx = plane_d + (size_t)yd * a.nx + xd;
+          const float2 u = urow[k];
+          // w = g * conj(u)
+          const float wr = g.x * u.x + g.y * u.y, wi = g.y * u.x - g.x * u.y;
+          const size_t gi = (size_t)yd * a.nx + xd;
+          a.gdn[gi] = (float)(kdz * (double)wi);
+          a.gab[gi] = (float)(-kdz * (double)wr);
+          g = cmul(g, cconj(ms_transmittance(a, a.dn[idx], a.ab[idx])));
+        }
+        s[pad_idx(k)] = g;
+      };
+      team_fft_ex<NX, true, false, true>(s, tw, lane, team, load_row, store1);
+    }
+    team_sync<C::LPV>(team);
+    auto load2 = [&](int n) -> float2 { return s[pad_idx(n)]; };
+    auto store2 = [&](int k, float2 v, int) { row[k] = v; };
+    team_fft<NX, false>(s, tw, lane, team, load2, store2);
+    }
+  }
+}
+
+cx_status ms_dispatch_rows(int n, const MsArgs& a, cudaStream_t st);
+
+}  // namespace cx

@@ -63,6 +63,7 @@ extern "C" cx_status cx_optical_fft(const cx_optfft_desc* d, const cx_fft_plane*
     return CX_ERR_WORKSPACE;
   }
   a.planes = planes_dev;
+  if ((s = ensure_twiddles(&a.twg)) != CX_OK) return s;
   cudaStream_t st = static_cast<cudaStream_t>(stream);
   float2* T = static_cast<float2*>(workspace);
   if ((s = opt_dispatch_rows(a.px, static_cast<const float2*>(u_in), T, a, st)) != CX_OK) return s;

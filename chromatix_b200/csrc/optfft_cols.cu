@@ -11,7 +11,7 @@ __global__ void __launch_bounds__(ColCfg<NY>::THREADS, ColCfg<NY>::MINB) k_opt_c
   extern __shared__ float2 sm[];
   float2* tw = sm;
   float2* tile = sm + C::TW;
-  init_twiddles<NY>(tw, threadIdx.x, blockDim.x);
+  load_twiddles<NY>(tw, a.twg, threadIdx.x, blockDim.x);
   const int team = threadIdx.x / C::LPV, lane = threadIdx.x % C::LPV;
   float2* s = tile + team * LEN;
   const int tiles_x = (a.px + V - 1) / V;
@@ -31,17 +31,19 @@ __global__ void __launch_bounds__(ColCfg<NY>::THREADS, ColCfg<NY>::MINB) k_opt_c
     const double rx = pl.dx_out * ((double)col - 0.5 * a.px) + pl.ox;
     const float2 post = make_float2((float)pl.post_re, (float)pl.post_im);
     auto load = [&](int n) -> float2 { return s[pad_idx(n)]; };
+    // the tile stays in FFT order (the staged store updates it in place);
+    // the fftshift along y is applied by the final copy
     auto store = [&](int k, float2 v, int) {
-      const int row = (k + a.py / 2) % a.py;  // fftshift along y
+      const int row = (k + a.py / 2) % a.py;  // output row of bin k (fftshift along y)
       if (pl.conj) v = cconj(v);
       v = cmul(post, v);
       if (pl.chirp_out != 0.0) {
         const double ry = pl.dy_out * ((double)row - 0.5 * a.py) + pl.oy;
         v = cmul(v, chirp(pl.chirp_out, ry, rx));
       }
-      s[pad_idx(row)] = v;
+      s[pad_idx(k)] = v;
     };
-    team_fft<NY, false>(s, tw, lane, team, load, store);
+    team_fft_ex<NY, false, false, true>(s, tw, lane, team, load, store);
     __syncthreads();
     const int b = q / a.W, w = q % a.W;
     for (int idx = threadIdx.x; idx < a.oy_n * V; idx += blockDim.x) {
@@ -49,7 +51,8 @@ __global__ void __launch_bounds__(ColCfg<NY>::THREADS, ColCfg<NY>::MINB) k_opt_c
       if (x >= a.px) continue;
       const int colo = (x + a.px / 2) % a.px - a.crop_x;
       if (colo < 0 || colo >= a.ox_n) continue;
-      out[(((size_t)b * a.oy_n + r) * a.ox_n + colo) * a.W + w] = tile[c * LEN + pad_idx(r + a.crop_y)];
+      const int k = (r + a.crop_y + a.py - a.py / 2) % a.py;  // FFT bin of output row r
+      out[(((size_t)b * a.oy_n + r) * a.ox_n + colo) * a.W + w] = tile[c * LEN + pad_idx(k)];
     }
   }
 }

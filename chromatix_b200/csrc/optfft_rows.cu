@@ -9,7 +9,7 @@ __global__ void __launch_bounds__(RowCfg<NX>::THREADS, RowCfg<NX>::MINB) k_opt_r
   using C = RowCfg<NX>;
   extern __shared__ float2 sm[];
   float2* tw = sm;
-  init_twiddles<NX>(tw, threadIdx.x, blockDim.x);
+  load_twiddles<NX>(tw, a.twg, threadIdx.x, blockDim.x);
   __syncthreads();
   const int team = threadIdx.x / C::LPV, lane = threadIdx.x % C::LPV;
   float2* s = sm + C::TW + team * Plan<NX>::LEN;
@@ -43,7 +43,7 @@ __global__ void __launch_bounds__(RowCfg<NX>::THREADS, RowCfg<NX>::MINB) k_opt_r
     auto store = [&](int k, float2 v, int) {
       if (valid) dst[k] = v;
     };
-    team_fft<NX, false>(s, tw, lane, team, load, store);
+    team_fft_ex<NX, false, true, false>(s, tw, lane, team, load, store);
   }
 }
 

@@ -59,6 +59,8 @@ static cx_status make_args(const cx_prop2d_desc* d, Prop2DArgs* a) {
   a->n_med = d->n_medium;
   a->ky0 = d->ky0;
   a->kx0 = d->kx0;
+  a->na_f2 = -1.0;
+  a->twg = nullptr;
   a->planes = nullptr;
   a->H = nullptr;
   if (!size_supported(a->py) || !size_supported(a->px)) {
@@ -108,6 +110,7 @@ extern "C" cx_status cx_prop2d(const cx_prop2d_desc* d, const cx_plane* planes_d
   }
   a.planes = planes_dev;
   a.H = static_cast<const float2*>(H);
+  if ((s = ensure_twiddles(&a.twg)) != CX_OK) return s;
   float2* T = static_cast<float2*>(workspace);
   float2* T2 = reinterpret_cast<float2*>(static_cast<char*>(workspace) + align256(ws_T_bytes(a)));
   cudaStream_t st = static_cast<cudaStream_t>(stream);

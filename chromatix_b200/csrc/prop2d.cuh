@@ -21,8 +21,10 @@ struct Prop2DArgs {
   int out_y0, out_ny, out_x0, out_nx;
   int kernel, precision, remove_evanescent, bandlimit;
   double n_med, ky0, kx0;
+  double na_f2;  // >= 0: k-space NA mask |f|^2 <= na_f2 (samples.py:276-280); < 0: none
   const cx_plane* planes;
   const float2* H;
+  const float2* twg;  // device twiddle tables (ensure_twiddles)
 };
 
 // --------------------------------------------------------------------------
@@ -30,6 +32,26 @@ struct Prop2DArgs {
 // --------------------------------------------------------------------------
 __device__ __forceinline__ float2 prop_kernel_accurate(int ky, int kx, const Prop2DArgs& a, const cx_plane& pl) {
   const double pi = 3.141592653589793238462643383279502884;
+  const double K = 2.0 * pi * fabs(pl.z) * a.n_med / pl.wavelength;  // largest ASM phase (rad)
+  if (a.kernel == CX_KERNEL_ASM && K <= 8.0 && !a.bandlimit && pl.shift_y == 0.0 && pl.shift_x == 0.0) {
+    // Short distances (thin slices): every phase term is below 8 rad, so FP32
+    // evaluation keeps the phase error below ~2e-6 rad -- inside the accuracy
+    // budget -- at a fraction of the FP64 cost.
+    const float fy = (float)freq_index(ky, a.py) * (float)(1.0 / ((double)a.py * pl.dy)) - (float)a.ky0;
+    const float fx = (float)freq_index(kx, a.px) * (float)(1.0 / ((double)a.px * pl.dx)) - (float)a.kx0;
+    const float q = (float)(pl.wavelength / a.n_med);
+    const float kern = 1.0f - (q * q) * (fy * fy + fx * fx);
+    float amp = 1.f, ph = 0.f;
+    if (kern >= 0.f || a.remove_evanescent) {
+      ph = (float)K * sqrtf(fmaxf(kern, 0.f));
+    } else {
+      amp = __expf(-(float)K * sqrtf(-kern));
+    }
+    float sn, cs;
+    __sincosf(ph - 6.2831853071795865f * rintf(ph * 0.15915494309189534f), &sn, &cs);
+    if (pl.z < 0.0) sn = -sn;
+    return make_float2(amp * cs, amp * sn);
+  }
   const double fy = (double)freq_index(ky, a.py) / ((double)a.py * pl.dy);
   const double fx = (double)freq_index(kx, a.px) / ((double)a.px * pl.dx);
   const double gy = fy - a.ky0, gx = fx - a.kx0;
@@ -41,7 +63,6 @@ __device__ __forceinline__ float2 prop_kernel_accurate(int ky, int kx, const Pro
   if (a.bandlimit && (fabs(fy - pl.bl_y0) > pl.bl_hy || fabs(fx - pl.bl_x0) > pl.bl_hx)) return make_float2(0.f, 0.f);
   const double q = pl.wavelength / a.n_med;
   const double kern = 1.0 - q * q * s;
-  const double K = 2.0 * pi * fabs(pl.z) * a.n_med / pl.wavelength;
   const double sh = 2.0 * pi * (fy * pl.shift_y + fx * pl.shift_x);
   double amp = 1.0, ph;
   if (kern >= 0.0 || a.remove_evanescent) {
@@ -90,7 +111,15 @@ __device__ __forceinline__ float2 prop_kernel_ref32(int ky, int kx, const Prop2D
   return make_float2(amp * cs, amp * sn);
 }
 
+__device__ __forceinline__ bool outside_na(int ky, int kx, const Prop2DArgs& a, const cx_plane& pl) {
+  if (a.na_f2 < 0.0) return false;
+  const double fy = (double)freq_index(ky, a.py) / ((double)a.py * pl.dy);
+  const double fx = (double)freq_index(kx, a.px) / ((double)a.px * pl.dx);
+  return fy * fy + fx * fx > a.na_f2;
+}
+
 __device__ __forceinline__ float2 prop_kernel(int ky, int kx, const Prop2DArgs& a, const cx_plane& pl) {
+  if (outside_na(ky, kx, a, pl)) return make_float2(0.f, 0.f);
   if (a.kernel == CX_KERNEL_EXPLICIT)
     return a.H[((size_t)pl.h_plane * a.py + ky) * a.px + kx];
   return a.precision == CX_PREC_REF32 ? prop_kernel_ref32(ky, kx, a, pl) : prop_kernel_accurate(ky, kx, a, pl);
@@ -105,7 +134,7 @@ __global__ void __launch_bounds__(RowCfg<NX>::THREADS, RowCfg<NX>::MINB) k_prop_
   using C = RowCfg<NX>;
   extern __shared__ float2 sm[];
   float2* tw = sm;
-  init_twiddles<NX>(tw, threadIdx.x, blockDim.x);
+  load_twiddles<NX>(tw, a.twg, threadIdx.x, blockDim.x);
   __syncthreads();
   const int team = threadIdx.x / C::LPV, lane = threadIdx.x % C::LPV;
   float2* s = sm + C::TW + team * Plan<NX>::LEN;
@@ -140,7 +169,7 @@ __global__ void __launch_bounds__(ColCfg<NY>::THREADS, ColCfg<NY>::MINB) k_prop_
   extern __shared__ float2 sm[];
   float2* tw = sm;
   float2* tile = sm + C::TW;
-  init_twiddles<NY>(tw, threadIdx.x, blockDim.x);
+  load_twiddles<NY>(tw, a.twg, threadIdx.x, blockDim.x);
   const int team = threadIdx.x / C::LPV, lane = threadIdx.x % C::LPV;
   float2* s = tile + team * LEN;
   const int tiles_x = (a.px + V - 1) / V;
@@ -162,7 +191,7 @@ __global__ void __launch_bounds__(ColCfg<NY>::THREADS, ColCfg<NY>::MINB) k_prop_
       return (n >= a.pad_y && n < a.pad_y + a.ny) ? s[pad_idx(n)] : make_float2(0.f, 0.f);
     };
     auto store1 = [&](int k, float2 v, int) { s[pad_idx(k)] = valid ? cmul(v, prop_kernel(k, kx, a, pl)) : v; };
-    team_fft<NY, false>(s, tw, lane, team, load1, store1);
+    team_fft_ex<NY, false, false, true>(s, tw, lane, team, load1, store1);
     team_sync<C::LPV>(team);
     auto load2 = [&](int n) -> float2 { return s[pad_idx(n)]; };
     auto store2 = [&](int k, float2 v, int) { s[pad_idx(k)] = cscale(v, scale); };
@@ -184,7 +213,7 @@ __global__ void __launch_bounds__(RowCfg<NX>::THREADS, RowCfg<NX>::MINB) k_prop_
   using C = RowCfg<NX>;
   extern __shared__ float2 sm[];
   float2* tw = sm;
-  init_twiddles<NX>(tw, threadIdx.x, blockDim.x);
+  load_twiddles<NX>(tw, a.twg, threadIdx.x, blockDim.x);
   __syncthreads();
   const int team = threadIdx.x / C::LPV, lane = threadIdx.x % C::LPV;
   float2* s = sm + C::TW + team * Plan<NX>::LEN;

@@ -230,6 +230,7 @@ static cx_status psf_setup(const cx_psf_desc* d, const cx_psf_spectrum* spec, co
   a.counts = static_cast<unsigned long long*>(workspace);
   a.srange = reinterpret_cast<int*>(static_cast<char*>(workspace) + 64);
   a.T = reinterpret_cast<float2*>(static_cast<char*>(workspace) + 256);
+  if ((s = ensure_twiddles(&a.twg)) != CX_OK) return s;
   a.rowsum = 0;
   for (int w = 0; w < a.W; ++w) {
     psf_rows(d, spec, w, &a.ylo[w], &a.nrows[w]);

@@ -47,6 +47,7 @@ struct PsfArgs {
   const unsigned long long* counts;  // [0, 8): pupil pixel counts per wavelength
   const int* srange;                 // [0, 8): ny - first support row ; [8, 16): last support row + 1
   float* out;
+  const float2* twg;  // device twiddle tables (ensure_twiddles)
 };
 
 // exact pupil row range [first, last + 1) of wavelength w (from the count pass)
@@ -106,7 +107,7 @@ __global__ void __launch_bounds__(RowCfg<NX>::THREADS, RowCfg<NX>::MINB) k_psf_r
   extern __shared__ float2 sm[];
   float2* tw = sm;
   __shared__ float2 cw[PSF_MAX_WV];
-  init_twiddles<NX>(tw, threadIdx.x, blockDim.x);
+  load_twiddles<NX>(tw, a.twg, threadIdx.x, blockDim.x);
   if (threadIdx.x < a.W) cw[threadIdx.x] = psf_const(a, threadIdx.x, a.counts);
   __syncthreads();
   const int team = threadIdx.x / C::LPV, lane = threadIdx.x % C::LPV;
@@ -158,7 +159,7 @@ __global__ void __launch_bounds__(RowCfg<NX>::THREADS, RowCfg<NX>::MINB) k_psf_r
     };
     float2* dst = a.T + ((size_t)zl * a.rowsum + rem) * a.nx;
     auto store = [&](int k, float2 v, int) { dst[k] = v; };
-    team_fft<NX, false>(s, tw, lane, team, load, store);
+    team_fft_ex<NX, false, true, false>(s, tw, lane, team, load, store);
   }
 }
 
@@ -181,7 +182,7 @@ __global__ void __launch_bounds__(ColCfg<NY>::THREADS, ColCfg<NY>::MINB) k_psf_c
   float2* tw = sm;
   float2* tile = sm + C::TW;
   float* accs = reinterpret_cast<float*>(reinterpret_cast<char*>(sm) + ((C::SMEM + 15) & ~(size_t)15));
-  init_twiddles<NY>(tw, threadIdx.x, blockDim.x);
+  load_twiddles<NY>(tw, a.twg, threadIdx.x, blockDim.x);
   const int team = threadIdx.x / C::LPV, lane = threadIdx.x % C::LPV;
   float2* s = tile + team * LEN;
   float* acc = accs + team * ACC;

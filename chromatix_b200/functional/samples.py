@@ -7,7 +7,7 @@ import numpy as np
 from .. import _native as nat
 from ..core.field import Field
 
-__all__ = ["thin_sample"]
+__all__ = ["thin_sample", "multislice_thick_sample"]
 
 
 def thin_sample(field: Field, absorption, dn, thickness) -> Field:
@@ -33,3 +33,159 @@ def thin_sample(field: Field, absorption, dn, thickness) -> Field:
     arg = 2 * np.pi * thickness / lam
     t = torch.polar(torch.exp(-arg * a), arg * d).to(torch.complex64)
     return field.replace(u=field.u * t)
+
+
+class cx_ms_desc(nat.ctypes.Structure):
+    _fields_ = [("ny", nat.c_int32), ("nx", nat.c_int32), ("pad", nat.c_int32), ("n_slices", nat.c_int32),
+                ("precision", nat.c_int32), ("remove_evanescent", nat.c_int32), ("bandlimit", nat.c_int32),
+                ("checkpoint_every", nat.c_int32), ("n_medium", nat.c_double), ("wavelength", nat.c_double),
+                ("dy", nat.c_double), ("dx", nat.c_double), ("dz", nat.c_double),
+                ("reverse_distance", nat.c_double), ("NA", nat.c_double), ("ky0", nat.c_double),
+                ("kx0", nat.c_double)]
+
+
+_MS_SIG = False
+
+
+def _ms_lib():
+    global _MS_SIG
+    L = nat.lib()
+    if not _MS_SIG:
+        P = nat.ctypes.POINTER(cx_ms_desc)
+        V = nat.c_void_p
+        L.cx_multislice_workspace_size.restype = nat.c_int32
+        L.cx_multislice_workspace_size.argtypes = [P, nat.c_int32, nat.ctypes.POINTER(nat.c_size_t)]
+        L.cx_multislice_num_checkpoints.restype = nat.c_int32
+        L.cx_multislice_num_checkpoints.argtypes = [P]
+        L.cx_multislice_forward.restype = nat.c_int32
+        L.cx_multislice_forward.argtypes = [P, V, V, V, V, V, V, nat.c_size_t, V]
+        L.cx_multislice_backward.restype = nat.c_int32
+        L.cx_multislice_backward.argtypes = [P, V, V, V, V, V, V, V, V, nat.c_size_t, V]
+        _MS_SIG = True
+    return L
+
+
+def _ms_forward(d: cx_ms_desc, u, dn, ab, want_ckpt: bool):
+    torch = nat.torch_mod()
+    L = _ms_lib()
+    dev = u.device
+    ws_b = nat.c_size_t(0)
+    nat.check(L.cx_multislice_workspace_size(d, 0, ws_b))
+    ws = nat.workspace(ws_b.value, dev)
+    out = torch.empty((d.ny, d.nx), dtype=torch.complex64, device=dev)
+    ck = None
+    if want_ckpt:
+        nck = L.cx_multislice_num_checkpoints(d)
+        ck = torch.empty((nck, d.ny + 2 * d.pad, d.nx + 2 * d.pad), dtype=torch.complex64, device=dev)
+    nat.check(L.cx_multislice_forward(d, nat.ptr(u), nat.ptr(dn), nat.ptr(ab), nat.ptr(out), nat.ptr(ck),
+                                      nat.ptr(ws), ws_b.value, nat.stream_handle(dev)))
+    return out, ck
+
+
+def _ms_backward(d: cx_ms_desc, dn, ab, ck, grad_out, need_u: bool):
+    torch = nat.torch_mod()
+    L = _ms_lib()
+    dev = grad_out.device
+    ws_b = nat.c_size_t(0)
+    nat.check(L.cx_multislice_workspace_size(d, 1, ws_b))
+    ws = nat.workspace(ws_b.value, dev)
+    gdn = torch.empty_like(dn)
+    gab = torch.empty_like(ab)
+    gu = torch.empty((d.ny, d.nx), dtype=torch.complex64, device=dev) if need_u else None
+    g = grad_out.to(torch.complex64).contiguous()
+    nat.check(L.cx_multislice_backward(d, nat.ptr(dn), nat.ptr(ab), nat.ptr(ck), nat.ptr(g), nat.ptr(gdn),
+                                       nat.ptr(gab), nat.ptr(gu), nat.ptr(ws), ws_b.value, nat.stream_handle(dev)))
+    return gdn, gab, gu
+
+
+def _autograd_fn():
+    torch = nat.torch_mod()
+
+    class _Multislice(torch.autograd.Function):
+        """Forward: the fused multislice loop; backward: the hand-written adjoint
+        (checkpoints every K slices, recomputation in between)."""
+
+        @staticmethod
+        def forward(ctx, u, dn, ab, desc_bytes):
+            d = cx_ms_desc.from_buffer_copy(desc_bytes)
+            need = ctx.needs_input_grad
+            out, ck = _ms_forward(d, u.contiguous(), dn, ab, want_ckpt=any(need[:3]))
+            ctx.desc_bytes = desc_bytes
+            if any(need[:3]):
+                ctx.save_for_backward(dn, ab, ck)
+            return out
+
+        @staticmethod
+        def backward(ctx, grad_out):
+            dn, ab, ck = ctx.saved_tensors
+            d = cx_ms_desc.from_buffer_copy(ctx.desc_bytes)
+            need = ctx.needs_input_grad
+            gdn, gab, gu = _ms_backward(d, dn, ab, ck, grad_out, need_u=need[0])
+            return (gu if need[0] else None, gdn if need[1] else None, gab if need[2] else None, None)
+
+    return _Multislice
+
+
+_MS_FN = None
+
+
+def multislice_thick_sample(field: Field, absorption_stack, dn_stack, n, thickness_per_slice, pad_width: int,
+                            NA=None, propagator=None, kykx=(0.0, 0.0), reverse_propagate_distance=None,
+                            return_stack: bool = False, remove_evanescent: bool = False, bandlimit: bool = False,
+                            *, checkpoint_every: int = 0, precision=None) -> Field:
+    """Thick sample as D thin slices (functional/samples.py:137-282).
+
+    Each slice: ``u <- t_i * IFFT2(H(dz) FFT2(u))`` with the ASM kernel H and
+    ``t_i = exp(i 2 pi (dn_i + i abs_i) dz / lambda)``; afterwards the field is
+    propagated back by ``reverse_propagate_distance`` (default: half the stack)
+    with an optional NA mask, and cropped by ``pad_width``.  Differentiable with
+    respect to the field, ``dn_stack`` and ``absorption_stack`` through a
+    hand-written adjoint that stores a checkpoint every ``checkpoint_every``
+    slices (default ceil(sqrt(D))) and recomputes in between.
+    """
+    from .. import config
+    from .sources import materialize
+
+    global _MS_FN
+    torch = nat.torch_mod()
+    field = materialize(field)
+    if field.chromatic and field.n_wv != 1:
+        raise NotImplementedError("multislice supports monochromatic scalar fields")
+    if propagator is not None:
+        raise NotImplementedError("a custom propagator is not supported by the fused slice kernel")
+    if return_stack:
+        raise NotImplementedError("return_stack is not supported by the fused slice kernel")
+    dev = field.device
+    dn = dn_stack if isinstance(dn_stack, torch.Tensor) else torch.as_tensor(np.asarray(dn_stack, np.float32))
+    ab = absorption_stack if isinstance(absorption_stack, torch.Tensor) else torch.as_tensor(
+        np.asarray(absorption_stack, np.float32))
+    dn = dn.to(device=dev, dtype=torch.float32).contiguous()
+    ab = ab.to(device=dev, dtype=torch.float32).contiguous()
+    if tuple(dn.shape) != tuple(ab.shape):
+        raise AssertionError("absorption_stack and dn_stack must have equal shapes")
+    D, ny, nx = dn.shape
+    if (ny, nx) != tuple(field.spatial_shape):
+        raise AssertionError("stack slices must match the field's spatial shape")
+    if reverse_propagate_distance is None:
+        reverse_propagate_distance = thickness_per_slice * D / 2
+    d = cx_ms_desc()
+    d.ny, d.nx, d.pad, d.n_slices = ny, nx, int(pad_width), D
+    d.precision = config.precision_code(precision)
+    d.remove_evanescent, d.bandlimit = int(bool(remove_evanescent)), int(bool(bandlimit))
+    d.checkpoint_every = int(checkpoint_every)
+    d.n_medium = float(n)
+    d.wavelength = float(field.spectrum.wavelength[0])
+    d.dy, d.dx = (float(v) for v in field.dx_wv[0])
+    d.dz = float(thickness_per_slice)
+    d.reverse_distance = float(reverse_propagate_distance)
+    d.NA = -1.0 if NA is None else float(NA)
+    d.ky0, d.kx0 = (float(v) for v in np.asarray(kykx, np.float64).reshape(2))
+    desc_bytes = bytes(d)
+    if _MS_FN is None:
+        _MS_FN = _autograd_fn()
+    u = field.u
+    lead = u.shape[:-3] if field.chromatic else u.shape[:-2]
+    u2 = u.reshape((-1, ny, nx))
+    outs = [_MS_FN.apply(u2[b], dn, ab, desc_bytes) for b in range(u2.shape[0])]
+    out = torch.stack(outs).reshape(u.shape)
+    return field.replace(u=out)

@@ -194,6 +194,41 @@ cx_status cx_optfft_workspace_size(const cx_optfft_desc* d, size_t* bytes);
 cx_status cx_optical_fft(const cx_optfft_desc* d, const cx_fft_plane* planes_dev, const void* u_in, void* u_out,
                          void* workspace, size_t workspace_bytes, cx_stream_t stream);
 
+/* ---------------------------------------------------------------------------
+ * Thick-sample multislice, forward and adjoint
+ *   multislice_thick_sample (functional/samples.py:137-282) with
+ *   thin_sample (samples.py:85-134) and the ASM kernel (propagation.py:499-580)
+ * u_{i+1} = t_i * IFFT2(H(dz) FFT2(u_i)), t_i = exp(i 2 pi dz/lambda (dn_i + i abs_i)),
+ * then the defocus by -reverse_distance (ASM, optional NA mask) and the crop.
+ * The adjoint takes g_out = dL/dRe(u_out) + i dL/dIm(u_out) and returns
+ * dL/d dn, dL/d abs (and dL/du_in), recomputing each checkpoint segment.
+ * ------------------------------------------------------------------------- */
+typedef struct {
+  int32_t ny, nx;            /* field shape (unpadded) */
+  int32_t pad;               /* pad_width on each side */
+  int32_t n_slices;          /* D */
+  int32_t precision;         /* cx_precision */
+  int32_t remove_evanescent, bandlimit;  /* slice propagator options */
+  int32_t checkpoint_every;  /* K; <= 0: ceil(sqrt(D)) */
+  double n_medium, wavelength, dy, dx;
+  double dz;                 /* thickness_per_slice */
+  double reverse_distance;   /* defocus back by this distance */
+  double NA;                 /* <= 0: no NA mask */
+  double ky0, kx0;           /* kykx */
+} cx_ms_desc;
+
+cx_status cx_multislice_workspace_size(const cx_ms_desc* d, int32_t need_grad, size_t* bytes);
+/* number of checkpoints the forward writes (each (ny + 2 pad) x (nx + 2 pad) complex64) */
+int32_t cx_multislice_num_checkpoints(const cx_ms_desc* d);
+/* dn, abs: (D, ny, nx) float32; u_in, u_out: (ny, nx) complex64; checkpoints may be NULL
+ * (forward only). */
+cx_status cx_multislice_forward(const cx_ms_desc* d, const void* u_in, const float* dn, const float* abs_,
+                                void* u_out, void* checkpoints, void* workspace, size_t workspace_bytes,
+                                cx_stream_t stream);
+cx_status cx_multislice_backward(const cx_ms_desc* d, const float* dn, const float* abs_, const void* checkpoints,
+                                 const void* grad_out, float* grad_dn, float* grad_abs, void* grad_u_in,
+                                 void* workspace, size_t workspace_bytes, cx_stream_t stream);
+
 /* Field.intensity (core/field.py:656-665, 735-740): out[b, y, x] =
  * sum_wv density[wv] |u[b, y, x, wv]|^2.  density_dev: n_wv doubles. */
 cx_status cx_intensity(const void* u, int64_t n_pix, int32_t n_wv, const double* density_dev, float* out,
@@ -204,6 +239,10 @@ cx_status cx_intensity(const void* u, int64_t n_pix, int32_t n_wv, const double*
  * ------------------------------------------------------------------------- */
 const char* cx_last_error(void);
 int32_t cx_version(void);
+/* One-time set-up of the current device (uploads the FFT twiddle tables).
+ * Every entry point does this on its first call on a device; call cx_init
+ * explicitly before capturing a stream into a CUDA graph. */
+cx_status cx_init(void);
 /* 1 if an FFT length is compiled in (fast path), else 0. */
 int32_t cx_fft_size_supported(int32_t n);
 /* Batched complex FFT along the last axis (test/utility entry):

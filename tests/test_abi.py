@@ -52,7 +52,7 @@ def test_library_loads_without_gpu():
     L = nat.lib()
     assert L.cx_version() >= 100
     assert L.cx_fft_size_supported(1280) == 1
-    assert L.cx_fft_size_supported(77) == 0
+    assert L.cx_fft_size_supported(143) == 0
 
 
 def test_workspace_queries_and_validation_without_gpu():
@@ -69,8 +69,8 @@ def test_workspace_queries_and_validation_without_gpu():
     d.ny = 0
     assert L.cx_prop2d_workspace_size(d, b) == 1
     assert b"invalid" in L.cx_last_error()
-    d.ny, d.pad_y = 7, 0
-    assert L.cx_prop2d_workspace_size(d, b) == 2  # 7 x 1024: length 7 not compiled in
+    d.ny, d.pad_y = 11, 0
+    assert L.cx_prop2d_workspace_size(d, b) == 2  # 11 x 1024: length 11 not compiled in
 
 
 def test_no_oracle_import_in_product():

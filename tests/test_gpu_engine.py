@@ -5,8 +5,8 @@ import pytest
 
 from tests.helpers import to_np
 
-SIZES = [2, 3, 4, 5, 6, 8, 10, 12, 16, 20, 24, 32, 40, 48, 64, 80, 96, 128, 160, 192, 256, 320, 384, 512, 640,
-         768, 1024, 1280, 1536, 2048, 2560, 3072, 4096]
+SIZES = [2, 3, 4, 5, 6, 7, 8, 10, 12, 14, 16, 20, 24, 28, 32, 40, 48, 56, 64, 80, 96, 112, 128, 160, 192, 224, 256,
+         320, 384, 448, 512, 640, 768, 896, 1024, 1280, 1536, 1792, 2048, 2560, 3072, 3584, 4096]
 
 
 @pytest.mark.gpu
@@ -36,6 +36,6 @@ def test_fft1d_unsupported_length_is_an_error():
 
     from chromatix_b200 import _native as nat
 
-    x = torch.zeros(7 * 11, dtype=torch.complex64, device="cuda")
+    x = torch.zeros(11 * 13, dtype=torch.complex64, device="cuda")
     with pytest.raises(nat.CxError):
-        nat.check(nat.lib().cx_fft1d(nat.ptr(x), nat.ptr(x), 77, 1, 0, nat.stream_handle()))
+        nat.check(nat.lib().cx_fft1d(nat.ptr(x), nat.ptr(x), 143, 1, 0, nat.stream_handle()))

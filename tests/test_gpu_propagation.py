@@ -185,6 +185,6 @@ def test_unsupported_sizes_fail_loudly():
     import chromatix_b200.functional as cf
     from chromatix_b200 import _native as nat
 
-    u = rand_field((7, 11), seed=10)
+    u = rand_field((11, 13), seed=10)
     with pytest.raises(nat.CxError):
         cf.asm_propagate(cuda_field(u, 0.1, 0.5), 1.0, 1.0, 0)
