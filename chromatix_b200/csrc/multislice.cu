@@ -11,6 +11,16 @@ struct MsPlan {
   Prop2DArgs col;  // column pass template (plane pointer set per launch)
 };
 
+// The slice propagator H(dz) is applied 2D times (and conj(H) D times in the
+// adjoint): it is evaluated once per call into a table with FP64 sin/cos
+// (correctly rounded to complex64), so its rounding does not accumulate
+// across slices, and read back from L2 by every column pass.
+__global__ void k_ms_fill_h(float2* __restrict__ H, Prop2DArgs a, cx_plane pl) {
+  const long total = (long)a.py * a.px;
+  for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < total; i += (long)gridDim.x * blockDim.x)
+    H[i] = prop_kernel(i / a.px, i % a.px, a, pl);
+}
+
 static cx_status ms_plan(const cx_ms_desc* d, MsPlan* p) {
   if (!d || d->ny <= 0 || d->nx <= 0 || d->pad < 0 || d->n_slices <= 0 || !(d->wavelength > 0.0) ||
       !(d->dy > 0.0) || !(d->dx > 0.0) || d->precision < 0 || d->precision > 1) {
@@ -58,10 +68,10 @@ static cx_status ms_plan(const cx_ms_desc* d, MsPlan* p) {
 
 static size_t al(size_t b) { return (b + 255) & ~(size_t)255; }
 
-// workspace: [planes (4 x cx_plane)] [F state] ([G state] [K records] for the adjoint)
+// workspace: [planes (4 x cx_plane)] [H table] [F state] ([G state] [K records] for the adjoint)
 static size_t ms_ws(const MsPlan& p, bool grad) {
   const size_t field = sizeof(float2) * (size_t)p.py * p.px;
-  size_t b = al(4 * sizeof(cx_plane)) + al(field);
+  size_t b = al(4 * sizeof(cx_plane)) + 2 * al(field);
   if (grad) b += al(field) + (size_t)p.K * al(field);
   return b;
 }
@@ -116,18 +126,50 @@ static cx_status ms_upload_planes(const cx_ms_desc* d, const MsPlan& p, cx_plane
   return CX_OK;
 }
 
-// slice_prop: the per-slice propagator (band limit / evanescent options of the
-// call); otherwise the plain ASM defocus kernel (samples.py:268-270)
+// slice_prop: the per-slice propagator, read from the H table (conjugated for
+// the adjoint); otherwise the plain ASM defocus kernel evaluated on the fly
+// (samples.py:268-270)
 static cx_status col_pass(const MsPlan& p, const cx_plane* plane, float2* buf, double na_f2, bool slice_prop,
-                          cudaStream_t st) {
+                          cudaStream_t st, const float2* Htab = nullptr, bool conj_h = false) {
   Prop2DArgs a = p.col;
   a.planes = plane;
   a.na_f2 = na_f2;
-  if (!slice_prop) {
+  if (slice_prop) {
+    a.kernel = CX_KERNEL_EXPLICIT;
+    a.H = Htab;
+    a.conj_h = conj_h ? 1 : 0;
+  } else {
     a.bandlimit = 0;
     a.remove_evanescent = 0;
   }
   return dispatch_cols(p.py, buf, buf, a, st);
+}
+
+static cx_status fill_h(const cx_ms_desc* d, const MsPlan& p, float2* H, cudaStream_t st) {
+  Prop2DArgs a = p.col;
+  a.precise = 1;
+  cx_plane pl = cx_plane{};
+  pl.z = d->dz;
+  pl.wavelength = d->wavelength;
+  pl.dy = d->dy;
+  pl.dx = d->dx;
+  if (d->bandlimit) {
+    // Matsushima band limit, shift 0 (propagation.py:557-579): centre 0, half width k
+    const double ext[2] = {d->dy * p.py, d->dx * p.px};
+    double km[2];
+    for (int i = 0; i < 2; ++i) {
+      const double half_period = ext[i] / 2.0;  // 1 / (2 df)
+      km[i] = std::pow(std::pow(half_period, -2.0) * pl.z * pl.z + 1.0, -0.5) / d->wavelength;
+    }
+    pl.bl_hy = km[0];
+    pl.bl_hx = km[1];
+  }
+  long total = (long)p.py * p.px;
+  int grid = (int)((total + 255) / 256);
+  if (grid > sm_count() * 8) grid = sm_count() * 8;
+  k_ms_fill_h<<<grid, 256, 0, st>>>(H, a, pl);
+  CX_LAUNCH_CHECK();
+  return CX_OK;
 }
 
 static double na_mask(const cx_ms_desc* d) {
@@ -171,11 +213,13 @@ extern "C" cx_status cx_multislice_forward(const cx_ms_desc* d, const void* u_in
   }
   cudaStream_t st = static_cast<cudaStream_t>(stream);
   char* w = static_cast<char*>(workspace);
-  cx_plane* planes = reinterpret_cast<cx_plane*>(w);
-  float2* F = reinterpret_cast<float2*>(w + al(4 * sizeof(cx_plane)));
-  float2* ck = static_cast<float2*>(checkpoints);
   const size_t field = (size_t)p.py * p.px;
+  cx_plane* planes = reinterpret_cast<cx_plane*>(w);
+  float2* Htab = reinterpret_cast<float2*>(w + al(4 * sizeof(cx_plane)));
+  float2* F = reinterpret_cast<float2*>(w + al(4 * sizeof(cx_plane)) + al(sizeof(float2) * field));
+  float2* ck = static_cast<float2*>(checkpoints);
   if ((s = ms_upload_planes(d, p, planes, st)) != CX_OK) return s;
+  if ((s = fill_h(d, p, Htab, st)) != CX_OK) return s;
   MsArgs a = ms_args(d, p);
   a.dn = dn;
   a.ab = ab;
@@ -190,14 +234,14 @@ extern "C" cx_status cx_multislice_forward(const cx_ms_desc* d, const void* u_in
   a.record = ck ? 1 : 0;
   a.rec = ck;
   if ((s = ms_dispatch_rows(p.px, a, st)) != CX_OK) return s;
-  if ((s = col_pass(p, planes + 0, F, -1.0, true, st)) != CX_OK) return s;
+  if ((s = col_pass(p, planes + 0, F, -1.0, true, st, Htab)) != CX_OK) return s;
   a.mode = MS_FWD;
   for (int i = 1; i <= p.D; ++i) {
     a.slice = i - 1;  // u_i = t_{i-1} P(u_{i-1})
     a.record = (ck && i < p.D && i % p.K == 0) ? 1 : 0;
     a.rec = a.record ? ck + (size_t)(i / p.K) * field : nullptr;
     if ((s = ms_dispatch_rows(p.px, a, st)) != CX_OK) return s;
-    if (i < p.D && (s = col_pass(p, planes + 0, F, -1.0, true, st)) != CX_OK) return s;
+    if (i < p.D && (s = col_pass(p, planes + 0, F, -1.0, true, st, Htab)) != CX_OK) return s;
   }
   // defocus back to the chosen plane, NA mask, crop (samples.py:265-282)
   if ((s = col_pass(p, planes + 2, F, na_mask(d), false, st)) != CX_OK) return s;
@@ -227,6 +271,8 @@ extern "C" cx_status cx_multislice_backward(const cx_ms_desc* d, const float* dn
   char* w = static_cast<char*>(workspace);
   cx_plane* planes = reinterpret_cast<cx_plane*>(w);
   w += al(4 * sizeof(cx_plane));
+  float2* Htab = reinterpret_cast<float2*>(w);
+  w += al(sizeof(float2) * field);
   float2* F = reinterpret_cast<float2*>(w);
   w += al(sizeof(float2) * field);
   float2* G = reinterpret_cast<float2*>(w);
@@ -235,6 +281,7 @@ extern "C" cx_status cx_multislice_backward(const cx_ms_desc* d, const float* dn
   const size_t seg_stride = al(sizeof(float2) * field) / sizeof(float2);
   const float2* ck = static_cast<const float2*>(checkpoints);
   if ((s = ms_upload_planes(d, p, planes, st)) != CX_OK) return s;
+  if ((s = fill_h(d, p, Htab, st)) != CX_OK) return s;
 
   MsArgs g = ms_args(d, p);
   g.dn = dn;
@@ -266,14 +313,14 @@ extern "C" cx_status cx_multislice_backward(const cx_ms_desc* d, const float* dn
     f.ox = 0;
     f.record = 0;
     if ((s = ms_dispatch_rows(p.px, f, st)) != CX_OK) return s;
-    if ((s = col_pass(p, planes + 0, F, -1.0, true, st)) != CX_OK) return s;
+    if ((s = col_pass(p, planes + 0, F, -1.0, true, st, Htab)) != CX_OK) return s;
     f.mode = MS_FWD;
     for (int i = i0 + 1; i <= i1; ++i) {
       f.slice = i - 1;
       f.record = 1;
       f.rec = seg + (size_t)(i - i0 - 1) * seg_stride;
       if ((s = ms_dispatch_rows(p.px, f, st)) != CX_OK) return s;
-      if (i < i1 && (s = col_pass(p, planes + 0, F, -1.0, true, st)) != CX_OK) return s;
+      if (i < i1 && (s = col_pass(p, planes + 0, F, -1.0, true, st, Htab)) != CX_OK) return s;
     }
     // adjoint through slices i1-1 .. i0
     g.mode = MS_BWD;
@@ -283,7 +330,7 @@ extern "C" cx_status cx_multislice_backward(const cx_ms_desc* d, const float* dn
       g.gdn = grad_dn + (size_t)i * d->ny * d->nx;
       g.gab = grad_ab + (size_t)i * d->ny * d->nx;
       if ((s = ms_dispatch_rows(p.px, g, st)) != CX_OK) return s;
-      if ((s = col_pass(p, planes + 1, G, -1.0, true, st)) != CX_OK) return s;
+      if ((s = col_pass(p, planes + 1, G, -1.0, true, st, Htab, true)) != CX_OK) return s;
     }
   }
   if (grad_u_in) {

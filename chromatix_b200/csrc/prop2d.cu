@@ -60,6 +60,8 @@ static cx_status make_args(const cx_prop2d_desc* d, Prop2DArgs* a) {
   a->ky0 = d->ky0;
   a->kx0 = d->kx0;
   a->na_f2 = -1.0;
+  a->precise = 0;
+  a->conj_h = 0;
   a->twg = nullptr;
   a->planes = nullptr;
   a->H = nullptr;

@@ -22,6 +22,8 @@ struct Prop2DArgs {
   int kernel, precision, remove_evanescent, bandlimit;
   double n_med, ky0, kx0;
   double na_f2;  // >= 0: k-space NA mask |f|^2 <= na_f2 (samples.py:276-280); < 0: none
+  int precise;   // 1: FP64 sin/cos (tables reused many times); 0: FP64 reduction + hardware sin/cos
+  int conj_h;    // 1: use conj(H) (explicit propagator tables, adjoint passes)
   const cx_plane* planes;
   const float2* H;
   const float2* twg;  // device twiddle tables (ensure_twiddles)
@@ -33,7 +35,8 @@ struct Prop2DArgs {
 __device__ __forceinline__ float2 prop_kernel_accurate(int ky, int kx, const Prop2DArgs& a, const cx_plane& pl) {
   const double pi = 3.141592653589793238462643383279502884;
   const double K = 2.0 * pi * fabs(pl.z) * a.n_med / pl.wavelength;  // largest ASM phase (rad)
-  if (a.kernel == CX_KERNEL_ASM && K <= 8.0 && !a.bandlimit && pl.shift_y == 0.0 && pl.shift_x == 0.0) {
+  if (!a.precise && a.kernel == CX_KERNEL_ASM && K <= 8.0 && !a.bandlimit && pl.shift_y == 0.0 &&
+      pl.shift_x == 0.0) {
     // Short distances (thin slices): every phase term is below 8 rad, so FP32
     // evaluation keeps the phase error below ~2e-6 rad -- inside the accuracy
     // budget -- at a fraction of the FP64 cost.
@@ -58,7 +61,13 @@ __device__ __forceinline__ float2 prop_kernel_accurate(int ky, int kx, const Pro
   const double s = gy * gy + gx * gx;
   if (a.kernel == CX_KERNEL_TRANSFER) {
     // phase = -pi lam / n z |f - kykx|^2  (propagation.py:493-496)
-    return expi_reduced(-pi * pl.wavelength / a.n_med * pl.z * s);
+    const double ph = -pi * pl.wavelength / a.n_med * pl.z * s;
+    if (a.precise) {
+      double sd, cd;
+      sincos(ph, &sd, &cd);
+      return make_float2((float)cd, (float)sd);
+    }
+    return expi_reduced(ph);
   }
   if (a.bandlimit && (fabs(fy - pl.bl_y0) > pl.bl_hy || fabs(fx - pl.bl_x0) > pl.bl_hx)) return make_float2(0.f, 0.f);
   const double q = pl.wavelength / a.n_med;
@@ -72,6 +81,11 @@ __device__ __forceinline__ float2 prop_kernel_accurate(int ky, int kx, const Pro
     ph = sh;
   }
   if (pl.z < 0.0) ph = -ph;  // conj(exp(i phase)) keeps the decay (propagation.py:556)
+  if (a.precise) {
+    double sd, cd;
+    sincos(ph, &sd, &cd);
+    return make_float2((float)(amp * cd), (float)(amp * sd));
+  }
   float2 e = expi_reduced(ph);
   return make_float2((float)amp * e.x, (float)amp * e.y);
 }
@@ -120,8 +134,10 @@ __device__ __forceinline__ bool outside_na(int ky, int kx, const Prop2DArgs& a, 
 
 __device__ __forceinline__ float2 prop_kernel(int ky, int kx, const Prop2DArgs& a, const cx_plane& pl) {
   if (outside_na(ky, kx, a, pl)) return make_float2(0.f, 0.f);
-  if (a.kernel == CX_KERNEL_EXPLICIT)
-    return a.H[((size_t)pl.h_plane * a.py + ky) * a.px + kx];
+  if (a.kernel == CX_KERNEL_EXPLICIT) {
+    const float2 h = a.H[((size_t)pl.h_plane * a.py + ky) * a.px + kx];
+    return a.conj_h ? cconj(h) : h;
+  }
   return a.precision == CX_PREC_REF32 ? prop_kernel_ref32(ky, kx, a, pl) : prop_kernel_accurate(ky, kx, a, pl);
 }
 
