@@ -63,6 +63,31 @@ extern "C" cx_status cx_optical_fft(const cx_optfft_desc* d, const cx_fft_plane*
     return CX_ERR_WORKSPACE;
   }
   a.planes = planes_dev;
+  a.H = nullptr;
+  if ((s = ensure_twiddles(&a.twg)) != CX_OK) return s;
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  float2* T = static_cast<float2*>(workspace);
+  if ((s = opt_dispatch_rows(a.px, static_cast<const float2*>(u_in), T, a, st)) != CX_OK) return s;
+  return opt_dispatch_cols(a.py, T, static_cast<float2*>(u_out), a, st);
+}
+
+extern "C" cx_status cx_optical_fft_h(const cx_optfft_desc* d, const cx_fft_plane* planes_dev, const void* H,
+                                      const void* u_in, void* u_out, void* workspace, size_t workspace_bytes,
+                                      cx_stream_t stream) {
+  OptArgs a;
+  cx_status s = opt_args(d, &a);
+  if (s != CX_OK) return s;
+  if (!planes_dev || !H || !u_in || !u_out || !workspace) {
+    set_error("null pointer argument");
+    return CX_ERR_INVALID;
+  }
+  const size_t need = sizeof(float2) * (size_t)a.n_out_planes * a.py * a.px;
+  if (workspace_bytes < need) {
+    set_error("workspace too small: %zu < %zu", workspace_bytes, need);
+    return CX_ERR_WORKSPACE;
+  }
+  a.planes = planes_dev;
+  a.H = static_cast<const float2*>(H);
   if ((s = ensure_twiddles(&a.twg)) != CX_OK) return s;
   cudaStream_t st = static_cast<cudaStream_t>(stream);
   float2* T = static_cast<float2*>(workspace);

@@ -17,6 +17,7 @@ struct OptArgs {
   int ny, nx, pad_y, pad_x, py, px, crop_y, crop_x, oy_n, ox_n, W;
   int n_in_planes, n_out_planes, precision;
   const cx_fft_plane* planes;
+  const float2* H;  // optional propagator table (planar, FFT order), multiplied before the fftshift
   const float2* twg;  // device twiddle tables (ensure_twiddles)
 };
 

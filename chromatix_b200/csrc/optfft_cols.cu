@@ -33,8 +33,10 @@ __global__ void __launch_bounds__(ColCfg<NY>::THREADS, ColCfg<NY>::MINB) k_opt_c
     auto load = [&](int n) -> float2 { return s[pad_idx(n)]; };
     // the tile stays in FFT order (the staged store updates it in place);
     // the fftshift along y is applied by the final copy
+    const float2* hcol = a.H ? a.H + (size_t)q * a.py * a.px + kx : nullptr;
     auto store = [&](int k, float2 v, int) {
       const int row = (k + a.py / 2) % a.py;  // output row of bin k (fftshift along y)
+      if (hcol && kx < a.px) v = cmul(v, hcol[(size_t)k * a.px]);
       if (pl.conj) v = cconj(v);
       v = cmul(post, v);
       if (pl.chirp_out != 0.0) {

@@ -254,11 +254,12 @@ def kernel_propagate(field: Field, propagator, absorbing_boundary=None, absorbin
 
 
 def _fill_propagator(field: Field, kernel: int, z, n, kykx, shift_yx=(0.0, 0.0), bandlimit=False,
-                     remove_evanescent=False, precision=None, zshape_rule="asm"):
+                     remove_evanescent=False, precision=None, shape=None):
+    """Propagator for ``field`` (or for a grid of ``shape`` with the field's spacing)."""
     torch = nat.torch_mod()
     prec = precision or config.get_precision()
     zs, zshape = _z_array(z)
-    ny, nx = field.spatial_shape
+    ny, nx = field.spatial_shape if shape is None else (int(shape[0]), int(shape[1]))
     W = field.n_wv
     # one plane per (z, wv): the propagator does not depend on the field batch
     planes, out_batch, _, nb_out = _plan_planes(field, zs, zshape, ny, nx, shift_yx, bandlimit, prec,

@@ -193,6 +193,12 @@ cx_status cx_optfft_workspace_size(const cx_optfft_desc* d, size_t* bytes);
  * (n_out_planes/n_wv, ny + 2 pad_y - 2 crop_y, nx + 2 pad_x - 2 crop_x, n_wv). */
 cx_status cx_optical_fft(const cx_optfft_desc* d, const cx_fft_plane* planes_dev, const void* u_in, void* u_out,
                          void* workspace, size_t workspace_bytes, cx_stream_t stream);
+/* Same, with a propagator table H (planar (n_out_planes, py, px), FFT order)
+ * multiplied into the spectrum before the fftshift: with pre = post = 1 this
+ * is fftshift(H * fft2(ifftshift(pad(u)))), the spectrum the CZT branch of
+ * kernel_propagate starts from (functional/propagation.py:414-418). */
+cx_status cx_optical_fft_h(const cx_optfft_desc* d, const cx_fft_plane* planes_dev, const void* H, const void* u_in,
+                           void* u_out, void* workspace, size_t workspace_bytes, cx_stream_t stream);
 
 /* ---------------------------------------------------------------------------
  * Thick-sample multislice, forward and adjoint
@@ -228,6 +234,31 @@ cx_status cx_multislice_forward(const cx_ms_desc* d, const void* u_in, const flo
 cx_status cx_multislice_backward(const cx_ms_desc* d, const float* dn, const float* abs_, const void* checkpoints,
                                  const void* grad_out, float* grad_dn, float* grad_abs, void* grad_u_in,
                                  void* workspace, size_t workspace_bytes, cx_stream_t stream);
+
+/* ---------------------------------------------------------------------------
+ * Chirp-Z transform along one axis (Bluestein)
+ *   czt / cztn / zoomed_fft (utils/czt.py:7-124) and the CZT branch of
+ *   kernel_propagate (functional/propagation.py:420-443)
+ * y[k] = scale [w^(-N k) a^N] sum_j x[j] a^(-j) w^(j k),  k < m
+ * Vectors v = o * inner + i; element j of vector v at
+ * x + o*in_ostride + i*in_istride + j*in_estride (likewise for y, k).
+ * ------------------------------------------------------------------------- */
+typedef struct {
+  int32_t n, m;        /* input / output length */
+  int32_t L;           /* FFT length >= n + m - 1 (0: smallest compiled length) */
+  int32_t inner;       /* vectors per outer index */
+  int64_t n_vec;
+  int64_t in_ostride, in_istride, in_estride;
+  int64_t out_ostride, out_istride, out_estride;
+  double a_re, a_im, w_re, w_im;
+  int32_t mod_n;       /* >= 0: multiply output k by w^(-mod_n k) a^mod_n */
+  int32_t layout;      /* 0: one team per vector; 1: column tiles (unit inner strides) */
+  double scale;
+} cx_czt_desc;
+
+cx_status cx_czt_workspace_size(const cx_czt_desc* d, size_t* bytes);
+cx_status cx_czt(const cx_czt_desc* d, const void* x, void* y, void* workspace, size_t workspace_bytes,
+                 cx_stream_t stream);
 
 /* Field.intensity (core/field.py:656-665, 735-740): out[b, y, x] =
  * sum_wv density[wv] |u[b, y, x, wv]|^2.  density_dev: n_wv doubles. */
