@@ -1,0 +1,252 @@
+// Modified Born series: the preconditioned fixed-point iteration on a 3D grid.
+//
+// Reference: experimental/modified_born_series/solver.py:42-146 and
+// sample.py:9-124.  With V(y) = y * (s eps - kb2) (shifted_discrepancy),
+// G(y) = IFFT3[ Y_T / (kb2 - s |k|^2) + Y_L / kb2 ] (shifted_approx_inv,
+// k normalised by k0, Y_L = k (k.Y)/|k|^2, Y_T = Y - Y_L) one iteration is
+//   x <- prec_y - prec_forward(x) + x = prec_y + V(G(V x) + x) + x.
+// The state is three component planes (X, Y, Z) complex64.  Passes:
+//   Z  (lines along z)    load x, V x, FFT_z
+//   Y  (column tiles)     FFT_y / IFFT_y in place
+//   X  (column tiles, 3 components per CTA) FFT_x, k-space projection and
+//      Green's-function division, IFFT_x
+//   Zi (lines along z)    IFFT_z / (X Y Z) -> G; x_new = prec_y + V(G + x) + x,
+//      FP64 partial sums of |x_new - x|^2 and |x_new|^2
+#pragma once
+
+#include "host.cuh"
+
+namespace cx {
+
+enum MbsZMode {
+  MBS_Z_DISC = 0,   // buf = FFT_z(V x)                (forward operator input)
+  MBS_Z_SCALE = 1,  // buf = FFT_z(s * src)            (preconditioned source)
+  MBS_ZI_STEP = 2,  // x_new = prec_y + V(G + x) + x, residual sums
+  MBS_ZI_PREC = 3   // prec_y = -V(G)
+};
+
+struct MbsArgs {
+  int X, Y, Z;
+  long vox;           // X * Y * Z
+  float2 s, kb2;      // scale (1 / (1.1 i R)) and k_bias^2 = shift * scale + 1
+  float kfx, kfy, kfz;  // 2 pi / (N spacing k0) per axis: k' = kf * fftfreq numerator
+  const float2* eps;  // (X, Y, Z) permittivity
+  const float2* x;    // current iterate (3 planes) / source for MBS_Z_SCALE
+  const float2* prec_y;
+  float2* buf;        // FFT work state (3 planes)
+  float2* x_new;      // output (3 planes)
+  double* acc;        // [0] sum |x_new - x|^2, [1] sum |x_new|^2
+  const float2* twg;
+};
+
+__device__ __forceinline__ float2 mbs_disc(const MbsArgs& a, float2 v, float2 e) {
+  // v * (s * eps - kb2)
+  const float2 f = make_float2(a.s.x * e.x - a.s.y * e.y - a.kb2.x, a.s.x * e.y + a.s.y * e.x - a.kb2.y);
+  return cmul(v, f);
+}
+
+// lines along z: one team per (component, ix, iy)
+template <int NZ, int MODE>
+__global__ void __launch_bounds__(RowCfg<NZ>::THREADS, RowCfg<NZ>::MINB) k_mbs_z(MbsArgs a) {
+  using C = RowCfg<NZ>;
+  extern __shared__ float2 sm[];
+  float2* tw = sm;
+  load_twiddles<NZ>(tw, a.twg, threadIdx.x, blockDim.x);
+  __syncthreads();
+  const int team = threadIdx.x / C::LPV, lane = threadIdx.x % C::LPV;
+  float2* s = sm + C::TW + team * Plan<NZ>::LEN;
+  const long lines = 3L * a.X * a.Y;
+  const float inv_n = 1.0f / ((float)a.X * (float)a.Y * (float)a.Z);
+  double dsum = 0.0, nsum = 0.0;
+  for (long base = (long)blockIdx.x * C::TEAMS; base < lines; base += (long)gridDim.x * C::TEAMS) {
+    const long line = base + team;
+    if (line >= lines) continue;
+    const long comp = line / ((long)a.X * a.Y);
+    const long xy = line % ((long)a.X * a.Y);
+    const size_t off = (size_t)comp * a.vox + (size_t)xy * a.Z;
+    const float2* erow = a.eps + (size_t)xy * a.Z;
+    float2* brow = a.buf + off;
+    if constexpr (MODE == MBS_Z_DISC || MODE == MBS_Z_SCALE) {
+      const float2* xrow = a.x + off;
+      auto load = [&](int k) -> float2 {
+        return MODE == MBS_Z_DISC ? mbs_disc(a, xrow[k], erow[k]) : cmul(a.s, xrow[k]);
+      };
+      auto store = [&](int k, float2 v, int) { brow[k] = v; };
+      team_fft_ex<NZ, false, true, false>(s, tw, lane, team, load, store);
+    } else {
+      auto load = [&](int k) -> float2 { return brow[k]; };
+      if constexpr (MODE == MBS_ZI_STEP) {
+        const float2* xrow = a.x + off;
+        const float2* prow = a.prec_y + off;
+        float2* orow = a.x_new + off;
+        auto store = [&](int k, float2 g, int) {
+          const float2 xo = xrow[k];
+          const float2 gk = cscale(g, inv_n);
+          const float2 vx = mbs_disc(a, cadd(gk, xo), erow[k]);
+          const float2 xn = cadd(cadd(prow[k], vx), xo);
+          orow[k] = xn;
+          const float2 dd = csub(xn, xo);
+          dsum += (double)dd.x * dd.x + (double)dd.y * dd.y;
+          nsum += (double)xn.x * xn.x + (double)xn.y * xn.y;
+        };
+        team_fft_ex<NZ, true, false, true>(s, tw, lane, team, load, store);
+      } else {  // MBS_ZI_PREC: prec_y = -V(G)
+        float2* orow = a.x_new + off;
+        auto store = [&](int k, float2 g, int) {
+          const float2 v = mbs_disc(a, cscale(g, inv_n), erow[k]);
+          orow[k] = make_float2(-v.x, -v.y);
+        };
+        team_fft_ex<NZ, true, false, true>(s, tw, lane, team, load, store);
+      }
+    }
+  }
+  if constexpr (MODE == MBS_ZI_STEP) {
+    // block reduction of the FP64 residual sums, one atomic pair per CTA
+    __shared__ double red[2][32];
+    for (int o = 16; o > 0; o >>= 1) {
+      dsum += __shfl_xor_sync(0xffffffffu, dsum, o);
+      nsum += __shfl_xor_sync(0xffffffffu, nsum, o);
+    }
+    const int wid = threadIdx.x >> 5, nw = (blockDim.x + 31) >> 5;
+    if ((threadIdx.x & 31) == 0) {
+      red[0][wid] = dsum;
+      red[1][wid] = nsum;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      double d0 = 0.0, n0 = 0.0;
+      for (int w = 0; w < nw; ++w) {
+        d0 += red[0][w];
+        n0 += red[1][w];
+      }
+      atomicAdd(a.acc, d0);
+      atomicAdd(a.acc + 1, n0);
+    }
+  }
+}
+
+// column tiles along an axis of length N with element stride E: vectors
+// (outer o, inner i), element j at buf + o * ostride + i + j * E; in place
+template <int N, bool INV>
+__global__ void __launch_bounds__(ColCfg<N>::THREADS, ColCfg<N>::MINB) k_mbs_cols(MbsArgs a, long n_outer,
+                                                                                int inner, long ostride, long E) {
+  using C = ColCfg<N>;
+  constexpr int V = C::V, LEN = C::LEN;
+  extern __shared__ float2 sm[];
+  float2* tw = sm;
+  float2* tile = sm + C::TW;
+  load_twiddles<N>(tw, a.twg, threadIdx.x, blockDim.x);
+  const int team = threadIdx.x / C::LPV, lane = threadIdx.x % C::LPV;
+  float2* s = tile + team * LEN;
+  const int tiles_i = (inner + V - 1) / V;
+  const long total = (long)tiles_i * n_outer;
+  for (long t = blockIdx.x; t < total; t += gridDim.x) {
+    const long o = t / tiles_i;
+    const int i0 = (int)(t % tiles_i) * V;
+    float2* base = a.buf + o * ostride;
+    __syncthreads();
+    load_col_tile<V, LEN>(tile, base, E, i0, inner, 0, N, [](int r) { return r; });
+    __syncthreads();
+    auto load = [&](int j) -> float2 { return s[pad_idx(j)]; };
+    auto store = [&](int k, float2 v, int) { s[pad_idx(k)] = v; };
+    team_fft<N, INV>(s, tw, lane, team, load, store);
+    __syncthreads();
+    for (int idx = threadIdx.x; idx < N * V; idx += blockDim.x) {
+      const int r = idx / V, c = idx % V, i = i0 + c;
+      if (i < inner) base[(long)r * E + i] = tile[c * LEN + pad_idx(r)];
+    }
+  }
+}
+
+// along x for all three components at once (inner = Y*Z, E = Y*Z), with the
+// k-space projection / Green's-function division between FFT_x and IFFT_x
+template <int NX>
+struct MbsXCfg {
+  using C = ColCfg<NX>;
+  static constexpr int LPV = C::LPV;
+  // about 128 lanes per component (at least 4 columns), at most 1024 threads
+  static constexpr int V0 = LPV < 32 ? (128 / LPV > 4 ? 128 / LPV : 4) : 4;
+  static constexpr int V = (3 * V0 * LPV <= 1024) ? V0 : ((3 * 2 * LPV <= 1024) ? 2 : 1);
+  static constexpr int LEN = col_len(NX, V);
+  static constexpr int THREADS = 3 * V * LPV;
+  static constexpr int MINB = minb_for(THREADS);
+  static constexpr size_t SMEM = sizeof(float2) * ((size_t)C::TW + 3 * (size_t)V * LEN);
+};
+
+template <int NX>
+__global__ void __launch_bounds__(MbsXCfg<NX>::THREADS, MbsXCfg<NX>::MINB) k_mbs_x(MbsArgs a) {
+  using Q = MbsXCfg<NX>;
+  constexpr int V = Q::V, LEN = Q::LEN, LPV = Q::LPV;
+  extern __shared__ float2 sm[];
+  float2* tw = sm;
+  float2* tile = sm + ColCfg<NX>::TW;  // [comp][V][LEN]
+  load_twiddles<NX>(tw, a.twg, threadIdx.x, blockDim.x);
+  const int team = threadIdx.x / LPV, lane = threadIdx.x % LPV;  // team = comp * V + column
+  float2* s = tile + team * LEN;
+  const long inner = (long)a.Y * a.Z;
+  const long tiles = (inner + V - 1) / V;
+  for (long t = blockIdx.x; t < tiles; t += gridDim.x) {
+    const long i0 = t * V;
+    __syncthreads();
+    for (int c = 0; c < 3; ++c)
+      load_col_tile<V, LEN>(tile + c * V * LEN, a.buf + (size_t)c * a.vox, inner, (int)i0, (int)inner, 0, NX,
+                            [](int r) { return r; });
+    __syncthreads();
+    auto load = [&](int j) -> float2 { return s[pad_idx(j)]; };
+    auto store = [&](int k, float2 v, int) { s[pad_idx(k)] = v; };
+    team_fft<NX, false>(s, tw, lane, team, load, store);
+    __syncthreads();
+    // k-space operator, cooperatively over (kx, column)
+    for (int idx = threadIdx.x; idx < NX * V; idx += blockDim.x) {
+      const int kx = idx / V, c = idx % V;
+      const long i = i0 + c;
+      if (i >= inner) continue;
+      const int iy = (int)(i / a.Z), iz = (int)(i % a.Z);
+      const float kxv = a.kfx * (float)freq_index(kx, a.X);
+      const float kyv = a.kfy * (float)freq_index(iy, a.Y);
+      const float kzv = a.kfz * (float)freq_index(iz, a.Z);
+      const float ksq = kxv * kxv + kyv * kyv + kzv * kzv;
+      float2* p0 = tile + (0 * V + c) * LEN + pad_idx(kx);
+      float2* p1 = tile + (1 * V + c) * LEN + pad_idx(kx);
+      float2* p2 = tile + (2 * V + c) * LEN + pad_idx(kx);
+      const float2 y0 = *p0, y1 = *p1, y2 = *p2;
+      // longitudinal part k (k . y) / |k|^2 (zero at k = 0)
+      float2 l0 = make_float2(0.f, 0.f), l1 = l0, l2 = l0;
+      if (ksq != 0.f) {
+        const float2 proj = make_float2((kxv * y0.x + kyv * y1.x + kzv * y2.x) / ksq,
+                                        (kxv * y0.y + kyv * y1.y + kzv * y2.y) / ksq);
+        l0 = cscale(proj, kxv);
+        l1 = cscale(proj, kyv);
+        l2 = cscale(proj, kzv);
+      }
+      // 1 / (kb2 - s ksq) and 1 / kb2
+      const float2 dt = make_float2(a.kb2.x - a.s.x * ksq, a.kb2.y - a.s.y * ksq);
+      const float dn = dt.x * dt.x + dt.y * dt.y;
+      const float2 it = make_float2(dt.x / dn, -dt.y / dn);
+      const float bn = a.kb2.x * a.kb2.x + a.kb2.y * a.kb2.y;
+      const float2 il = make_float2(a.kb2.x / bn, -a.kb2.y / bn);
+      *p0 = cadd(cmul(csub(y0, l0), it), cmul(l0, il));
+      *p1 = cadd(cmul(csub(y1, l1), it), cmul(l1, il));
+      *p2 = cadd(cmul(csub(y2, l2), it), cmul(l2, il));
+    }
+    __syncthreads();
+    team_fft<NX, true>(s, tw, lane, team, load, store);
+    __syncthreads();
+    for (int c = 0; c < 3; ++c) {
+      float2* dst = a.buf + (size_t)c * a.vox;
+      const float2* src = tile + c * V * LEN;
+      for (int idx = threadIdx.x; idx < NX * V; idx += blockDim.x) {
+        const int r = idx / V, cc = idx % V;
+        const long i = i0 + cc;
+        if (i < inner) dst[(long)r * inner + i] = src[cc * LEN + pad_idx(r)];
+      }
+    }
+  }
+}
+
+cx_status mbs_dispatch_z(int n, int mode, const MbsArgs& a, cudaStream_t st);
+cx_status mbs_dispatch_cols(int n, bool inv, const MbsArgs& a, long n_outer, int inner, long ostride, long E,
+                            cudaStream_t st);
+cx_status mbs_dispatch_x(int n, const MbsArgs& a, cudaStream_t st);
+
+}  // namespace cx

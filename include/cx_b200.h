@@ -260,6 +260,27 @@ cx_status cx_czt_workspace_size(const cx_czt_desc* d, size_t* bytes);
 cx_status cx_czt(const cx_czt_desc* d, const void* x, void* y, void* workspace, size_t workspace_bytes,
                  cx_stream_t stream);
 
+/* ---------------------------------------------------------------------------
+ * Modified Born series (experimental/modified_born_series/solver.py:42-146)
+ * Grid (X, Y, Z); fields are three component planes (3, X, Y, Z) complex64;
+ * eps (X, Y, Z) complex64.  s = 1 / (1.1 i R) and kb2 = shift * s + 1 are the
+ * preconditioner's scale and k_bias^2 (solver.py:64-65).
+ * ------------------------------------------------------------------------- */
+typedef struct {
+  int32_t X, Y, Z;
+  double spacing, k0;
+  double s_re, s_im, kb2_re, kb2_im;
+} cx_mbs_desc;
+
+cx_status cx_mbs_workspace_size(const cx_mbs_desc* d, size_t* bytes);
+/* prec_y = -V(G(s * src)) (solver.py:87-96, before the num_scale division) */
+cx_status cx_mbs_precondition(const cx_mbs_desc* d, const void* eps, const void* src, void* prec_y, void* workspace,
+                              size_t workspace_bytes, cx_stream_t stream);
+/* x_new = prec_y - prec_forward(x) + x (solver.py:91-93, 136-142);
+ * acc (device, 2 doubles) = (sum |x_new - x|^2, sum |x_new|^2), FP64. */
+cx_status cx_mbs_iterate(const cx_mbs_desc* d, const void* eps, const void* prec_y, const void* x, void* x_new,
+                         double* acc, void* workspace, size_t workspace_bytes, cx_stream_t stream);
+
 /* Field.intensity (core/field.py:656-665, 735-740): out[b, y, x] =
  * sum_wv density[wv] |u[b, y, x, wv]|^2.  density_dev: n_wv doubles. */
 cx_status cx_intensity(const void* u, int64_t n_pix, int32_t n_wv, const double* density_dev, float* out,
