@@ -1,5 +1,6 @@
 // C API of the chirp-Z transform (kernels in czt.cuh).
 #include <cmath>
+#include <mutex>
 
 #include "czt.cuh"
 
@@ -93,6 +94,74 @@ extern "C" cx_status cx_czt(const cx_czt_desc* d, const void* x, void* y, void* 
   cudaStream_t st = static_cast<cudaStream_t>(stream);
   if ((s = ensure_twiddles(&a.twg)) != CX_OK) return s;
   float2* c = static_cast<float2*>(workspace);
+  float2* chat = c + a.L;
+  k_czt_filter<<<(a.L + 255) / 256, 256, 0, st>>>(c, a.n, a.m, a.L, a.tw, a.lw);
+  CX_LAUNCH_CHECK();
+  if ((s = cx_fft1d(c, chat, a.L, 1, 0, stream)) != CX_OK) return s;
+  a.chat = chat;
+  a.x = static_cast<const float2*>(x);
+  a.y = static_cast<float2*>(y);
+  return d->layout == 1 ? czt_dispatch_cols(a.L, a, st) : czt_dispatch_rows(a.L, a, st);
+}
+
+// ---------------------------------------------------------------------------
+// cx_czt_noalloc: the same transform with its scratch in a static device buffer
+// ---------------------------------------------------------------------------
+
+namespace cx {
+
+// chirp filter (L entries) followed by its spectrum (L entries); 64 KiB.
+// Every entry a call reads is written earlier in the same call (the filter
+// kernel writes zeros past n + m - 1), so nothing has to start at zero.
+constexpr int kCztNoAllocMaxL = 4096;
+static __device__ __align__(256) float2 g_czt_scratch[2 * kCztNoAllocMaxL];
+
+// Address of g_czt_scratch on the current device, looked up once per device.
+static cx_status czt_noalloc_scratch(float2** out) {
+  static std::mutex mu;
+  static float2* addr[64] = {nullptr};
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) {
+    set_error("cx_czt_noalloc: no current CUDA device");
+    return CX_ERR_CUDA;
+  }
+  std::lock_guard<std::mutex> lock(mu);
+  if (!addr[dev]) {
+    void* p = nullptr;
+    const cudaError_t e = cudaGetSymbolAddress((void**)&p, g_czt_scratch);
+    if (e != cudaSuccess || !p) {
+      set_error("cx_czt_noalloc: cudaGetSymbolAddress of the static scratch failed: %s", cudaGetErrorString(e));
+      return CX_ERR_CUDA;
+    }
+    addr[dev] = static_cast<float2*>(p);
+  }
+  *out = addr[dev];
+  return CX_OK;
+}
+
+}  // namespace cx
+
+extern "C" cx_status cx_czt_noalloc(const cx_czt_desc* d, const void* x, void* y, cx_stream_t stream) {
+  if (d && (d->L > kCztNoAllocMaxL || (int64_t)d->n + d->m - 1 > kCztNoAllocMaxL)) {
+    set_error("cx_czt_noalloc: FFT length %d (n + m - 1 = %lld) exceeds the static scratch, which holds L <= %d",
+              d->L, (long long)d->n + d->m - 1, kCztNoAllocMaxL);
+    return CX_ERR_UNSUPPORTED;
+  }
+  CztArgs a;
+  cx_status s = czt_args(d, &a);
+  if (s != CX_OK) return s;
+  if (a.L > kCztNoAllocMaxL) {
+    set_error("cx_czt_noalloc: FFT length %d exceeds the static scratch, which holds L <= %d", a.L, kCztNoAllocMaxL);
+    return CX_ERR_UNSUPPORTED;
+  }
+  if (!x || !y) {
+    set_error("null pointer argument");
+    return CX_ERR_INVALID;
+  }
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  if ((s = ensure_twiddles(&a.twg)) != CX_OK) return s;
+  float2* c = nullptr;
+  if ((s = czt_noalloc_scratch(&c)) != CX_OK) return s;
   float2* chat = c + a.L;
   k_czt_filter<<<(a.L + 255) / 256, 256, 0, st>>>(c, a.n, a.m, a.L, a.tw, a.lw);
   CX_LAUNCH_CHECK();

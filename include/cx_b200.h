@@ -260,6 +260,25 @@ cx_status cx_czt_workspace_size(const cx_czt_desc* d, size_t* bytes);
 cx_status cx_czt(const cx_czt_desc* d, const void* x, void* y, void* workspace, size_t workspace_bytes,
                  cx_stream_t stream);
 
+/* cx_czt without a workspace argument; allocates no device memory.  No
+ * counterpart in the reference: its czt (utils/czt.py:7-52) is a traced JAX
+ * function whose temporaries XLA places.  This entry point is for callers that
+ * can neither allocate device memory nor hand out scratch, e.g. a
+ * foreign-function handler running under a framework that owns the whole
+ * device pool and offers no allocator for temporaries.
+ *  - The chirp filter and its spectrum live in one static 64 KiB device
+ *    buffer inside the library: FFT lengths L <= 4096 (n + m - 1 <= 4096);
+ *    larger requests return CX_ERR_UNSUPPORTED with a message.
+ *  - The first call on each device (with that device current) uploads the
+ *    twiddle table and looks up the buffer's address with synchronous runtime
+ *    calls; make that first call (or cx_init plus one call) before any stream
+ *    capture begins.
+ *  - Every call on a device uses the same buffer: calls that can overlap in
+ *    time (streams without ordering between them, several host threads)
+ *    race on it and must be serialised by the caller.
+ *  - Results are identical to cx_czt's for the same descriptor and input. */
+cx_status cx_czt_noalloc(const cx_czt_desc* d, const void* x, void* y, cx_stream_t stream);
+
 /* ---------------------------------------------------------------------------
  * Modified Born series (experimental/modified_born_series/solver.py:42-146)
  * Grid (X, Y, Z); fields are three component planes (3, X, Y, Z) complex64;
