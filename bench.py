@@ -216,14 +216,14 @@ def gpu_arm(args):
         # attributed to the row pass
         alg_bytes = kern["zc"] * N * N * 4
         achieved = alg_bytes / (kern["ms"] * 1e-3) / 1e9
+        # DRAM bytes of one column-pass launch from the committed ncu summary
+        # (read + write per z-plane, scaled to this launch's z-planes)
         traffic = None
-        tp = os.path.join(ROOT, "profiles", "psf_cols_1280.traffic.json")
+        tp = os.path.join(ROOT, "profiles", "psf_4f_1280_bench.md")
         if os.path.exists(tp):
-            try:
-                tj = _json.load(open(tp))
-                traffic = tj["dram_bytes_per_z"] * kern["zc"]
-            except Exception:
-                traffic = None
+            for ln in open(tp):
+                if ln.startswith("traffic_bytes_per_z_plane:"):
+                    traffic = int(ln.split(":")[1]) * kern["zc"]
         # FP32 work of the pipeline (5 N log2 N per complex FFT of N points)
         rows_ffts = NZ * kern["rowsum"]
         cols_ffts = NZ * NWV * N
