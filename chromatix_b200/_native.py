@@ -231,6 +231,20 @@ def to_device_bytes(arr: np.ndarray, device):
     return torch.from_numpy(b.copy()).to(device, non_blocking=False)
 
 
+_copy_streams = {}
+
+
+def copy_stream(device):
+    """A side stream per device for device-to-host result copies."""
+    torch = torch_mod()
+    dev = torch.device(device)
+    idx = dev.index if dev.index is not None else torch.cuda.current_device()
+    s = _copy_streams.get(idx)
+    if s is None:
+        s = _copy_streams[idx] = torch.cuda.Stream(device=idx)
+    return s
+
+
 def require_cuda(t, what="tensor"):
     if not t.is_cuda:
         raise ValueError(f"{what} must live on a CUDA device (the library has no CPU path)")

@@ -208,6 +208,17 @@ class Field:
                                          nat.stream_handle(u.device)))
         return out
 
+    def intensity_to(self, out):
+        """Write the intensity into ``out`` (a float32 tensor of the intensity's
+        shape, on the device or in host memory) and return ``out``.  Host
+        output is copied asynchronously when ``out`` is page-locked; it is
+        valid once the current stream has been synchronised."""
+        I = self.intensity
+        if tuple(out.shape) != tuple(I.shape):
+            raise ValueError(f"out has shape {tuple(out.shape)}, the intensity {tuple(I.shape)}")
+        out.copy_(I, non_blocking=True)
+        return out
+
     @property
     def power(self):
         """area * sum over (y, x) of the intensity (core/field.py:656-661, 728-733)."""

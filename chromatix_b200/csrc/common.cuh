@@ -22,6 +22,12 @@ __device__ __forceinline__ float2 mul_mi(float2 a) {
 }
 __device__ __forceinline__ float cabs2(float2 a) { return a.x * a.x + a.y * a.y; }
 
+// (n + s) mod m for 0 <= n < m and 0 <= s < m, without an integer division
+__host__ __device__ __forceinline__ int add_mod(int n, int s, int m) {
+  const int t = n + s;
+  return t >= m ? t - m : t;
+}
+
 // fftfreq numerator of FFT bin k for length n (numpy/jax convention).
 __host__ __device__ __forceinline__ int freq_index(int k, int n) { return k < (n + 1) / 2 ? k : k - n; }
 
@@ -39,6 +45,14 @@ __device__ __forceinline__ float2 expi_reduced(double ph) {
   float s, c;
   __sincosf(reduce_phase(ph), &s, &c);
   return make_float2(c, s);
+}
+
+// exp(i ph) with FP64 sin/cos, rounded once to float: for values that are
+// evaluated once and reused (tables, per-row factors)
+__device__ __forceinline__ float2 expi_precise(double ph) {
+  double s, c;
+  sincos(ph, &s, &c);
+  return make_float2((float)c, (float)s);
 }
 
 // Cast helpers that block FMA contraction, for the float32 reference-order

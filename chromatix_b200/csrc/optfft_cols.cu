@@ -27,7 +27,7 @@ __global__ void __launch_bounds__(ColCfg<NY>::THREADS, ColCfg<NY>::MINB) k_opt_c
     }
     __syncthreads();
     const int kx = x0 + team;
-    const int col = (kx + a.px / 2) % a.px;  // fftshift along x
+    const int col = add_mod(kx, a.px / 2, a.px);  // fftshift along x
     const double rx = pl.dx_out * ((double)col - 0.5 * a.px) + pl.ox;
     const float2 post = make_float2((float)pl.post_re, (float)pl.post_im);
     auto load = [&](int n) -> float2 { return s[pad_idx(n)]; };
@@ -35,7 +35,7 @@ __global__ void __launch_bounds__(ColCfg<NY>::THREADS, ColCfg<NY>::MINB) k_opt_c
     // the fftshift along y is applied by the final copy
     const float2* hcol = a.H ? a.H + (size_t)q * a.py * a.px + kx : nullptr;
     auto store = [&](int k, float2 v, int) {
-      const int row = (k + a.py / 2) % a.py;  // output row of bin k (fftshift along y)
+      const int row = add_mod(k, a.py / 2, a.py);  // output row of bin k (fftshift along y)
       if (hcol && kx < a.px) v = cmul(v, hcol[(size_t)k * a.px]);
       if (pl.conj) v = cconj(v);
       v = cmul(post, v);
@@ -51,9 +51,9 @@ __global__ void __launch_bounds__(ColCfg<NY>::THREADS, ColCfg<NY>::MINB) k_opt_c
     for (int idx = threadIdx.x; idx < a.oy_n * V; idx += blockDim.x) {
       const int r = idx / V, c = idx % V, x = x0 + c;
       if (x >= a.px) continue;
-      const int colo = (x + a.px / 2) % a.px - a.crop_x;
+      const int colo = add_mod(x, a.px / 2, a.px) - a.crop_x;
       if (colo < 0 || colo >= a.ox_n) continue;
-      const int k = (r + a.crop_y + a.py - a.py / 2) % a.py;  // FFT bin of output row r
+      const int k = add_mod(r + a.crop_y, a.py - a.py / 2, a.py);  // FFT bin of output row r
       out[(((size_t)b * a.oy_n + r) * a.ox_n + colo) * a.W + w] = tile[c * LEN + pad_idx(k)];
     }
   }

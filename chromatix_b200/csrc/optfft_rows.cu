@@ -20,7 +20,7 @@ __global__ void __launch_bounds__(RowCfg<NX>::THREADS, RowCfg<NX>::MINB) k_opt_r
     const int q = valid ? (int)(item / a.py) : 0;
     const int yy = valid ? (int)(item % a.py) : 0;
     const cx_fft_plane pl = a.planes[q];
-    const int yp = (yy + a.py / 2) % a.py;  // ifftshift: padded-grid row feeding FFT row yy
+    const int yp = add_mod(yy, a.py / 2, a.py);  // ifftshift: padded-grid row feeding FFT row yy
     const int y = yp - a.pad_y;
     const bool row_data = valid && y >= 0 && y < a.ny;
     const int b = pl.in_plane / a.W, w = pl.in_plane % a.W;
@@ -28,7 +28,7 @@ __global__ void __launch_bounds__(RowCfg<NX>::THREADS, RowCfg<NX>::MINB) k_opt_r
     const double ry = pl.dy_in * ((double)yp - 0.5 * a.py) + pl.oy;
     const float2 pre = make_float2((float)pl.pre_re, (float)pl.pre_im);
     auto load = [&](int n) -> float2 {
-      const int xp = (n + a.px / 2) % a.px;
+      const int xp = add_mod(n, a.px / 2, a.px);
       const int x = xp - a.pad_x;
       if (!row_data || x < 0 || x >= a.nx) return make_float2(0.f, 0.f);
       float2 v = src[(size_t)x * a.W];

@@ -42,6 +42,39 @@ __global__ void k_psf_count(PsfArgs a, unsigned long long* counts, int* srange) 
 }
 
 // ---------------------------------------------------------------------------
+// accurate-mode source tables (PsfArgs::M, PsfArgs::CX), FP64 phases
+// ---------------------------------------------------------------------------
+__global__ void k_psf_tables(PsfArgs a) {
+  const long ncx = (long)a.nz * a.csum;
+  const double PI = 3.141592653589793238462643383279502884;
+  for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < a.msum + ncx; i += (long)gridDim.x * blockDim.x) {
+    if (i < a.msum) {
+      int w = 0;
+      while (w + 1 < a.W && i >= a.mprefix[w + 1]) ++w;
+      const PsfWv& p = a.wv[w];
+      const long loc = i - a.mprefix[w];
+      const int y = a.ylo[w] + (int)(loc / a.ncols[w]), x = a.xlo[w] + (int)(loc % a.ncols[w]);
+      float2 v = make_float2(0.f, 0.f);
+      if (y < a.ny && x < a.nx && in_pupil(a, p, y, x)) {
+        v = psf_const(a, w, a.counts);
+        if (a.has_phase) v = cmul(v, expi_precise((double)a.phase[(size_t)y * a.nx + x] * p.mod));
+      }
+      a.M[i] = v;
+    } else {
+      const long j = i - a.msum;
+      const int iz = (int)(j / a.csum), loc = (int)(j % a.csum);
+      int w = 0;
+      while (w + 1 < a.W && loc >= a.cprefix[w + 1]) ++w;
+      const PsfWv& p = a.wv[w];
+      const int x = a.xlo[w] + (loc - a.cprefix[w]);
+      const double gxo = p.dx * ((double)x - (double)a.nx * 0.5) - a.offx;
+      const double qz = -PI * (a.z[iz] / a.f_obj) / p.L2;
+      a.CX[j] = expi_precise(qz * gxo * gxo);
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
 // materialised source field (objective_point_source [-> phase_change]) for
 // callers that need u itself: out (zc, ny, nx, W) complex64, without the lens
 // normalisation
@@ -103,6 +136,25 @@ static void psf_rows(const cx_psf_desc* d, const cx_psf_spectrum* spec, int w, i
   if (hi < lo) hi = lo;
   *ylo = (int)lo;
   *nrows = (int)(hi - lo + 1);
+}
+
+// columns of the grid that can hold pupil pixels for wavelength w (same
+// conservative rule as psf_rows, along x)
+static void psf_cols_box(const cx_psf_desc* d, const cx_psf_spectrum* spec, int w, int* xlo, int* ncols) {
+  const double lam0 = spec->wavelength[0];
+  const double D = 2.0 * d->f_obj * d->NA / d->n_medium;
+  double r = (lam0 / spec->wavelength[w]) * D / 2.0;
+  if (d->lens_NA > 0.0) {
+    const double rl = (lam0 / spec->wavelength[w]) * (2.0 * d->f_lens * d->lens_NA / d->n_medium) / 2.0;
+    r = rl < r ? rl : r;
+  }
+  const double h = r / spec->dx[w];
+  long lo = (long)floor(0.5 * d->nx - h) - 1, hi = (long)ceil(0.5 * d->nx + h) + 1;
+  if (lo < 0) lo = 0;
+  if (hi > d->nx - 1) hi = d->nx - 1;
+  if (hi < lo) hi = lo;
+  *xlo = (int)lo;
+  *ncols = (int)(hi - lo + 1);
 }
 
 // Row spectra of one z-chunk are written by pass A and read back by pass B;
@@ -187,10 +239,17 @@ static PsfArgs psf_make_args(const cx_psf_desc* d, const cx_psf_spectrum* spec, 
 
 // workspace: 256 bytes of pupil counters, then one chunk of row spectra
 // (sized for the worst case rowsum = n_wv * ny, independent of the spectrum)
-static size_t psf_ws(const cx_psf_desc* d) {
+static size_t psf_t_bytes(const cx_psf_desc* d) {
   const size_t worst_z = (size_t)d->n_wv * d->ny * d->nx * sizeof(float2);
   const size_t t = psf_chunk_budget() > worst_z ? psf_chunk_budget() : worst_z;
-  return 256 + ((t + 255) & ~(size_t)255);
+  return (t + 255) & ~(size_t)255;
+}
+static size_t psf_m_bytes(const cx_psf_desc* d) {
+  return ((size_t)d->n_wv * d->ny * d->nx * sizeof(float2) + 255) & ~(size_t)255;
+}
+static size_t psf_ws(const cx_psf_desc* d) {
+  const size_t cx_bytes = ((size_t)d->n_z * d->n_wv * d->nx * sizeof(float2) + 255) & ~(size_t)255;
+  return 256 + psf_t_bytes(d) + psf_m_bytes(d) + cx_bytes;
 }
 
 }  // namespace cx
@@ -232,14 +291,23 @@ static cx_status psf_setup(const cx_psf_desc* d, const cx_psf_spectrum* spec, co
   a.T = reinterpret_cast<float2*>(static_cast<char*>(workspace) + 256);
   if ((s = ensure_twiddles(&a.twg)) != CX_OK) return s;
   a.rowsum = 0;
+  a.msum = 0;
+  a.csum = 0;
   for (int w = 0; w < a.W; ++w) {
     psf_rows(d, spec, w, &a.ylo[w], &a.nrows[w]);
     a.prefix[w] = a.rowsum;
     a.rowsum += a.nrows[w];
+    psf_cols_box(d, spec, w, &a.xlo[w], &a.ncols[w]);
+    a.mprefix[w] = (int)a.msum;
+    a.msum += (long)a.nrows[w] * a.ncols[w];
+    a.cprefix[w] = a.csum;
+    a.csum += a.ncols[w];
   }
-  // z planes per chunk: as many compact planes as the workspace holds
+  a.M = reinterpret_cast<float2*>(static_cast<char*>(workspace) + 256 + psf_t_bytes(d));
+  a.CX = reinterpret_cast<float2*>(static_cast<char*>(workspace) + 256 + psf_t_bytes(d) + psf_m_bytes(d));
+  // z planes per chunk: as many compact planes as the row-spectrum region holds
   const size_t zbytes = sizeof(float2) * (size_t)a.rowsum * a.nx;
-  int zc = (int)((psf_ws(d) - 256) / zbytes);
+  int zc = (int)(psf_t_bytes(d) / zbytes);
   if (zc < 1) zc = 1;
   if (zc > a.nz) zc = a.nz;
   *out_args = a;
@@ -252,6 +320,12 @@ static cx_status psf_prepare(const PsfArgs& a, void* workspace, cudaStream_t st)
   k_psf_count<<<(a.W * a.ny + 127) / 128, 128, 0, st>>>(a, const_cast<unsigned long long*>(a.counts),
                                                          const_cast<int*>(a.srange));
   CX_LAUNCH_CHECK();
+  if (a.precision != CX_PREC_REF32) {
+    const long n = a.msum + (long)a.nz * a.csum;
+    const int blocks = (int)((n + 255) / 256 < 4096 ? (n + 255) / 256 : 4096);
+    k_psf_tables<<<blocks, 256, 0, st>>>(a);
+    CX_LAUNCH_CHECK();
+  }
   return CX_OK;
 }
 
@@ -288,7 +362,7 @@ extern "C" cx_status cx_psf_plan_info(const cx_psf_desc* d, const cx_psf_spectru
     rowsum += nr;
   }
   const size_t zbytes = sizeof(float2) * (size_t)rowsum * d->nx;
-  int zc = (int)((psf_ws(d) - 256) / zbytes);
+  int zc = (int)(psf_t_bytes(d) / zbytes);
   if (zc < 1) zc = 1;
   if (zc > d->n_z) zc = d->n_z;
   info[0] = zc;
@@ -314,6 +388,120 @@ extern "C" cx_status cx_psf_4f_stage(const cx_psf_desc* d, const cx_psf_spectrum
   }
   a.zc = (a.nz - a.z0) < zc ? (a.nz - a.z0) : zc;
   return stage == 0 ? psf_dispatch_rows(a.nx, a, st) : psf_dispatch_cols(a.ny, a, st);
+}
+
+// ---------------------------------------------------------------------------
+// cx_psf_4f_to_host: the PSF stack streamed into host memory.  Groups of whole
+// z-chunks are computed on `stream` into a ring of device slots; each group's
+// device-to-host copy runs on `copy_stream` while the next groups compute.
+// ---------------------------------------------------------------------------
+
+namespace cx {
+
+constexpr int kPsfHostSlots = 3;
+constexpr int kPsfHostGroups = 8;  // target number of copy groups per stack
+
+// group = z-planes per copy group; first = planes of the first group (one
+// chunk, so that the first copy starts early)
+static cx_status psf_host_plan(const cx_psf_desc* d, const cx_psf_spectrum* spec, int* group, size_t* slot_bytes,
+                               int* first = nullptr) {
+  int32_t info[4];
+  cx_status s = cx_psf_plan_info(d, spec, info);
+  if (s != CX_OK) return s;
+  const int zc = info[0], chunks = info[2];
+  const int per_group = (chunks + kPsfHostGroups - 1) / kPsfHostGroups;
+  int g = zc * (per_group > 0 ? per_group : 1);
+  if (g > d->n_z) g = d->n_z;
+  *group = g;
+  if (first) *first = zc < g ? zc : g;
+  *slot_bytes = (((size_t)g * d->ny * d->nx * sizeof(float)) + 255) & ~(size_t)255;
+  return CX_OK;
+}
+
+}  // namespace cx
+
+extern "C" cx_status cx_psf_host_workspace_size(const cx_psf_desc* d, const cx_psf_spectrum* spec, size_t* bytes) {
+  cx_status s = psf_check(d);
+  if (s != CX_OK) return s;
+  if (!bytes || !spec || !spec->wavelength || !spec->dy || !spec->dx) {
+    set_error("null pointer argument");
+    return CX_ERR_INVALID;
+  }
+  int g = 1;
+  size_t slot = 0;
+  if ((s = psf_host_plan(d, spec, &g, &slot)) != CX_OK) return s;
+  cx_psf_desc dg = *d;
+  dg.n_z = g;
+  *bytes = psf_ws(&dg) + kPsfHostSlots * slot;
+  return CX_OK;
+}
+
+extern "C" cx_status cx_psf_4f_to_host(const cx_psf_desc* d, const cx_psf_spectrum* spec, const double* z_dev,
+                                       const float* phase, float* intensity_host, void* workspace,
+                                       size_t workspace_bytes, cx_stream_t stream, cx_stream_t copy_stream) {
+  cx_status s = psf_check(d);
+  if (s != CX_OK) return s;
+  if (!intensity_host || !workspace || !z_dev) {
+    set_error("null pointer argument");
+    return CX_ERR_INVALID;
+  }
+  size_t need = 0;
+  if ((s = cx_psf_host_workspace_size(d, spec, &need)) != CX_OK) return s;
+  if (workspace_bytes < need) {
+    set_error("workspace too small: %zu < %zu", workspace_bytes, need);
+    return CX_ERR_WORKSPACE;
+  }
+  int g = 1, g0 = 1;
+  size_t slot = 0;
+  if ((s = psf_host_plan(d, spec, &g, &slot, &g0)) != CX_OK) return s;
+  cx_psf_desc dg = *d;
+  dg.n_z = g;
+  const size_t pws = psf_ws(&dg);
+  char* ring = static_cast<char*>(workspace) + pws;
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  cudaStream_t cs = copy_stream ? static_cast<cudaStream_t>(copy_stream) : st;
+  const size_t plane = (size_t)d->ny * d->nx;
+  cudaEvent_t computed[kPsfHostSlots], copied[kPsfHostSlots];
+  int made = 0;
+  cudaError_t e = cudaSuccess;
+  for (; made < kPsfHostSlots; ++made) {
+    if ((e = cudaEventCreateWithFlags(&computed[made], cudaEventDisableTiming)) != cudaSuccess) break;
+    if ((e = cudaEventCreateWithFlags(&copied[made], cudaEventDisableTiming)) != cudaSuccess) {
+      cudaEventDestroy(computed[made]);
+      break;
+    }
+  }
+  if (e == cudaSuccess) {
+    for (int z0 = 0, j = 0, gj = g0; z0 < d->n_z && s == CX_OK && e == cudaSuccess; z0 += gj, ++j, gj = g) {
+      const int k = j % kPsfHostSlots;
+      const int nz = (d->n_z - z0) < gj ? (d->n_z - z0) : gj;
+      float* dst = reinterpret_cast<float*>(ring + (size_t)k * slot);
+      if (j >= kPsfHostSlots && (e = cudaStreamWaitEvent(st, copied[k], 0)) != cudaSuccess) break;
+      cx_psf_desc dj = *d;
+      dj.n_z = nz;
+      if ((s = cx_psf_4f(&dj, spec, z_dev + z0, phase, dst, workspace, pws, stream)) != CX_OK) break;
+      if ((e = cudaEventRecord(computed[k], st)) != cudaSuccess) break;
+      if ((e = cudaStreamWaitEvent(cs, computed[k], 0)) != cudaSuccess) break;
+      if ((e = cudaMemcpyAsync(intensity_host + (size_t)z0 * plane, dst, sizeof(float) * nz * plane,
+                               cudaMemcpyDeviceToHost, cs)) != cudaSuccess)
+        break;
+      if ((e = cudaEventRecord(copied[k], cs)) != cudaSuccess) break;
+    }
+    // the call is complete in `stream` order once the last copy is
+    if (e == cudaSuccess && s == CX_OK && cs != st) {
+      for (int k = 0; k < kPsfHostSlots && e == cudaSuccess; ++k) e = cudaStreamWaitEvent(st, copied[k], 0);
+    }
+  }
+  for (int k = 0; k < made; ++k) {
+    cudaEventDestroy(computed[k]);
+    cudaEventDestroy(copied[k]);
+  }
+  if (s != CX_OK) return s;
+  if (e != cudaSuccess) {
+    set_error("cx_psf_4f_to_host: %s", cudaGetErrorString(e));
+    return CX_ERR_CUDA;
+  }
+  return CX_OK;
 }
 
 extern "C" cx_status cx_psf_source(const cx_psf_desc* d, const cx_psf_spectrum* spec, const double* z_dev,

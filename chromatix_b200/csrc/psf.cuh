@@ -41,6 +41,17 @@ struct PsfArgs {
   double f_obj, n, amp, offy, offx, power;
   PsfWv wv[PSF_MAX_WV];
   int ylo[PSF_MAX_WV], nrows[PSF_MAX_WV], prefix[PSF_MAX_WV], rowsum;  // compact row spectra
+  // accurate mode: the source is evaluated from tables built once per call.
+  // M (z-independent, per wavelength w a box of nrows_w x ncols_w pixels from
+  // (ylo_w, xlo_w)): amp (-1j / L^2) sqrt(P / power) lens_norm exp(i phase mod)
+  // on pupil pixels, 0 elsewhere.  CX (nz, csum): exp(i qz (x dx - off_x)^2),
+  // qz = -pi (z / f) / L^2.  The defocus phase is separable, so a pixel is
+  // M(y, x) CX(z, x) exp(i qz (y dy - off_y)^2).
+  int xlo[PSF_MAX_WV], ncols[PSF_MAX_WV], mprefix[PSF_MAX_WV], cprefix[PSF_MAX_WV];
+  long msum;
+  int csum;
+  float2* M;
+  float2* CX;
   const double* z;
   const float* phase;
   float2* T;  // (zc, rowsum, nx): only the rows [ylo_w, ylo_w + nrows_w) of each wavelength
@@ -101,7 +112,7 @@ __device__ __forceinline__ float2 psf_const(const PsfArgs& a, int w, const unsig
 // ---------------------------------------------------------------------------
 // pass A: analytic source -> row FFT, for the rows inside the pupil only
 // ---------------------------------------------------------------------------
-template <int NX>
+template <int NX, bool TAB>
 __global__ void __launch_bounds__(RowCfg<NX>::THREADS, RowCfg<NX>::MINB) k_psf_rows(PsfArgs a) {
   using C = RowCfg<NX>;
   extern __shared__ float2 sm[];
@@ -132,8 +143,23 @@ __global__ void __launch_bounds__(RowCfg<NX>::THREADS, RowCfg<NX>::MINB) k_psf_r
     const double gy = p.dy * ((double)y - (double)a.ny * 0.5);
     const double qz = -PI * (z / a.f_obj) / p.L2;
     const double gyo = gy - a.offy;
+    float2* dst = a.T + ((size_t)zl * a.rowsum + rem) * a.nx;
+    auto store = [&](int k, float2 v, int) { dst[k] = v; };
+    if constexpr (TAB) {
+      const float2* mrow = a.M + a.mprefix[w] + (size_t)(y - a.ylo[w]) * a.ncols[w];
+      const float2* cxz = a.CX + (size_t)(a.z0 + zl) * a.csum + a.cprefix[w];
+      const int xlo = a.xlo[w], nc = a.ncols[w];
+      const float2 cy = expi_precise(qz * gyo * gyo);
+      auto load = [&](int n) -> float2 {
+        const int c = add_mod(n, NX / 2, NX) - xlo;  // ifftshift along x, then the box column
+        if ((unsigned)c >= (unsigned)nc) return make_float2(0.f, 0.f);
+        return cmul(cmul(mrow[c], cxz[c]), cy);
+      };
+      team_fft<NX, false>(s, tw, lane, team, load, store);
+      continue;
+    }
     auto load = [&](int n) -> float2 {
-      const int x = (n + a.nx / 2) % a.nx;  // ifftshift along x
+      const int x = add_mod(n, NX / 2, NX);  // ifftshift along x
       if (!in_pupil(a, p, y, x)) return make_float2(0.f, 0.f);
       if (a.precision == CX_PREC_REF32) {
         // objective_point_source: u = (amp*-1j/L^2) * exp(1j*phase) (sources.py:201-204)
@@ -157,8 +183,6 @@ __global__ void __launch_bounds__(RowCfg<NX>::THREADS, RowCfg<NX>::MINB) k_psf_r
       if (a.has_phase) ph += (double)ph_row[x] * p.mod;
       return cmul(cst, expi_reduced(ph));
     };
-    float2* dst = a.T + ((size_t)zl * a.rowsum + rem) * a.nx;
-    auto store = [&](int k, float2 v, int) { dst[k] = v; };
     team_fft_ex<NX, false, true, false>(s, tw, lane, team, load, store);
   }
 }
@@ -200,11 +224,14 @@ __global__ void __launch_bounds__(ColCfg<NY>::THREADS, ColCfg<NY>::MINB) k_psf_c
       __syncthreads();
       // field rows [slo, shi) feed FFT rows (y - ny/2) mod ny (ifftshift)
       load_col_tile<V, LEN>(tile, src - (size_t)ylo * a.nx, a.nx, x0, a.nx, slo, shi,
-                            [&](int y) { return (y - a.ny / 2 + a.ny) % a.ny; });
+                            [&](int y) { return add_mod(y, NY - NY / 2, NY); });
       __syncthreads();
+      // FFT row n holds field row (n + NY/2) mod NY; the support [slo, shi)
+      // contains the centre row NY/2 (or is empty), so it maps to
+      // n < shi - NY/2 or n >= slo + NY - NY/2
+      const int n_lo = shi - NY / 2, n_hi = slo + (NY - NY / 2);
       auto load = [&](int n) -> float2 {
-        const int y = (n + a.ny / 2) % a.ny;
-        return (y >= slo && y < shi) ? s[pad_idx(n)] : make_float2(0.f, 0.f);
+        return (n < n_lo || n >= n_hi) ? s[pad_idx(n)] : make_float2(0.f, 0.f);
       };
       auto store = [&](int k, float2 v, int) {
         const float e = dens * cabs2(v);
@@ -217,12 +244,15 @@ __global__ void __launch_bounds__(ColCfg<NY>::THREADS, ColCfg<NY>::MINB) k_psf_c
     for (int idx = threadIdx.x; idx < a.ny * V; idx += blockDim.x) {
       const int row = idx / V, c = idx % V, x = x0 + c;
       if (x < a.nx) {
-        const int k = (row - a.ny / 2 + a.ny) % a.ny;  // fftshift along y
-        outz[(size_t)row * a.nx + (x + a.nx / 2) % a.nx] = accs[c * ACC + k];
+        const int k = add_mod(row, NY - NY / 2, NY);  // fftshift along y
+        outz[(size_t)row * a.nx + add_mod(x, a.nx / 2, a.nx)] = accs[c * ACC + k];
       }
     }
   }
 }
+
+// accurate-mode source tables M and CX (see PsfArgs), after the count pass
+__global__ void k_psf_tables(PsfArgs a);
 
 cx_status psf_dispatch_rows(int n, const PsfArgs& a, cudaStream_t st);
 cx_status psf_dispatch_cols(int n, const PsfArgs& a, cudaStream_t st);

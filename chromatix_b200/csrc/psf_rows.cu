@@ -6,7 +6,7 @@ namespace cx {
 template <int NX>
 static cx_status launch_psf_rows(const PsfArgs& a, cudaStream_t st) {
   using C = RowCfg<NX>;
-  auto k = k_psf_rows<NX>;
+  auto k = a.precision == CX_PREC_REF32 ? k_psf_rows<NX, false> : k_psf_rows<NX, true>;
   CX_CUDA_TRY(set_smem(k, C::SMEM));
   const long items = ((long)a.zc * a.rowsum + C::TEAMS - 1) / C::TEAMS;
   const int grid = persistent_grid(k, C::THREADS, C::SMEM, items);

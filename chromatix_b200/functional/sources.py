@@ -31,6 +31,12 @@ def _sigs(L):
             fn.restype = nat.c_int32
             fn.argtypes = [nat.ctypes.POINTER(nat.cx_psf_desc), nat.ctypes.POINTER(nat.cx_psf_spectrum),
                            nat.c_void_p, nat.c_void_p, nat.c_void_p, nat.c_void_p, nat.c_size_t, nat.c_void_p]
+        P, S = nat.ctypes.POINTER(nat.cx_psf_desc), nat.ctypes.POINTER(nat.cx_psf_spectrum)
+        L.cx_psf_host_workspace_size.restype = nat.c_int32
+        L.cx_psf_host_workspace_size.argtypes = [P, S, nat.ctypes.POINTER(nat.c_size_t)]
+        L.cx_psf_4f_to_host.restype = nat.c_int32
+        L.cx_psf_4f_to_host.argtypes = [P, S, nat.c_void_p, nat.c_void_p, nat.c_void_p, nat.c_void_p, nat.c_size_t,
+                                        nat.c_void_p, nat.c_void_p]
         _SIG = True
     return L
 
@@ -196,6 +202,36 @@ class LazySourceField(Field):
                               nat.stream_handle(self._device)))
         del keep
         return out if r["zbatch"] else out[0]
+
+
+    def intensity_to(self, out):
+        """PSF stack into ``out``.  For a host (CPU) ``out`` the stack is
+        streamed: groups of z-planes are copied to the host on a side stream
+        while later groups compute (``cx_psf_4f_to_host``); page-locked memory
+        gives the overlap.  ``out`` is valid once the current stream has been
+        synchronised."""
+        r = self._recipe
+        if self.stage != "lens" or self._u is not None or out.is_cuda:
+            return super().intensity_to(out)
+        torch = nat.torch_mod()
+        ny, nx = r["shape"]
+        shape = ((int(r["nz"]),) if r["zbatch"] else ()) + (ny, nx)
+        if tuple(out.shape) != shape or out.dtype != torch.float32 or not out.is_contiguous():
+            raise ValueError(f"out must be a contiguous float32 tensor of shape {shape}")
+        L = _sigs(nat.lib())
+        d = self._desc()
+        spec, keep = self._spec()
+        ws_b = nat.c_size_t(0)
+        nat.check(L.cx_psf_host_workspace_size(d, spec, ws_b))
+        ws = nat.workspace(ws_b.value, self._device)
+        cs = nat.copy_stream(self._device)
+        ws.record_stream(cs)
+        zd = self._z_dev()
+        ph = r.get("phase")
+        nat.check(L.cx_psf_4f_to_host(d, spec, nat.ptr(zd), nat.ptr(ph), out.data_ptr(), nat.ptr(ws), ws_b.value,
+                                      nat.stream_handle(self._device), cs.cuda_stream))
+        del keep
+        return out
 
 
 def materialize(field: Field) -> Field:

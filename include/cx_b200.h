@@ -142,6 +142,19 @@ cx_status cx_psf_4f(const cx_psf_desc* d, const cx_psf_spectrum* spec, const dou
  * per plane stack (pupil rows of all wavelengths), info[2] = number of chunks. */
 cx_status cx_psf_plan_info(const cx_psf_desc* d, const cx_psf_spectrum* spec, int32_t* info);
 
+/* The PSF stack of cx_psf_4f written into HOST memory (n_z x ny x nx
+ * float32 at intensity_host).  Groups of z-planes are computed on `stream`
+ * into a ring of device slots inside the workspace, and each group's copy to
+ * the host runs on `copy_stream` while later groups compute, so the transfer
+ * overlaps the FFTs (intensity_host must be page-locked for that; pageable
+ * memory works without overlap).  Everything is ordered before later work on
+ * `stream`.  No counterpart in the reference (XLA decides its transfers).
+ * Workspace: cx_psf_host_workspace_size. */
+cx_status cx_psf_host_workspace_size(const cx_psf_desc* d, const cx_psf_spectrum* spec, size_t* bytes);
+cx_status cx_psf_4f_to_host(const cx_psf_desc* d, const cx_psf_spectrum* spec, const double* z_dev,
+                            const float* phase, float* intensity_host, void* workspace, size_t workspace_bytes,
+                            cx_stream_t stream, cx_stream_t copy_stream);
+
 /* One stage of cx_psf_4f, for measuring kernels in isolation: stage -1 =
  * pupil counts (must run first), 0 = row pass of `chunk`, 1 = column pass of
  * `chunk`.  Same arguments as cx_psf_4f. */

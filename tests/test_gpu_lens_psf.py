@@ -161,3 +161,24 @@ def test_thin_sample_kats():
     np.testing.assert_allclose(to_np(out.u), -to_np(f.u), atol=1e-6)
     out = cf.thin_sample(f, np.ones((2, 2)) / (2 * np.pi), z0, 0.532)
     np.testing.assert_allclose(to_np(out.u) * np.e, to_np(f.u), rtol=1e-5)
+
+
+@pytest.mark.parametrize("nz,pinned", [(64, True), (7, False), (1, True)])
+def test_psf_streamed_to_host_equals_device_result(nz, pinned):
+    """intensity_to(host buffer): grouped device->host copies on a side stream
+    give exactly the device result (same kernels, same chunks per plane)."""
+    import torch
+
+    p = _psf_inputs(n=256, nz=nz, seed=5)
+    f = _cuda_psf(p)
+    dev = f.intensity.cpu()
+    shape = (nz, 256, 256) if nz > 1 else (256, 256)
+    host = torch.full(shape, float("nan"), dtype=torch.float32)
+    if pinned:
+        host = host.pin_memory()
+    out = f.intensity_to(host)
+    torch.cuda.current_stream().synchronize()
+    assert out is host
+    assert torch.equal(host, dev)
+    with pytest.raises(ValueError):
+        f.intensity_to(torch.empty((3, 3), dtype=torch.float32))
