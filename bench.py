@@ -329,6 +329,104 @@ def accuracy_check(dev):
 
 
 # ---------------------------------------------------------------------------
+# serving workload: Poisson stream of mixed propagation requests
+# ---------------------------------------------------------------------------
+SERVE_SIDES = (256, 512, 1024, 2048)
+SERVE_OPS = ("asm", "transfer", "czt_zoom")
+
+
+def serve_arm(args):
+    """Poisson arrivals (mean ``--rate`` req/s) of requests with side N in
+    {256, 512, 1024, 2048}, op in {ASM, Fresnel transfer, CZT zoom to 512^2},
+    z ~ U[1, 500] um, lambda ~ U[0.4, 0.7] um, n = 1.33, dx = 0.3 um,
+    random-phase fields resident in HBM, mode "same" with pad N/2, 60 GB
+    admission budget; p50 / p99 latency from arrival to completion."""
+    import torch
+
+    from chromatix_b200.serving import PropagationServer, Request, percentile
+
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300), device_id=dev)
+    rng = np.random.default_rng(1000 + rank)
+    fields = {}
+    for N in SERVE_SIDES:
+        g = torch.Generator(device=dev)
+        g.manual_seed(N + 7919 * rank)
+        ph = torch.rand((4, N, N), device=dev, dtype=torch.float32, generator=g) * (2 * np.pi)
+        fields[N] = [torch.polar(torch.ones_like(ph[k]), ph[k]).contiguous() for k in range(4)]
+    srv = PropagationServer(dev, budget_bytes=60e9, n_streams=4, max_batch=32)
+
+    def make(t):
+        N = int(rng.choice(SERVE_SIDES))
+        return Request(op=SERVE_OPS[int(rng.integers(0, 3))], u=fields[N][int(rng.integers(0, 4))], dx=0.3,
+                       z=float(rng.uniform(1, 500)), wavelength=float(rng.uniform(0.4, 0.7)), n=1.33,
+                       zoom=float(rng.uniform(0.25, 4)), out_shape=(512, 512), t_arrival=t)
+
+    # warm-up: every (op, N) once
+    for op in SERVE_OPS:
+        for N in SERVE_SIDES:
+            srv.submit(Request(op=op, u=fields[N][0], dx=0.3, z=100.0, wavelength=0.5, zoom=2.0))
+    srv.drain()
+    torch.cuda.synchronize(dev)
+    if dist:
+        dist.barrier()
+    n_req = max(1, int(args.rate * args.serve_seconds))
+    arrivals = np.cumsum(rng.exponential(1.0 / args.rate, n_req))
+    reqs = []
+    with ClockSampler(local) as clk:
+        t0 = time.perf_counter()
+        i = 0
+        while i < n_req or srv.busy:
+            now = time.perf_counter() - t0
+            while i < n_req and arrivals[i] <= now:
+                reqs.append(srv.submit(make(t0 + arrivals[i])))
+                i += 1
+            srv.step()
+        torch.cuda.synchronize(dev)
+        t_end = time.perf_counter()
+    elapsed = t_end - t0
+    lat = np.array([r.latency for r in reqs]) * 1e3
+    px = float(sum(r.side * r.side for r in reqs))
+    stats = [elapsed, px, percentile(lat, 50), percentile(lat, 99)]
+    if dist:
+        t = torch.tensor(stats, dtype=torch.float64, device=dev)
+        mx, sm = t.clone(), t.clone()
+        dist.all_reduce(mx, op=dist.ReduceOp.MAX)
+        dist.all_reduce(sm, op=dist.ReduceOp.SUM)
+        stats = [float(mx[0]), float(sm[1]), float(mx[2]), float(mx[3])]
+    elapsed, px, p50, p99 = stats
+    if rank == 0:
+        by_op = {op: round(percentile([r.latency * 1e3 for r in reqs if r.op == op], 99), 3) for op in SERVE_OPS}
+        line = {
+            "metric": "served Mpx/s (p50/p99 request latency)", "value": round(px / elapsed / 1e6, 1),
+            "unit": "Mpx/s", "n_gpus": world, "steps": n_req, "warmup": len(SERVE_OPS) * len(SERVE_SIDES),
+            "ms_per_step": round(elapsed * 1e3 / n_req, 4), "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "c64", "data": "synthetic (seeded Poisson stream)",
+            "config": {"workload": "serving stream: Poisson arrivals of ASM / Fresnel transfer / CZT-zoom requests, "
+                                   "N in {256,512,1024,2048}, pad N/2, mode same, 60 GB admission budget",
+                       "rate_req_s": args.rate, "seconds": args.serve_seconds, "streams": 4, "max_batch": 32,
+                       "parallelism": f"replicas x{world}" if world > 1 else "single GPU"},
+            "latency_ms": {"p50": round(p50, 3), "p99": round(p99, 3), "mean": round(float(lat.mean()), 3),
+                           "p99_by_op": by_op},
+            "requests": n_req * world, "achieved_req_s": round(n_req * world / elapsed, 1),
+            "clocks": clk.summary(),
+        }
+        print(json.dumps(line), flush=True)
+    if dist:
+        dist.destroy_process_group()
+
+
+# ---------------------------------------------------------------------------
 # CPU baseline / reference arm: the oracle (float32 reference order)
 # ---------------------------------------------------------------------------
 def cpu_baseline(n_z_sample: int = 2):
@@ -399,11 +497,17 @@ def main():
     ap.add_argument("--cpu-sample-z", type=int, default=2)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--accuracy", action="store_true", help="also report the error vs the FP64 oracle")
+    ap.add_argument("--workload", default="psf", choices=["psf", "serve"],
+                    help="psf: the batched 4f PSF stack (headline); serve: the Poisson request stream")
+    ap.add_argument("--rate", type=float, default=2000.0, help="serve: mean arrivals per second")
+    ap.add_argument("--serve-seconds", type=float, default=2.0, help="serve: length of the arrival stream")
     args = ap.parse_args()
     if args.warmup < 3 and args.impl == "ours":
         args.warmup = 3
     if args.impl == "reference":
         reference_arm(args)
+    elif args.workload == "serve":
+        serve_arm(args)
     else:
         gpu_arm(args)
 

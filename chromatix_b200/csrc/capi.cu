@@ -125,7 +125,7 @@ extern "C" cx_status cx_fft1d(const void* in, void* out, int32_t n, int64_t batc
 #define CX_CASE_(N) \
   case N:           \
     return launch_fft1d<N>(i, o, batch, inverse != 0, twg, st);
-    CX_FOR_EACH_SIZE(CX_CASE_)
+    CX_FOR_EACH_1D_SIZE(CX_CASE_)
 #undef CX_CASE_
   }
   set_error("FFT length %d is not supported", n);

@@ -37,8 +37,8 @@ static cx_status czt_args(const cx_czt_desc* d, CztArgs* a) {
     return CX_ERR_INVALID;
   }
   const int L = czt_length(d->n, d->m, d->L);
-  if (L < d->n + d->m - 1 || !size_supported(L)) {
-    set_error("CZT needs an FFT length >= n + m - 1 = %d (largest compiled length 4096)", d->n + d->m - 1);
+  if (L < d->n + d->m - 1 || !size_supported_1d(L)) {
+    set_error("CZT needs an FFT length >= n + m - 1 = %d (largest compiled length 8192)", d->n + d->m - 1);
     return CX_ERR_UNSUPPORTED;
   }
   if (d->layout == 1 && (d->in_istride != 1 || d->out_istride != 1)) {

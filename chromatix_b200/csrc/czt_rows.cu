@@ -18,7 +18,7 @@ cx_status czt_dispatch_rows(int L, const CztArgs& a, cudaStream_t st) {
 #define CX_CASE_(N) \
   case N:           \
     return launch_czt_rows<N>(a, st);
-    CX_FOR_EACH_SIZE(CX_CASE_)
+    CX_FOR_EACH_1D_SIZE(CX_CASE_)
 #undef CX_CASE_
   }
   set_error("FFT length %d is not supported", L);

@@ -38,6 +38,12 @@ void set_error(const char* fmt, ...);
   X(56) X(64) X(80) X(96) X(112) X(128) X(160) X(192) X(224) X(256) X(320) X(384) X(448) X(512)    \
   X(640) X(768) X(896) X(1024) X(1280) X(1536) X(1792) X(2048) X(2560) X(3072) X(3584) X(4096)
 
+// Longer lengths compiled only for the 1D transform (cx_fft1d) and the
+// chirp-Z passes, whose Bluestein length reaches n + m - 1 (up to 8192 for a
+// 4096-point input): 2^9 3^2, 2^10 5, 2^11 3, 2^10 7, 2^13.
+#define CX_FOR_EACH_LONG_SIZE(X) X(4608) X(5120) X(6144) X(7168) X(8192)
+#define CX_FOR_EACH_1D_SIZE(X) CX_FOR_EACH_SIZE(X) CX_FOR_EACH_LONG_SIZE(X)
+
 inline bool size_supported(int n) {
   switch (n) {
 #define CX_CASE_(N) case N:
@@ -49,10 +55,21 @@ inline bool size_supported(int n) {
   }
 }
 
+inline bool size_supported_1d(int n) {
+  switch (n) {
+#define CX_CASE_(N) case N:
+    CX_FOR_EACH_1D_SIZE(CX_CASE_)
+#undef CX_CASE_
+    return true;
+    default:
+      return false;
+  }
+}
+
 // Offsets of the per-length twiddle tables inside one device array (lengths in
-// CX_FOR_EACH_SIZE order, tw_len(N) entries each).
+// CX_FOR_EACH_1D_SIZE order, tw_len(N) entries each).
 #define CX_SIZE_LIST_(N) N,
-constexpr int kSizes[] = {CX_FOR_EACH_SIZE(CX_SIZE_LIST_)};
+constexpr int kSizes[] = {CX_FOR_EACH_1D_SIZE(CX_SIZE_LIST_)};
 #undef CX_SIZE_LIST_
 constexpr int kNumSizes = sizeof(kSizes) / sizeof(int);
 constexpr int tw_offset(int N) {
@@ -111,7 +128,7 @@ struct RowCfg {
 // in distinct bank pairs: stride = 16/V (mod 16) for V <= 16, odd above.
 __host__ __device__ constexpr int col_len(int N, int V) {
   int l = pad_idx(N - 1) + 1;
-  if (V >= 16) return (l % 2 == 0) ? l + 1 : l;
+  if (V >= 16 || V == 1) return (l % 2 == 0) ? l + 1 : l;
   const int want = 16 / V;
   while (l % 16 != want) ++l;
   return l;
@@ -121,10 +138,13 @@ __host__ __device__ constexpr int col_len(int N, int V) {
 template <int N>
 struct ColCfg {
   static constexpr int LPV = Plan<N>::LPV;
-  static constexpr int V0 = LPV < 32 ? (256 / LPV > 16 ? 256 / LPV : 16) : 4;
+  // multi-warp teams: up to 4 columns, at most 1024 threads per CTA
+  static constexpr int VT = 1024 / LPV >= 4 ? 4 : (1024 / LPV >= 2 ? 2 : 1);
+  static constexpr int V0 = LPV < 32 ? (256 / LPV > 16 ? 256 / LPV : 16) : VT;
   static constexpr int TW = tw_len(N);
   static constexpr size_t smem_for(int v) { return sizeof(float2) * ((size_t)TW + (size_t)v * col_len(N, v)); }
   static constexpr int V = smem_for(V0) <= 200 * 1024 ? V0 : (smem_for(V0 / 2) <= 200 * 1024 ? V0 / 2 : V0 / 4);
+  static_assert(V >= 1 && V * LPV <= 1024, "column tile does not fit one CTA");
   static constexpr int LEN = col_len(N, V);
   static constexpr int THREADS = V * LPV;
   static constexpr int MINB = minb_for(THREADS);
@@ -143,7 +163,7 @@ __device__ __forceinline__ void load_col_tile(float2* tile, const float2* __rest
   if (nr <= 0) return;
   const bool vec = (V % 2 == 0) && (ld % 2 == 0) && (x0 % 2 == 0);
   if (vec) {
-    constexpr int PR = V / 2;
+    constexpr int PR = V / 2 > 0 ? V / 2 : 1;  // (vec is false for odd V)
     const int total = nr * PR;
     for (int base = threadIdx.x; base < total; base += 4 * blockDim.x) {
       float4 v[4];

@@ -121,6 +121,38 @@ extern "C" cx_status cx_prop2d(const cx_prop2d_desc* d, const cx_plane* planes_d
   return dispatch_rows_inv(a.px, T2, static_cast<float2*>(u_out), a, st);
 }
 
+extern "C" cx_status cx_prop2d_ptrs(const cx_prop2d_desc* d, const cx_plane* planes_dev,
+                                    const void* const* u_in_ptrs_dev, void* const* u_out_ptrs_dev, const void* H,
+                                    void* workspace, size_t workspace_bytes, cx_stream_t stream) {
+  Prop2DArgs a;
+  cx_status s = make_args(d, &a);
+  if (s != CX_OK) return s;
+  if (!planes_dev || !u_in_ptrs_dev || !u_out_ptrs_dev || !workspace) {
+    set_error("null pointer argument");
+    return CX_ERR_INVALID;
+  }
+  if (d->kernel == CX_KERNEL_EXPLICIT && !H) {
+    set_error("explicit propagator requested but H is null");
+    return CX_ERR_INVALID;
+  }
+  const size_t need = align256(ws_T_bytes(a)) + align256(ws_T2_bytes(a));
+  if (workspace_bytes < need) {
+    set_error("workspace too small: %zu < %zu", workspace_bytes, need);
+    return CX_ERR_WORKSPACE;
+  }
+  a.planes = planes_dev;
+  a.H = static_cast<const float2*>(H);
+  a.in_ptrs = reinterpret_cast<const float2* const*>(u_in_ptrs_dev);
+  a.out_ptrs = reinterpret_cast<float2* const*>(u_out_ptrs_dev);
+  if ((s = ensure_twiddles(&a.twg)) != CX_OK) return s;
+  float2* T = static_cast<float2*>(workspace);
+  float2* T2 = reinterpret_cast<float2*>(static_cast<char*>(workspace) + align256(ws_T_bytes(a)));
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  if ((s = dispatch_rows_fwd(a.px, nullptr, T, a, st)) != CX_OK) return s;
+  if ((s = dispatch_cols(a.py, T, T2, a, st)) != CX_OK) return s;
+  return dispatch_rows_inv(a.px, T2, nullptr, a, st);
+}
+
 extern "C" cx_status cx_fill_propagator(const cx_prop2d_desc* d, const cx_plane* planes_dev, void* H_out,
                                         cx_stream_t stream) {
   Prop2DArgs a;

@@ -27,6 +27,11 @@ struct Prop2DArgs {
   const cx_plane* planes;
   const float2* H;
   const float2* twg;  // device twiddle tables (ensure_twiddles)
+  // optional per-batch-element field pointers (cx_prop2d_ptrs): element b of
+  // the input / output batch at in_ptrs[b] / out_ptrs[b] instead of at a
+  // fixed stride from one base pointer
+  const float2* const* in_ptrs = nullptr;
+  float2* const* out_ptrs = nullptr;
 };
 
 // --------------------------------------------------------------------------
@@ -161,7 +166,8 @@ __global__ void __launch_bounds__(RowCfg<NX>::THREADS, RowCfg<NX>::MINB) k_prop_
     const int p = valid ? (int)(item / a.ny) : 0;
     const int y = valid ? (int)(item % a.ny) : 0;
     const int b = p / a.W, w = p % a.W;
-    const float2* src = u + ((size_t)b * a.ny + y) * a.nx * a.W + w;
+    const float2* ub = a.in_ptrs ? (valid ? a.in_ptrs[b] : a.in_ptrs[0]) : u + (size_t)b * a.ny * a.nx * a.W;
+    const float2* src = ub + (size_t)y * a.nx * a.W + w;
     float2* dst = T + ((size_t)p * a.ny + y) * a.px;
     auto load = [&](int n) -> float2 {
       const int x = n - a.pad_x;
@@ -241,7 +247,8 @@ __global__ void __launch_bounds__(RowCfg<NX>::THREADS, RowCfg<NX>::MINB) k_prop_
     const int r = valid ? (int)(item % a.out_ny) : 0;
     const int b = q / a.W, w = q % a.W;
     const float2* src = T2 + ((size_t)q * a.out_ny + r) * a.px;
-    float2* dst = out + ((size_t)b * a.out_ny + r) * a.out_nx * a.W + w;
+    float2* ob = a.out_ptrs ? (valid ? a.out_ptrs[b] : a.out_ptrs[0]) : out + (size_t)b * a.out_ny * a.out_nx * a.W;
+    float2* dst = ob + (size_t)r * a.out_nx * a.W + w;
     auto load = [&](int n) -> float2 { return valid ? src[n] : make_float2(0.f, 0.f); };
     auto store = [&](int k, float2 v, int) {
       const int x = k - a.out_x0;

@@ -1,0 +1,305 @@
+"""Continuous-batching propagation server.
+
+Requests are independent propagations of one square field each, resident in
+device memory:
+
+  ``"asm"``       ``asm_propagate(field, z, n, pad_width=N/2, mode="same")``
+  ``"transfer"``  ``transfer_propagate(field, z, n, pad_width=N/2, mode="same")``
+  ``"czt_zoom"``  ``asm_propagate(field, z, n, pad_width=N/2, output_dx=dx/zoom,
+                  output_shape=out_shape)`` (the rescaled CZT branch)
+
+(functional/propagation.py:168-352, 395-443).  ASM / transfer requests that
+share (op, N, n) form a bucket; each scheduler tick launches, per free
+stream, the oldest bucket's pending requests as ONE batched ``cx_prop2d_ptrs``
+call (per-request z, wavelength and spacing in the plane table, per-request
+input / output pointers), so a batch costs three kernel launches whatever its
+size.  CZT-zoom requests run one call sequence each.  Every batch is admitted
+only while the bytes of the batches in flight (outputs + workspaces) stay
+under the HBM budget; requests wait in FIFO order otherwise.  Completion is
+detected with CUDA events; latency is host time from arrival to the event.
+
+A request's output does not depend on the batch it ran in: each plane of a
+batch is transformed by the same per-row / per-column code as a lone call.
+Outputs are allocated on the server's streams and are complete once the
+request is reported done.
+
+The scheduling policy (:class:`Scheduler`) is plain Python over request
+metadata, so it is tested without a GPU.
+"""
+
+from __future__ import annotations
+
+import collections
+import dataclasses
+import time
+
+import numpy as np
+
+from . import _native as nat
+from . import config
+
+__all__ = ["Request", "Scheduler", "PropagationServer", "percentile", "request_bytes"]
+
+OPS = ("asm", "transfer", "czt_zoom")
+
+
+@dataclasses.dataclass(eq=False)
+class Request:
+    op: str
+    u: object  # (N, N) complex64 device tensor (stays owned by the client)
+    dx: float
+    z: float
+    wavelength: float
+    n: float = 1.33
+    zoom: float = 1.0
+    out_shape: tuple = (512, 512)
+    t_arrival: float = 0.0
+    id: int = -1
+    t_launch: float = float("nan")
+    t_done: float = float("nan")
+    out: object = None
+
+    @property
+    def side(self) -> int:
+        return int(self.u.shape[-1])
+
+    @property
+    def latency(self) -> float:
+        return self.t_done - self.t_arrival
+
+    def bucket(self):
+        return (self.op, self.side, float(self.n)) if self.op != "czt_zoom" else ("czt_zoom", self.id)
+
+
+def _prop_bytes(N: int, batch: int) -> int:
+    """Device bytes one batched ASM/transfer call holds while in flight:
+    outputs (N x N each) and the workspace of the padded (2N x 2N) grid."""
+    py = px = 2 * N
+    ws = 8 * batch * (N * px + py * px)  # row spectra of the inputs + filtered spectra
+    return ws + 8 * batch * N * N + batch * 64 * 2
+
+
+def _czt_bytes(N: int, out_shape) -> int:
+    py = px = 2 * N
+    my, mx = out_shape
+    return 8 * (2 * py * px + my * px + my * mx) + 8 * 2 * 8192
+
+
+def request_bytes(r: Request) -> int:
+    return _czt_bytes(r.side, r.out_shape) if r.op == "czt_zoom" else _prop_bytes(r.side, 1)
+
+
+class Scheduler:
+    """FIFO continuous batching with an HBM admission budget.
+
+    ``pick(budget_left)`` returns the next batch to launch: the pending
+    requests of the bucket whose oldest request is the oldest overall, up to
+    ``max_batch`` and to what the budget admits, or None when even its oldest
+    request does not fit (it then waits for batches in flight to finish).
+    """
+
+    def __init__(self, budget_bytes: float, max_batch: int = 32):
+        self.budget = float(budget_bytes)
+        self.max_batch = int(max_batch)
+        self.queues: dict = collections.OrderedDict()
+        self._n = 0
+
+    def add(self, r: Request) -> None:
+        if request_bytes(r) > self.budget:
+            raise ValueError(f"request needs {request_bytes(r)} bytes, more than the whole budget {self.budget:.0f}")
+        self.queues.setdefault(r.bucket(), collections.deque()).append(r)
+        self._n += 1
+
+    def __len__(self):
+        return self._n
+
+    def pick(self, budget_left: float):
+        best, best_t = None, None
+        for key, q in self.queues.items():
+            if q and (best_t is None or q[0].t_arrival < best_t):
+                best, best_t = key, q[0].t_arrival
+        if best is None:
+            return None
+        q = self.queues[best]
+        if best[0] == "czt_zoom":
+            if request_bytes(q[0]) > budget_left:
+                return None
+            batch = [q.popleft()]
+        else:
+            N = best[1]
+            k = 0
+            while k < min(len(q), self.max_batch) and _prop_bytes(N, k + 1) <= budget_left:
+                k += 1
+            if k == 0:
+                return None
+            batch = [q.popleft() for _ in range(k)]
+        if not q:
+            del self.queues[best]
+        self._n -= len(batch)
+        return batch
+
+
+def percentile(values, p):
+    v = np.sort(np.asarray(values, dtype=np.float64))
+    if v.size == 0:
+        return float("nan")
+    return float(np.percentile(v, p))
+
+
+class _Slot:
+    """A stream with its pinned staging buffer for plane tables and pointers."""
+
+    def __init__(self, torch, device, staging_bytes):
+        self.stream = torch.cuda.Stream(device=device)
+        self.pinned = torch.empty(staging_bytes, dtype=torch.uint8).pin_memory()
+        self.dev = torch.empty(staging_bytes, dtype=torch.uint8, device=device)
+        self.busy = None  # (event, batch, bytes, keepalive) of the batch in flight
+
+
+class PropagationServer:
+    """Continuous-batching server on one device (one per GPU; replicas scale out)."""
+
+    def __init__(self, device="cuda", budget_bytes: float = 60e9, n_streams: int = 4, max_batch: int = 32,
+                 precision=None):
+        torch = nat.torch_mod()
+        self.torch = torch
+        self.device = torch.device(device)
+        if self.device.index is None:
+            self.device = torch.device("cuda", torch.cuda.current_device())
+        self.sched = Scheduler(budget_bytes, max_batch)
+        self.max_batch = int(max_batch)
+        self.precision = precision or config.get_precision()
+        staging = self.max_batch * (nat.PLANE_DTYPE.itemsize + 16) + 256
+        self.slots = [_Slot(torch, self.device, staging) for _ in range(int(n_streams))]
+        self.inflight_bytes = 0
+        self.completed: list = []
+        self._next_id = 0
+        L = nat.lib()
+        if not hasattr(L, "_cx_prop2d_ptrs_sig"):
+            L.cx_prop2d_ptrs.restype = nat.c_int32
+            L.cx_prop2d_ptrs.argtypes = [nat.ctypes.POINTER(nat.cx_prop2d_desc), nat.c_void_p, nat.c_void_p,
+                                         nat.c_void_p, nat.c_void_p, nat.c_void_p, nat.c_size_t, nat.c_void_p]
+            L._cx_prop2d_ptrs_sig = True
+        self.L = L
+
+    # -- client side ------------------------------------------------------------
+    def submit(self, r: Request) -> Request:
+        if r.op not in OPS:
+            raise ValueError(f"unknown op {r.op!r}; expected one of {OPS}")
+        u = r.u
+        if not (u.is_cuda and u.dtype == self.torch.complex64 and u.ndim == 2 and u.shape[0] == u.shape[1]
+                and u.is_contiguous()):
+            raise ValueError("a request field is a contiguous square (N, N) complex64 CUDA tensor")
+        if not r.t_arrival:
+            r.t_arrival = time.perf_counter()
+        r.id = self._next_id
+        self._next_id += 1
+        self.sched.add(r)
+        return r
+
+    @property
+    def busy(self) -> bool:
+        return len(self.sched) > 0 or any(s.busy is not None for s in self.slots)
+
+    # -- scheduler tick -----------------------------------------------------------
+    def step(self) -> list:
+        """Retire finished batches, launch new ones on free streams; returns
+        the requests completed in this tick."""
+        done = self._retire()
+        for slot in self.slots:
+            if slot.busy is not None:
+                continue
+            batch = self.sched.pick(self.sched.budget - self.inflight_bytes)
+            if batch is None:
+                break
+            self._launch(slot, batch)
+        return done
+
+    def drain(self) -> list:
+        out = []
+        while self.busy:
+            out += self.step()
+        return out
+
+    def _retire(self) -> list:
+        done = []
+        for slot in self.slots:
+            if slot.busy is None:
+                continue
+            ev, batch, nbytes, _keep = slot.busy
+            if not ev.query():
+                continue
+            t = time.perf_counter()
+            for r in batch:
+                r.t_done = t
+            self.inflight_bytes -= nbytes
+            slot.busy = None
+            done += batch
+        self.completed += done
+        return done
+
+    def _launch(self, slot: _Slot, batch: list) -> None:
+        torch = self.torch
+        t = time.perf_counter()
+        for r in batch:
+            r.t_launch = t
+        with torch.cuda.stream(slot.stream):
+            if batch[0].op == "czt_zoom":
+                nbytes = request_bytes(batch[0])
+                keep = self._run_czt(batch[0])
+            else:
+                nbytes = _prop_bytes(batch[0].side, len(batch))
+                keep = self._run_prop(slot, batch)
+            ev = torch.cuda.Event()
+            ev.record(slot.stream)
+        self.inflight_bytes += nbytes
+        slot.busy = (ev, batch, nbytes, keep)
+
+    def _run_prop(self, slot: _Slot, batch: list):
+        torch = self.torch
+        N = batch[0].side
+        B = len(batch)
+        planes = np.zeros(B, dtype=nat.PLANE_DTYPE)
+        for i, r in enumerate(batch):
+            planes[i]["z"] = r.z
+            planes[i]["wavelength"] = r.wavelength
+            planes[i]["dy"] = planes[i]["dx"] = r.dx
+            planes[i]["in_plane"] = i
+            r.out = torch.empty((N, N), dtype=torch.complex64, device=self.device)
+        ptrs = np.array([r.u.data_ptr() for r in batch] + [r.out.data_ptr() for r in batch], dtype=np.uint64)
+        pb = planes.view(np.uint8)
+        off_p = (pb.size + 15) // 16 * 16
+        host = slot.pinned.numpy()
+        host[: pb.size] = pb
+        host[off_p: off_p + ptrs.nbytes] = ptrs.view(np.uint8)
+        n_up = off_p + ptrs.nbytes
+        slot.dev[:n_up].copy_(slot.pinned[:n_up], non_blocking=True)
+        d = nat.cx_prop2d_desc()
+        d.ny = d.nx = N
+        d.pad_y = d.pad_x = N // 2
+        d.n_wv = 1
+        d.n_in_planes = d.n_out_planes = B
+        d.mode_same = 1
+        d.kernel = nat.CX_KERNEL_ASM if batch[0].op == "asm" else nat.CX_KERNEL_TRANSFER
+        d.precision = config.precision_code(self.precision)
+        d.n_medium = float(batch[0].n)
+        wsb = nat.c_size_t(0)
+        nat.check(self.L.cx_prop2d_workspace_size(d, wsb))
+        ws = torch.empty(max(wsb.value, 256), dtype=torch.uint8, device=self.device)
+        base = slot.dev.data_ptr()
+        nat.check(self.L.cx_prop2d_ptrs(d, base, base + off_p, base + off_p + 8 * B, None, ws.data_ptr(),
+                                        wsb.value, slot.stream.cuda_stream))
+        for r in batch:
+            r.u.record_stream(slot.stream)
+        return ws
+
+    def _run_czt(self, r: Request):
+        from .core.field import Field
+        from .functional.propagation import asm_propagate
+
+        f = Field.build(r.u, r.dx, r.wavelength)
+        out = asm_propagate(f, r.z, r.n, r.side // 2, output_dx=np.array([r.dx / r.zoom] * 2), output_shape=r.out_shape,
+                            precision=self.precision)
+        r.out = out.u
+        r.u.record_stream(self.torch.cuda.current_stream(self.device))
+        return out

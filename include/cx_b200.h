@@ -92,6 +92,17 @@ cx_status cx_prop2d_workspace_size(const cx_prop2d_desc* d, size_t* bytes);
 cx_status cx_prop2d(const cx_prop2d_desc* d, const cx_plane* planes_dev, const void* u_in, void* u_out,
                     const void* H, void* workspace, size_t workspace_bytes, cx_stream_t stream);
 
+/* cx_prop2d over a batch of fields at independent addresses: element b of the
+ * input batch (ny, nx, n_wv interleaved) starts at u_in_ptrs_dev[b], element b
+ * of the output batch at u_out_ptrs_dev[b]; both arrays live in DEVICE
+ * memory, with n_in_planes / n_wv and n_out_planes / n_wv entries.  The
+ * planes' in_plane indices refer to positions in the input batch.  Used by
+ * the continuous-batching server, whose requests own separate buffers.  No
+ * counterpart in the reference (jax batches through vmap). */
+cx_status cx_prop2d_ptrs(const cx_prop2d_desc* d, const cx_plane* planes_dev, const void* const* u_in_ptrs_dev,
+                         void* const* u_out_ptrs_dev, const void* H, void* workspace, size_t workspace_bytes,
+                         cx_stream_t stream);
+
 /* compute_transfer_propagator / compute_asm_propagator
  * (functional/propagation.py:466-496, 499-580): writes the ifftshifted
  * propagator, planar (n_out_planes, py, px) complex64, py/px = padded size. */

@@ -39,7 +39,8 @@ def test_czt_against_scipy_and_general_a_w():
     from chromatix_b200.utils import czt
 
     rng = np.random.default_rng(0)
-    for (n, m) in [(100, 10), (37, 211), (1024, 512), (5, 3)]:
+    # the last two need Bluestein lengths above 4096 (4608 and 6144)
+    for (n, m) in [(100, 10), (37, 211), (1024, 512), (5, 3), (4096, 512), (3000, 3000)]:
         x = (rng.standard_normal((7, n)) + 1j * rng.standard_normal((7, n))).astype(np.complex64)
         a = np.exp(1j * 0.3)
         w = np.exp(-1j * 2 * np.pi / (1.7 * n))
