@@ -378,6 +378,19 @@ def serve_arm(args):
             srv.submit(Request(op=op, u=fields[N][0], dx=0.3, z=100.0, wavelength=0.5, zoom=2.0))
     srv.drain()
     torch.cuda.synchronize(dev)
+    # device time of each (op, N) request run alone (3 repeats): the offered
+    # device load of the stream is rate * the mean over the uniform mix
+    service = {}
+    for op in SERVE_OPS:
+        for N in SERVE_SIDES:
+            srv.gpu_ms.clear()
+            for _ in range(3):
+                srv.submit(Request(op=op, u=fields[N][1], dx=0.3, z=250.0, wavelength=0.55, zoom=1.7))
+                srv.drain()
+            service[f"{op}/{N}"] = round(srv.gpu_ms[op] / 3, 4)
+    offered_load = args.rate * float(np.mean(list(service.values()))) / 1e3
+    for c in (srv.host_s, srv.gpu_ms, srv.batches):
+        c.clear()
     if dist:
         dist.barrier()
     n_req = max(1, int(args.rate * args.serve_seconds))
@@ -391,7 +404,8 @@ def serve_arm(args):
             while i < n_req and arrivals[i] <= now:
                 reqs.append(srv.submit(make(t0 + arrivals[i])))
                 i += 1
-            srv.step()
+            for r in srv.step():
+                r.out = None  # the client consumes the result: its buffer returns to the pool
         torch.cuda.synchronize(dev)
         t_end = time.perf_counter()
     elapsed = t_end - t0
@@ -419,6 +433,10 @@ def serve_arm(args):
             "latency_ms": {"p50": round(p50, 3), "p99": round(p99, 3), "mean": round(float(lat.mean()), 3),
                            "p99_by_op": by_op},
             "requests": n_req * world, "achieved_req_s": round(n_req * world / elapsed, 1),
+            "service_ms_alone": service, "offered_device_load": round(offered_load, 3),
+            "launch_host_ms_by_op": {k: round(v * 1e3, 1) for k, v in srv.host_s.items()},
+            "device_ms_by_op": {k: round(v, 1) for k, v in srv.gpu_ms.items()},
+            "batches_by_op": dict(srv.batches),
             "clocks": clk.summary(),
         }
         print(json.dumps(line), flush=True)

@@ -224,11 +224,18 @@ def workspace(nbytes: int, device):
     return torch.empty(max(int(nbytes), 256), dtype=torch.uint8, device=device)
 
 
-def to_device_bytes(arr: np.ndarray, device):
-    """Copy a numpy (structured) array to device memory as raw bytes."""
+def upload(arr: np.ndarray, device):
+    """Host array -> device tensor through page-locked memory, asynchronous on
+    the current stream: the host does not wait for the stream (a pageable
+    blocking copy would synchronise it, serialising host and device)."""
     torch = torch_mod()
-    b = np.ascontiguousarray(arr).view(np.uint8).reshape(-1)
-    return torch.from_numpy(b.copy()).to(device, non_blocking=False)
+    t = torch.from_numpy(np.ascontiguousarray(arr)).pin_memory()
+    return t.to(device, non_blocking=True)
+
+
+def to_device_bytes(arr: np.ndarray, device):
+    """Copy a numpy (structured) array to device memory as raw bytes (asynchronously)."""
+    return upload(np.ascontiguousarray(arr).view(np.uint8).reshape(-1), device)
 
 
 _copy_streams = {}

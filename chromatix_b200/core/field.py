@@ -201,8 +201,7 @@ class Field:
         W = self.n_wv if self.chromatic else 1
         out_shape = u.shape[:-1] if self.chromatic else u.shape
         out = torch.empty(out_shape, dtype=torch.float32, device=u.device)
-        dens = torch.as_tensor(np.asarray(self.spectrum.density, np.float64) if self.chromatic else np.ones(1),
-                               device=u.device)
+        dens = nat.upload(np.asarray(self.spectrum.density, np.float64) if self.chromatic else np.ones(1), u.device)
         n_pix = out.numel()
         nat.check(nat.lib().cx_intensity(nat.ptr(u), n_pix, W, nat.ptr(dens), nat.ptr(out),
                                          nat.stream_handle(u.device)))

@@ -80,6 +80,9 @@ def rescaled_propagate(field: Field, kernel: int, z, n, pad_width, kykx=(0.0, 0.
     pad = _pad_tuple(pad_width)
     ny, nx = field.spatial_shape
     py, px = ny + 2 * pad[0], nx + 2 * pad[1]
+    if not bandlimit:
+        return _rescaled_one_call(field, kernel, z, n, pad, kykx, shift_yx, output_dx, output_shape, mode,
+                                  remove_evanescent, pad_width, prec)
     # propagator of the padded field (asm: shift handled by the CZT grid, not in H)
     if kernel == nat.CX_KERNEL_ASM:
         H = _fill_propagator(field, kernel, z, n, kykx, (0.0, 0.0), bandlimit, remove_evanescent, prec, shape=(py, px))
@@ -109,6 +112,73 @@ def rescaled_propagate(field: Field, kernel: int, z, n, pad_width, kykx=(0.0, 0.
         N = (m[d] - 1) // 2
         scale = 1.0 / float(np.prod(alpha)) if d == 1 else 1.0
         u = czt_axis(u, m[d], a, w, axis=u.ndim + spatial[d], mod_n=N, scale=scale)
+    out = shift_grid(field, sh)
+    dx_new = dx_out.reshape(field.dx.shape) if np.size(field.dx) == 2 else np.broadcast_to(dx_out, field.dx.shape)
+    out = out.replace(u=u, dx=np.array(dx_new, dtype=np.float64))
+    if mode == "same":
+        out = crop(out, pad_width)
+    return out
+
+
+class cx_czt_prop_desc(nat.ctypes.Structure):
+    _fields_ = [(k, nat.c_int32) for k in ("ny", "nx", "pad_y", "pad_x", "my", "mx", "n_fields", "kernel",
+                                           "precision", "remove_evanescent", "bandlimit", "reserved")] + \
+               [(k, nat.c_double) for k in ("n_medium", "z", "wavelength", "dy_in", "dx_in", "dy_out", "dx_out",
+                                            "shift_y", "shift_x", "ky0", "kx0")]
+
+
+def _czt_prop_sigs(L):
+    if not hasattr(L, "_cx_czt_propagate_sig"):
+        P = nat.ctypes.POINTER(cx_czt_prop_desc)
+        L.cx_czt_propagate_workspace_size.restype = nat.c_int32
+        L.cx_czt_propagate_workspace_size.argtypes = [P, nat.ctypes.POINTER(nat.c_size_t)]
+        L.cx_czt_propagate.restype = nat.c_int32
+        L.cx_czt_propagate.argtypes = [P, nat.c_void_p, nat.c_void_p, nat.c_void_p, nat.c_size_t, nat.c_void_p]
+        L._cx_czt_propagate_sig = True
+    return L
+
+
+def _rescaled_one_call(field: Field, kernel, z, n, pad, kykx, shift_yx, output_dx, output_shape, mode,
+                       remove_evanescent, pad_width, prec) -> Field:
+    """The whole CZT branch as one native call (``cx_czt_propagate``)."""
+    torch = nat.torch_mod()
+    L = _czt_prop_sigs(nat.lib())
+    ny, nx = field.spatial_shape
+    py, px = ny + 2 * pad[0], nx + 2 * pad[1]
+    m = (py, px) if output_shape is None else (int(output_shape[0]), int(output_shape[1]))
+    dx_in = field.dx_wv[0]
+    if output_dx is None:
+        dx_out = dx_in.copy()
+    else:
+        if np.ndim(output_dx) != np.ndim(field.dx):
+            # Field.empty_like (core/field.py:333-337)
+            raise AssertionError("New spacing must have same number of dimensions as old spacing")
+        dx_out = np.asarray(output_dx, dtype=np.float64).reshape(-1, 2)[0].copy()
+    sh = np.broadcast_to(np.asarray(shift_yx, dtype=np.float64).reshape(-1), (2,))
+    B = field.batch_shape
+    nb = int(np.prod(B)) if B else 1
+    d = cx_czt_prop_desc()
+    d.ny, d.nx, d.pad_y, d.pad_x = ny, nx, pad[0], pad[1]
+    d.my, d.mx = m
+    d.n_fields = nb
+    d.kernel = kernel
+    d.precision = config.precision_code(prec)
+    d.remove_evanescent = int(bool(remove_evanescent))
+    d.n_medium, d.z, d.wavelength = float(n), float(z), float(field.spectrum.wavelength[0])
+    d.dy_in, d.dx_in = float(dx_in[0]), float(dx_in[1])
+    d.dy_out, d.dx_out = float(dx_out[0]), float(dx_out[1])
+    d.shift_y, d.shift_x = float(sh[0]), float(sh[1])
+    ky0, kx0 = np.asarray(kykx, dtype=np.float64).reshape(2)
+    d.ky0, d.kx0 = float(ky0), float(kx0)
+    wsb = nat.c_size_t(0)
+    nat.check(L.cx_czt_propagate_workspace_size(d, wsb))
+    ws = nat.workspace(wsb.value, field.device)
+    u_in = field.u.contiguous()
+    spatial_last = not field.chromatic
+    u = torch.empty(tuple(B) + tuple(m) + (() if spatial_last else (1,)), dtype=torch.complex64,
+                    device=field.device)
+    nat.check(L.cx_czt_propagate(d, nat.ptr(u_in), nat.ptr(u), nat.ptr(ws), wsb.value,
+                                 nat.stream_handle(field.device)))
     out = shift_grid(field, sh)
     dx_new = dx_out.reshape(field.dx.shape) if np.size(field.dx) == 2 else np.broadcast_to(dx_out, field.dx.shape)
     out = out.replace(u=u, dx=np.array(dx_new, dtype=np.float64))

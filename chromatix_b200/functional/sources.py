@@ -146,7 +146,7 @@ class LazySourceField(Field):
         r = self._recipe
         if r.get("z_dev") is not None:
             return r["z_dev"]
-        return torch.as_tensor(np.ascontiguousarray(r["z"], dtype=np.float64), device=self._device)
+        return nat.upload(np.ascontiguousarray(r["z"], dtype=np.float64), self._device)
 
     def _source_field(self) -> Field:
         """Materialise the source (+ phase) stage."""

@@ -154,6 +154,19 @@ class _Slot:
         self.pinned = torch.empty(staging_bytes, dtype=torch.uint8).pin_memory()
         self.dev = torch.empty(staging_bytes, dtype=torch.uint8, device=device)
         self.busy = None  # (event, batch, bytes, keepalive) of the batch in flight
+        self.ws = None  # workspace, grown to the largest batch this stream has run
+        self._torch = torch
+        self._device = device
+
+    def workspace(self, nbytes: int, reserve: int = 0):
+        """At least ``nbytes``; a regrowth allocates ``reserve`` bytes at once
+        (the largest batch of that shape), so a stream regrows at most once
+        per request shape instead of on every larger batch."""
+        if self.ws is None or self.ws.numel() < nbytes:
+            self.ws = None
+            self.ws = self._torch.empty(max(int(nbytes), int(reserve), 256), dtype=self._torch.uint8,
+                                        device=self._device)
+        return self.ws
 
 
 class PropagationServer:
@@ -174,6 +187,12 @@ class PropagationServer:
         self.inflight_bytes = 0
         self.completed: list = []
         self._next_id = 0
+        # per-op totals: host seconds spent launching, device ms between the
+        # batch's first and last kernel (streams overlap, so these can exceed
+        # wall time), batches
+        self.host_s = collections.Counter()
+        self.gpu_ms = collections.Counter()
+        self.batches = collections.Counter()
         L = nat.lib()
         if not hasattr(L, "_cx_prop2d_ptrs_sig"):
             L.cx_prop2d_ptrs.restype = nat.c_int32
@@ -226,10 +245,11 @@ class PropagationServer:
         for slot in self.slots:
             if slot.busy is None:
                 continue
-            ev, batch, nbytes, _keep = slot.busy
+            ev, batch, nbytes, keep = slot.busy
             if not ev.query():
                 continue
             t = time.perf_counter()
+            self.gpu_ms[batch[0].op] += keep[0].elapsed_time(ev)
             for r in batch:
                 r.t_done = t
             self.inflight_bytes -= nbytes
@@ -244,27 +264,32 @@ class PropagationServer:
         for r in batch:
             r.t_launch = t
         with torch.cuda.stream(slot.stream):
+            # recorded just before the batch's kernels are issued (device time only)
+            slot.ev0 = ev0 = torch.cuda.Event(enable_timing=True)
             if batch[0].op == "czt_zoom":
                 nbytes = request_bytes(batch[0])
-                keep = self._run_czt(batch[0])
+                keep = self._run_czt(slot, batch[0])
             else:
                 nbytes = _prop_bytes(batch[0].side, len(batch))
                 keep = self._run_prop(slot, batch)
-            ev = torch.cuda.Event()
+            ev = torch.cuda.Event(enable_timing=True)
             ev.record(slot.stream)
         self.inflight_bytes += nbytes
-        slot.busy = (ev, batch, nbytes, keep)
+        slot.busy = (ev, batch, nbytes, (ev0, keep))
+        op = batch[0].op
+        self.host_s[op] += time.perf_counter() - t
+        self.batches[op] += 1
 
     def _run_prop(self, slot: _Slot, batch: list):
         torch = self.torch
         N = batch[0].side
         B = len(batch)
         planes = np.zeros(B, dtype=nat.PLANE_DTYPE)
-        for i, r in enumerate(batch):
-            planes[i]["z"] = r.z
-            planes[i]["wavelength"] = r.wavelength
-            planes[i]["dy"] = planes[i]["dx"] = r.dx
-            planes[i]["in_plane"] = i
+        planes["z"] = [r.z for r in batch]
+        planes["wavelength"] = [r.wavelength for r in batch]
+        planes["dy"] = planes["dx"] = [r.dx for r in batch]
+        planes["in_plane"] = np.arange(B)
+        for r in batch:
             r.out = torch.empty((N, N), dtype=torch.complex64, device=self.device)
         ptrs = np.array([r.u.data_ptr() for r in batch] + [r.out.data_ptr() for r in batch], dtype=np.uint64)
         pb = planes.view(np.uint8)
@@ -285,21 +310,39 @@ class PropagationServer:
         d.n_medium = float(batch[0].n)
         wsb = nat.c_size_t(0)
         nat.check(self.L.cx_prop2d_workspace_size(d, wsb))
-        ws = torch.empty(max(wsb.value, 256), dtype=torch.uint8, device=self.device)
+        ws = slot.workspace(wsb.value, reserve=(wsb.value // B + 512) * self.max_batch)
         base = slot.dev.data_ptr()
+        slot.ev0.record(slot.stream)
         nat.check(self.L.cx_prop2d_ptrs(d, base, base + off_p, base + off_p + 8 * B, None, ws.data_ptr(),
                                         wsb.value, slot.stream.cuda_stream))
         for r in batch:
             r.u.record_stream(slot.stream)
-        return ws
+        return None
 
-    def _run_czt(self, r: Request):
-        from .core.field import Field
-        from .functional.propagation import asm_propagate
+    def _run_czt(self, slot: _Slot, r: Request):
+        """``asm_propagate(..., output_dx=dx/zoom, output_shape=out_shape)`` as
+        one ``cx_czt_propagate`` call (the path the functional API takes)."""
+        from .functional.rescaled import _czt_prop_sigs, cx_czt_prop_desc
 
-        f = Field.build(r.u, r.dx, r.wavelength)
-        out = asm_propagate(f, r.z, r.n, r.side // 2, output_dx=np.array([r.dx / r.zoom] * 2), output_shape=r.out_shape,
-                            precision=self.precision)
-        r.out = out.u
-        r.u.record_stream(self.torch.cuda.current_stream(self.device))
-        return out
+        torch = self.torch
+        L = _czt_prop_sigs(self.L)
+        N = r.side
+        d = cx_czt_prop_desc()
+        d.ny = d.nx = N
+        d.pad_y = d.pad_x = N // 2
+        d.my, d.mx = int(r.out_shape[0]), int(r.out_shape[1])
+        d.n_fields = 1
+        d.kernel = nat.CX_KERNEL_ASM
+        d.precision = config.precision_code(self.precision)
+        d.n_medium, d.z, d.wavelength = float(r.n), float(r.z), float(r.wavelength)
+        d.dy_in = d.dx_in = float(r.dx)
+        d.dy_out = d.dx_out = float(np.array([r.dx / r.zoom] * 2)[0])
+        wsb = nat.c_size_t(0)
+        nat.check(L.cx_czt_propagate_workspace_size(d, wsb))
+        ws = slot.workspace(wsb.value)
+        r.out = torch.empty((d.my, d.mx), dtype=torch.complex64, device=self.device)
+        slot.ev0.record(slot.stream)
+        nat.check(L.cx_czt_propagate(d, r.u.data_ptr(), r.out.data_ptr(), ws.data_ptr(), wsb.value,
+                                     slot.stream.cuda_stream))
+        r.u.record_stream(slot.stream)
+        return None

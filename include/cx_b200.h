@@ -303,6 +303,33 @@ cx_status cx_czt(const cx_czt_desc* d, const void* x, void* y, void* workspace, 
  *  - Results are identical to cx_czt's for the same descriptor and input. */
 cx_status cx_czt_noalloc(const cx_czt_desc* d, const void* x, void* y, cx_stream_t stream);
 
+/* Rescaled-output propagation in one call: the CZT branch of kernel_propagate
+ * (functional/propagation.py:395-443) as reached from transfer_propagate /
+ * asm_propagate with output_dx / output_shape (:168-352): propagator of the
+ * padded grid, fftshift(H fft2(ifftshift(pad u))), then a chirp-Z transform
+ * along y and along x onto the (my, mx) output grid of spacing (dy_out,
+ * dx_out) shifted by (shift_y, shift_x).  n_fields single-wavelength fields
+ * (ny, nx) complex64 sharing every parameter; u_out (n_fields, my, mx).
+ * Band-limited propagators are not supported here (CX_ERR_UNSUPPORTED). */
+typedef struct {
+  int32_t ny, nx;          /* input shape */
+  int32_t pad_y, pad_x;    /* zero padding on each side */
+  int32_t my, mx;          /* output shape (>= 2 each) */
+  int32_t n_fields;
+  int32_t kernel;          /* CX_KERNEL_TRANSFER or CX_KERNEL_ASM */
+  int32_t precision;       /* cx_precision */
+  int32_t remove_evanescent, bandlimit;
+  int32_t reserved;
+  double n_medium, z, wavelength;
+  double dy_in, dx_in, dy_out, dx_out;
+  double shift_y, shift_x;
+  double ky0, kx0;
+} cx_czt_prop_desc;
+
+cx_status cx_czt_propagate_workspace_size(const cx_czt_prop_desc* d, size_t* bytes);
+cx_status cx_czt_propagate(const cx_czt_prop_desc* d, const void* u_in, void* u_out, void* workspace,
+                           size_t workspace_bytes, cx_stream_t stream);
+
 /* ---------------------------------------------------------------------------
  * Modified Born series (experimental/modified_born_series/solver.py:42-146)
  * Grid (X, Y, Z); fields are three component planes (3, X, Y, Z) complex64;
