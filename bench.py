@@ -329,6 +329,232 @@ def accuracy_check(dev):
 
 
 # ---------------------------------------------------------------------------
+# secondary workloads (one JSON line each; parity cases of the other configs)
+# ---------------------------------------------------------------------------
+def _device_timer(torch, dev, steps, warmup, flush_bytes=256 << 20):
+    flush = torch.empty(flush_bytes // 4, dtype=torch.float32, device=dev)
+
+    def run(fn):
+        for _ in range(warmup):
+            fn()
+        torch.cuda.synchronize(dev)
+        st = torch.cuda.current_stream(dev)
+        total = 0.0
+        for _ in range(steps):
+            flush.fill_(1.0)  # evict L2 between steps (outside the timed events)
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(st)
+            fn()
+            e1.record(st)
+            e1.synchronize()
+            total += e0.elapsed_time(e1)
+        return total / steps
+
+    return run
+
+
+def _peak_hbm():
+    try:
+        pk = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+        return float(pk["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def _base_line(metric, value, unit, steps, warmup, ms, dtype, config, **kw):
+    line = {"metric": metric, "value": value, "unit": unit, "n_gpus": 1, "steps": steps, "warmup": warmup,
+            "ms_per_step": round(ms, 4), "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": dtype, "data": "synthetic (seeded)", "config": config}
+    line.update(kw)
+    return line
+
+
+def psf_published_arm(args):
+    """The reference's own published PSF benchmark configuration
+    (examples/parallel_psf.py:10-44, docs/parallelism.md:53-81): 128 planes
+    z = linspace(-4, 4), 1536^2, spacing 0.3 um, lambda 0.532 um, f = 100 um,
+    n = 1.33, NA 0.8, PhaseMask(ones), FFLens(f, n), intensity; published
+    25.06 ms on one A100 (device-resident inputs, block_until_ready)."""
+    import torch
+
+    import chromatix_b200.functional as cf
+
+    dev = torch.device("cuda", 0)
+    n_z, N = 128, 1536
+    z = torch.linspace(-4, 4, n_z, dtype=torch.float64, device=dev)
+    ones = torch.ones((N, N), dtype=torch.float32, device=dev)
+
+    def step():
+        f = cf.objective_point_source((N, N), 0.3, 0.532, z, 100.0, 1.33, 0.8, device=dev)
+        return cf.ff_lens(cf.phase_change(f, ones), 100.0, 1.33).intensity
+
+    with ClockSampler(0) as clk:
+        ms = _device_timer(torch, dev, args.steps, args.warmup)(step)
+    px = n_z * N * N
+    published_ms = 25.06
+    value = px / (ms * 1e-3) / 1e6
+    line = _base_line("Mpx/s, widefield PSF (the reference's published configuration)", round(value, 1), "Mpx/s",
+                      args.steps, args.warmup, ms, "c64/f32",
+                      {"workload": "objective_point_source 1536x1536, 128 z in [-4,4] um, lambda 0.532, f 100 um, "
+                                   "n 1.33, NA 0.8, PhaseMask(ones), FFLens, intensity",
+                       "l2": "flushed between timed steps"},
+                      vs_baseline=round(value / (px / (published_ms * 1e-3) / 1e6), 2),
+                      baseline={"ms": published_ms, "hardware": "1x A100 (docs/parallelism.md:79)"},
+                      clocks=clk.summary())
+    print(json.dumps(line), flush=True)
+
+
+def asm_arm(args):
+    """Single-field angular-spectrum / Fresnel-transfer propagation: 512^2
+    complex64 A exp(i phi), A ~ U[0.5, 1], phi ~ U[0, 2 pi), dx 0.3 um,
+    lambda 0.532 um, n 1.33, z 100 um, pad 256 (1024^2 FFT), mode "full";
+    one field and a batch of 64 independent fields."""
+    import torch
+
+    import chromatix_b200.functional as cf
+    from chromatix_b200.core.field import ScalarField
+    from chromatix_b200.core.spectrum import Spectrum
+
+    dev = torch.device("cuda", 0)
+    rng = np.random.default_rng(0)
+    hbm, src = _peak_hbm()
+    res = {}
+    for B in (1, 64):
+        a = rng.uniform(0.5, 1.0, (B, 512, 512))
+        ph = rng.uniform(0, 2 * np.pi, (B, 512, 512))
+        u = torch.as_tensor((a * np.exp(1j * ph)).astype(np.complex64), device=dev)
+        f = ScalarField(u if B > 1 else u[0], 0.3, 0.0, Spectrum.build(0.532))
+        for kind in ("asm_propagate", "transfer_propagate"):
+            fn = getattr(cf, kind)
+            ms = _device_timer(torch, dev, args.steps, args.warmup)(lambda: fn(f, 100.0, 1.33, 256))
+            alg = B * (512 * 512 * 8 + 1024 * 1024 * 8)
+            res[f"{kind}/batch{B}"] = {"ms": round(ms, 4), "Mpx_s": round(B * 1024 * 1024 / (ms * 1e-3) / 1e6, 1),
+                                       "achieved_GBs": round(alg / (ms * 1e-3) / 1e9, 1),
+                                       "frac": round(alg / (ms * 1e-3) / 1e9 / hbm, 4)}
+    main = res["asm_propagate/batch64"]
+    line = _base_line("Mpx/s, ASM propagation 512^2 -> 1024^2 (batch 64)", main["Mpx_s"], "Mpx/s", args.steps,
+                      args.warmup, main["ms"], "c64 (FP64 phase arguments)",
+                      {"workload": "asm/transfer_propagate 512x512, pad 256, z 100 um, lambda 0.532, n 1.33, dx 0.3, "
+                                   "mode full", "l2": "flushed between timed steps"},
+                      roofline={"bound": "hbm", "achieved": main["achieved_GBs"], "peak": hbm, "unit": "GB/s",
+                                "frac": main["frac"], "peak_source": src,
+                                "algorithmic_bytes_per_field": 512 * 512 * 8 + 1024 * 1024 * 8},
+                      cases=res)
+    print(json.dumps(line), flush=True)
+
+
+def multislice_arm(args):
+    """Differentiable multislice: 256 slices of 1024^2, dn = Gaussian-filtered
+    (sigma 4 px, periodic) N(0, 0.02), alpha ~ U[0, 0.05] (absorption =
+    alpha / (k0 dz)), dz 0.2 um, spacing 0.1 um, lambda 0.532 um, n 1.33,
+    plane-wave input, L2 loss against a seeded target intensity, forward plus
+    adjoint gradient w.r.t. dn, checkpoint every 16 slices."""
+    import torch
+
+    import chromatix_b200.functional as cf
+
+    dev = torch.device("cuda", 0)
+    D, N, dz, lam = 256, 1024, 0.2, 0.532
+    g = torch.Generator(device=dev)
+    g.manual_seed(0)
+    dn = torch.randn((D, N, N), generator=g, device=dev) * 0.02
+    f = torch.fft.fftfreq(N, device=dev)
+    gauss = torch.exp(-2 * (np.pi * 4.0) ** 2 * (f[:, None] ** 2 + f[None, :] ** 2))
+    for i in range(D):  # periodic Gaussian filter, slice by slice
+        dn[i] = torch.fft.ifft2(torch.fft.fft2(dn[i]) * gauss).real
+    k0 = 2 * np.pi / lam
+    ab = torch.rand((D, N, N), generator=g, device=dev) * (0.05 / (k0 * dz))
+    g.manual_seed(1)
+    target = torch.rand((N, N), generator=g, device=dev)
+    field = cf.plane_wave((N, N), 0.1, lam, device=dev)
+    dn_p = dn.clone().requires_grad_(True)
+
+    def step():
+        dn_p.grad = None
+        out = cf.multislice_thick_sample(field, ab, dn_p, 1.33, dz, 0, checkpoint_every=16)
+        loss = ((out.u.real ** 2 + out.u.imag ** 2 - target) ** 2).sum()
+        loss.backward()
+        return loss
+
+    def fwd():
+        with torch.no_grad():
+            return cf.multislice_thick_sample(field, ab, dn, 1.33, dz, 0)
+
+    hbm, src = _peak_hbm()
+    with ClockSampler(0) as clk:
+        ms = _device_timer(torch, dev, args.steps, args.warmup)(step)
+    ms_f = _device_timer(torch, dev, args.steps, args.warmup)(fwd)
+    units = D * N * N
+    alg, alg_f = 84 * units, 24 * units
+    line = _base_line("Mpx-slices/s, multislice forward + adjoint gradient", round(units / (ms * 1e-3) / 1e6, 1),
+                      "Mpx-slices/s", args.steps, args.warmup, ms, "c64/f32 (FP64 propagator)",
+                      {"workload": "multislice 256 x 1024^2, dz 0.2, dx 0.1, lambda 0.532, n 1.33, plane wave, L2 "
+                                   "loss, grad w.r.t. dn, checkpoint every 16", "l2": "inputs larger than L2"},
+                      roofline={"bound": "hbm", "achieved": round(alg / (ms * 1e-3) / 1e9, 1), "peak": hbm,
+                                "unit": "GB/s", "frac": round(alg / (ms * 1e-3) / 1e9 / hbm, 4), "peak_source": src,
+                                "algorithmic_bytes_per_step": alg},
+                      forward={"ms": round(ms_f, 4), "Mpx_slices_s": round(units / (ms_f * 1e-3) / 1e6, 1),
+                               "achieved_GBs": round(alg_f / (ms_f * 1e-3) / 1e9, 1),
+                               "frac": round(alg_f / (ms_f * 1e-3) / 1e9 / hbm, 4)},
+                      clocks=clk.summary())
+    print(json.dumps(line), flush=True)
+
+
+def mbs_arm(args):
+    """Modified Born series: 256^3 grid of 200 random spheres (radius U[0.5, 3]
+    um, n U[1.36, 1.45]) in n = 1.33, spacing 0.1 um, lambda 0.5 um, 32-voxel
+    absorbing boundary on every face (320^3), y-polarised current sheet at
+    x-index 34, iterated to a relative residual below 1e-5 (FP64 residual)."""
+    import torch
+
+    from chromatix_b200.experimental import mbs
+
+    dev = torch.device("cuda", 0)
+    rng = np.random.default_rng(0)
+    n_in, sp, lam = 256, 0.1, 0.5
+    ax = (torch.arange(n_in, device=dev, dtype=torch.float32) - n_in // 2) * sp
+    n = torch.full((n_in, n_in, n_in), 1.33, device=dev)
+    for _ in range(200):
+        c = rng.uniform(ax[0].item(), ax[-1].item(), 3)
+        r = rng.uniform(0.5, 3.0)
+        ni = rng.uniform(1.36, 1.45)
+        m = ((ax[:, None, None] - c[0]) ** 2 + (ax[None, :, None] - c[1]) ** 2 + (ax[None, None, :] - c[2]) ** 2) <= r * r
+        n[m] = ni
+    sample = mbs.add_absorbing_bc(mbs.Sample((n ** 2).to(torch.complex64), sp), (0, 1, 2), 3.2, 0.25, 1.33)
+    X = sample.shape[0]
+    J = torch.zeros(sample.shape + (3,), dtype=torch.complex64, device=dev)
+    J[34, :, :, 1] = 1.0
+    src = mbs.Source(J, 2 * np.pi / lam)
+    torch.cuda.synchronize(dev)
+    with ClockSampler(0) as clk:
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        E, info = mbs.solve(sample, src, maxiter=args.mbs_maxiter, tol=0.0, rtol=1e-5, return_info=True)
+        e1.record()
+        e1.synchronize()
+    ms = e0.elapsed_time(e1)
+    it = info["iterations"]
+    loop_ms = info["loop_ms"]
+    hbm, srcp = _peak_hbm()
+    vox = X ** 3
+    alg = 2.62e9 * (vox / 320 ** 3)
+    per_it = loop_ms / it
+    line = _base_line("Mvoxel-iterations/s, modified Born series", round(vox * it / (ms * 1e-3) / 1e6, 1),
+                      "Mvoxel-iterations/s", it, 0, ms, "c64 (FP64 residual)",
+                      {"workload": "MBS 256^3 + 32-voxel absorbing boundary (320^3), 200 spheres, spacing 0.1, "
+                                   "lambda 0.5, current sheet, to relative residual < 1e-5", "l2": "inputs larger than L2"},
+                      iterations=it, residual_rel=info["residual_rel"], converged=info["residual_rel"] < 1e-5,
+                      ms_per_iteration=round(per_it, 4), iteration_loop_ms=round(loop_ms, 2),
+                      setup_ms=round(ms - loop_ms, 2),
+                      roofline={"bound": "hbm", "achieved": round(alg / (per_it * 1e-3) / 1e9, 1), "peak": hbm,
+                                "unit": "GB/s", "frac": round(alg / (per_it * 1e-3) / 1e9 / hbm, 4),
+                                "peak_source": srcp, "algorithmic_bytes_per_iteration": alg},
+                      clocks=clk.summary())
+    print(json.dumps(line), flush=True)
+
+
+# ---------------------------------------------------------------------------
 # serving workload: Poisson stream of mixed propagation requests
 # ---------------------------------------------------------------------------
 SERVE_SIDES = (256, 512, 1024, 2048)
@@ -515,8 +741,11 @@ def main():
     ap.add_argument("--cpu-sample-z", type=int, default=2)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--accuracy", action="store_true", help="also report the error vs the FP64 oracle")
-    ap.add_argument("--workload", default="psf", choices=["psf", "serve"],
-                    help="psf: the batched 4f PSF stack (headline); serve: the Poisson request stream")
+    ap.add_argument("--workload", default="psf",
+                    choices=["psf", "serve", "psf_published", "asm", "multislice", "mbs"],
+                    help="psf: the batched 4f PSF stack (headline); the others print one line each for the "
+                         "other configurations")
+    ap.add_argument("--mbs-maxiter", type=int, default=4000)
     ap.add_argument("--rate", type=float, default=2000.0, help="serve: mean arrivals per second")
     ap.add_argument("--serve-seconds", type=float, default=2.0, help="serve: length of the arrival stream")
     args = ap.parse_args()
@@ -526,6 +755,14 @@ def main():
         reference_arm(args)
     elif args.workload == "serve":
         serve_arm(args)
+    elif args.workload == "psf_published":
+        psf_published_arm(args)
+    elif args.workload == "asm":
+        asm_arm(args)
+    elif args.workload == "multislice":
+        multislice_arm(args)
+    elif args.workload == "mbs":
+        mbs_arm(args)
     else:
         gpu_arm(args)
 

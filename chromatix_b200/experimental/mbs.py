@@ -233,18 +233,27 @@ def solve(sample: Sample, source: Source, initial_E=None, maxiter: int = 1000, t
     x = prec_y.clone() if initial_E is None else _planes(initial_E.to(torch.complex64)) / num_scale
     x_new = torch.empty_like(x)
     acc = torch.zeros(2, dtype=torch.float64, device=dev)
+    acc_h = torch.zeros(2, dtype=torch.float64).pin_memory()
+    done = torch.cuda.Event()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ev0.record()
     it, res_abs, res_rel = 0, float("inf"), float("inf")
     for it in range(1, maxiter + 1):
         nat.check(L.cx_mbs_iterate(d, nat.ptr(eps), nat.ptr(prec_y), nat.ptr(x), nat.ptr(x_new), nat.ptr(acc),
                                    nat.ptr(ws), ws_b.value, st))
         x, x_new = x_new, x
-        a = acc.cpu().numpy()
+        acc_h.copy_(acc, non_blocking=True)
+        done.record()
+        done.synchronize()
+        a = acc_h.numpy()
         res_abs = math.sqrt(a[0])
         res_rel = math.sqrt(a[0] / a[1]) if a[1] > 0 else float("inf")
         if res_abs <= tol or (rtol is not None and res_rel < rtol):
             break
+    ev1.record()
     E = (x * num_scale).movedim(0, -1).contiguous()
     if return_info:
+        ev1.synchronize()
         return E, {"iterations": it, "residual_abs": res_abs, "residual_rel": res_rel, "shift": shift,
-                   "scale": scale, "num_scale": num_scale}
+                   "scale": scale, "num_scale": num_scale, "loop_ms": ev0.elapsed_time(ev1)}
     return E
