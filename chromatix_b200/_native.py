@@ -27,6 +27,7 @@ CX_PREC_REF32 = 1
 CX_KERNEL_TRANSFER = 0
 CX_KERNEL_ASM = 1
 CX_KERNEL_EXPLICIT = 2
+CX_KERNEL_SAS = 3
 
 _STATUS = {
     0: "CX_OK",

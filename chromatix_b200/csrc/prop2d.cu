@@ -28,7 +28,7 @@ static cx_status make_args(const cx_prop2d_desc* d, Prop2DArgs* a) {
               d->pad_x, d->n_wv, d->n_in_planes, d->n_out_planes);
     return CX_ERR_INVALID;
   }
-  if (d->kernel < 0 || d->kernel > 2 || d->precision < 0 || d->precision > 1) {
+  if (d->kernel < 0 || d->kernel > 3 || d->precision < 0 || d->precision > 1) {
     set_error("invalid kernel kind or precision");
     return CX_ERR_INVALID;
   }

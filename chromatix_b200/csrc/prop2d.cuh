@@ -62,6 +62,23 @@ __device__ __forceinline__ float2 prop_kernel_accurate(int ky, int kx, const Pro
   }
   const double fy = (double)freq_index(ky, a.py) / ((double)a.py * pl.dy);
   const double fx = (double)freq_index(kx, a.px) / ((double)a.px * pl.dx);
+  if (a.kernel == CX_KERNEL_SAS) {
+    // Delta H = W exp(i kz (H_AS - H_Fr)), s = lam f / n, W the band limit
+    // s^2 (2 + 1/t^2) <= 1 per axis with t = extent / |z| + |s| (propagation.py:85-103)
+    const double lam = pl.wavelength, n = a.n_med;
+    const double sy = lam * fy / n, sx = lam * fx / n;
+    const double ty = (double)a.py * pl.dy / fabs(pl.z) + fabs(sy);
+    const double tx = (double)a.px * pl.dx / fabs(pl.z) + fabs(sx);
+    if (!(sy * sy * (2.0 + 1.0 / (ty * ty)) <= 1.0) || !(sx * sx * (2.0 + 1.0 / (tx * tx)) <= 1.0))
+      return make_float2(0.f, 0.f);
+    const double ss = sy * sy + sx * sx;
+    const double h_as = sqrt(1.0 - ss > 0.0 ? 1.0 - ss : 0.0);
+    const double h_fr = 1.0 - ss / 2.0;
+    const double ph = 2.0 * pl.z * pi * n / lam * (h_as - h_fr);
+    double sd, cd;
+    sincos(ph, &sd, &cd);
+    return make_float2((float)cd, (float)sd);
+  }
   const double gy = fy - a.ky0, gx = fx - a.kx0;
   const double s = gy * gy + gx * gx;
   if (a.kernel == CX_KERNEL_TRANSFER) {
@@ -104,6 +121,23 @@ __device__ __forceinline__ float2 prop_kernel_ref32(int ky, int kx, const Prop2D
   const float gy = fs(fy, (float)a.ky0), gx = fs(fx, (float)a.kx0);
   const float s = fa(fm(gy, gy), fm(gx, gx));
   const float lam = (float)pl.wavelength, n = (float)a.n_med, z = (float)pl.z;
+  if (a.kernel == CX_KERNEL_SAS) {
+    // float32 in the order of compute_sas_precompensation (propagation.py:90-102)
+    const float kz = fd(fm(fm(fm(2.f, z), PI), n), lam);
+    const float sy = fd(fm(lam, fy), n), sx = fd(fm(lam, fx), n);
+    const float qy = fm(sy, sy), qx = fm(sx, sx);
+    const float Ly = fm(2.f, fm((float)a.py, dyf)), Lx = fm(2.f, fm((float)a.px, dxf));
+    const float ty = fa(fd(fd(Ly, 2.f), fabsf(z)), fabsf(sy)), tx = fa(fd(fd(Lx, 2.f), fabsf(z)), fabsf(sx));
+    const bool wy = fm(qy, fa(2.f, fd(1.f, fm(ty, ty)))) <= 1.f;
+    const bool wx = fm(qx, fa(2.f, fd(1.f, fm(tx, tx)))) <= 1.f;
+    if (!(wy && wx)) return make_float2(0.f, 0.f);
+    const float ss = fa(qy, qx);
+    const float h_as = __fsqrt_rn(fmaxf(0.f, fs(1.f, ss)));
+    const float h_fr = fs(1.f, fd(ss, 2.f));
+    float sn, cs;
+    sincosf(fm(kz, fs(h_as, h_fr)), &sn, &cs);
+    return make_float2(cs, sn);
+  }
   if (a.kernel == CX_KERNEL_TRANSFER) {
     const float ph = fm(fm(fd(fm(-PI, lam), n), z), s);
     float sn, cs;

@@ -9,6 +9,7 @@ from .propagation import (
     compute_padding_exact,
     compute_padding_transfer,
     compute_padding_transform,
+    compute_sas_precompensation,
     compute_transfer_propagator,
     kernel_propagate,
     transfer_propagate,

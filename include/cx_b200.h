@@ -50,7 +50,8 @@ typedef enum {
 typedef enum {
   CX_KERNEL_TRANSFER = 0, /* Fresnel transfer function (propagation.py:466-496) */
   CX_KERNEL_ASM = 1,      /* angular spectrum (propagation.py:499-580) */
-  CX_KERNEL_EXPLICIT = 2  /* caller-supplied propagator array (propagation.py:355-393) */
+  CX_KERNEL_EXPLICIT = 2, /* caller-supplied propagator array (propagation.py:355-393) */
+  CX_KERNEL_SAS = 3       /* scalable-ASM precompensation Delta H of the padded grid (propagation.py:85-103) */
 } cx_kernel_kind;
 
 /* One output plane of a batched propagation. */

@@ -182,3 +182,31 @@ def test_psf_streamed_to_host_equals_device_result(nz, pinned):
     assert torch.equal(host, dev)
     with pytest.raises(ValueError):
         f.intensity_to(torch.empty((3, 3), dtype=torch.float32))
+
+
+def test_transform_propagate_sas_vs_oracle_and_kat():
+    """transform_propagate_sas (functional/propagation.py:85-165), both signs of
+    z, against the FP64 oracle; the analytic square aperture
+    (tests/test_propagate.py:60-76)."""
+    import chromatix_b200.functional as cf
+
+    u = rand_field((128, 96), seed=7)
+    fc, fo = cuda_field(u, 0.4, 0.532), oracle_field(u, 0.4, 0.532)
+    for z in (150.0, -150.0):
+        a = cf.transform_propagate_sas(fc, z, 1.33)
+        b = O.transform_propagate_sas(fo, z, 1.33)
+        assert a.u.shape == b.u.shape
+        assert rel(to_np(a.u), b.u) < TOL, z
+        np.testing.assert_allclose(a.dx, b.dx, rtol=1e-12)
+    H = cf.compute_sas_precompensation(fc, 150.0, 1.33)
+    Ho = O.compute_sas_precompensation(fo, 150.0, 1.33)
+    assert rel(to_np(H), Ho) < TOL
+    D, z, lam, n = 40.0, 100.0, 0.532, 1.33
+    for shape in ((256, 256), (1024, 256)):
+        dxi = D / np.array(shape)
+        field = cf.plane_wave(shape, dxi[np.newaxis], (lam, 1.0), pupil=lambda f: cf.square_pupil(f, D))
+        out = cf.transform_propagate_sas(field, z, n)
+        I_num = to_np(out.intensity).squeeze()
+        xi = to_np(out.grid).squeeze().astype(np.float64)
+        I_an = np.abs(O.fresnel_square_aperture(xi, z, D, lam, n)) ** 2
+        assert np.mean((I_an - I_num) ** 2) / np.mean(I_an**2) < 2e-2
