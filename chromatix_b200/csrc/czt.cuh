@@ -115,14 +115,14 @@ __global__ void __launch_bounds__(ColCfg<L>::THREADS, ColCfg<L>::MINB) k_czt_col
       return j < a.n ? cmul(s[pad_idx(j)], czt_in_chirp(a, j)) : make_float2(0.f, 0.f);
     };
     auto st1 = [&](int k, float2 val, int) { s[pad_idx(k)] = cmul(val, a.chat[k]); };
-    team_fft_ex<L, false, true, true>(s, tw, lane, team, load, st1);
-    team_sync<C::LPV>(team);
+    team_fft_ex<L, false, true, true, C::LPV, C::CTA>(s, tw, lane, team, load, st1);
+    team_barrier<C::LPV, C::CTA>(team);
     auto ld2 = [&](int k) -> float2 { return s[pad_idx(k)]; };
     auto st2 = [&](int k, float2 val, int) {
       const int r = k - (a.n - 1);
       if (r >= 0 && r < a.m) s[pad_idx(k)] = cmul(val, czt_out_chirp(a, r));
     };
-    team_fft_ex<L, true, false, true>(s, tw, lane, team, ld2, st2);
+    team_fft_ex<L, true, false, true, C::LPV, C::CTA>(s, tw, lane, team, ld2, st2);
     __syncthreads();
     float2* yo = a.y + o * a.out_ostride;
     for (int idx = threadIdx.x; idx < a.m * V; idx += blockDim.x) {

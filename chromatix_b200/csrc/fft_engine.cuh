@@ -94,6 +94,9 @@ struct Plan {
   static constexpr Radices P = make_radices(N);
   static constexpr int S = P.n;
   static constexpr int LPV = lanes_per_vector(N);
+  // one lane per butterfly of the largest-radix stage, without rounding to a
+  // warp-friendly team size: teams of this size need CTA-wide barriers
+  static constexpr int LPV_X = N / max_radix(N);
   static constexpr int LEN = vec_len(N);
   __host__ __device__ static constexpr int radix(int s) { return P.r[s]; }
   // outputs a lane holds after the last stage: the store functor's `slot`
@@ -308,6 +311,17 @@ __device__ __forceinline__ void team_sync(int team) {
   }
 }
 
+// Team barrier: team-local (CTA = false) or CTA-wide (CTA = true, for teams
+// that do not tile warps; every thread of the CTA must then reach it)
+template <int LPV, bool CTA>
+__device__ __forceinline__ void team_barrier(int team) {
+  if constexpr (CTA) {
+    __syncthreads();
+  } else {
+    team_sync<LPV>(team);
+  }
+}
+
 // ---------------------------------------------------------------------------
 // twiddle table: tw[m] = exp(-2 pi i m / N), computed in FP64
 // ---------------------------------------------------------------------------
@@ -398,7 +412,7 @@ __device__ __forceinline__ void apply_twiddles(const float2* tw, int m, float2* 
 // ---------------------------------------------------------------------------
 // the stage recursion
 // ---------------------------------------------------------------------------
-template <int N, int LPV, bool INV, int SI, int NS>
+template <int N, int LPV, bool INV, int SI, int NS, bool CTA = false>
 struct Stage {
   static constexpr int S = Plan<N>::S;
   static constexpr int R = Plan<N>::radix(SI);
@@ -438,7 +452,7 @@ struct Stage {
     }
     if constexpr (LAST) {
       // the store functor may write the team's buffer that this stage read
-      team_sync<LPV>(team);
+      team_barrier<LPV, CTA>(team);
 #pragma unroll
       for (int it = 0; it < IT; ++it) {
         const int j = lane + it * LPV;
@@ -448,7 +462,7 @@ struct Stage {
         }
       }
     } else {
-      team_sync<LPV>(team);
+      team_barrier<LPV, CTA>(team);
 #pragma unroll
       for (int it = 0; it < IT; ++it) {
         const int j = lane + it * LPV;
@@ -459,15 +473,15 @@ struct Stage {
           for (int r = 0; r < R; ++r) s[pad_idx(base + r * NS)] = v[it][r];
         }
       }
-      team_sync<LPV>(team);
-      Stage<N, LPV, INV, SI + 1, NS * R>::run(s, tw, lane, team, load, store);
+      team_barrier<LPV, CTA>(team);
+      Stage<N, LPV, INV, SI + 1, NS * R, CTA>::run(s, tw, lane, team, load, store);
     }
   }
 };
 
 // terminate recursion past the last stage (never instantiated at run time)
-template <int N, int LPV, bool INV, int NS>
-struct Stage<N, LPV, INV, 16, NS> {
+template <int N, int LPV, bool INV, int NS, bool CTA>
+struct Stage<N, LPV, INV, 16, NS, CTA> {
   template <class Load, class Store>
   __device__ static void run(float2*, const float2*, int, int, Load&, Store&) {}
 };
@@ -479,9 +493,9 @@ struct Stage<N, LPV, INV, 16, NS> {
 // lanes of the team must call this (inactive lanes still take part in the
 // team barriers).  Outputs are unnormalised (numpy convention for the
 // forward transform; the inverse omits the 1/N).
-template <int N, bool INV, class Load, class Store>
+template <int N, bool INV, int LPV = Plan<N>::LPV, bool CTA = false, class Load, class Store>
 __device__ __forceinline__ void team_fft(float2* s, const float2* tw, int lane, int team, Load& load, Store& store) {
-  Stage<N, Plan<N>::LPV, INV, 0, 1>::run(s, tw, lane, team, load, store);
+  Stage<N, LPV, INV, 0, 1, CTA>::run(s, tw, lane, team, load, store);
 }
 
 // Same transform with the load and/or store functor applied in a compact,
@@ -491,31 +505,31 @@ __device__ __forceinline__ void team_fft(float2* s, const float2* tw, int lane, 
 // functor's code once: for heavy functors (FP64 phase evaluation, sin/cos,
 // transmittances) this keeps the kernel within the instruction cache.
 // Staged store functors receive slot = 0.
-template <int N, bool INV, bool STAGE_LOAD, bool STAGE_STORE, class Load, class Store>
+template <int N, bool INV, bool STAGE_LOAD, bool STAGE_STORE, int LPV = Plan<N>::LPV, bool CTA = false, class Load,
+          class Store>
 __device__ __forceinline__ void team_fft_ex(float2* s, const float2* tw, int lane, int team, Load& load,
                                             Store& store) {
-  constexpr int LPV = Plan<N>::LPV;
   auto sld = [&](int n) -> float2 { return s[pad_idx(n)]; };
   auto sst = [&](int k, float2 v, int) { s[pad_idx(k)] = v; };
   if constexpr (STAGE_LOAD) {
-    team_sync<LPV>(team);  // the previous use of the buffer is complete
+    team_barrier<LPV, CTA>(team);  // the previous use of the buffer is complete
 #pragma unroll 4
     for (int n = lane; n < N; n += LPV) s[pad_idx(n)] = load(n);
-    team_sync<LPV>(team);
+    team_barrier<LPV, CTA>(team);
     if constexpr (STAGE_STORE) {
-      Stage<N, LPV, INV, 0, 1>::run(s, tw, lane, team, sld, sst);
+      Stage<N, LPV, INV, 0, 1, CTA>::run(s, tw, lane, team, sld, sst);
     } else {
-      Stage<N, LPV, INV, 0, 1>::run(s, tw, lane, team, sld, store);
+      Stage<N, LPV, INV, 0, 1, CTA>::run(s, tw, lane, team, sld, store);
     }
   } else {
     if constexpr (STAGE_STORE) {
-      Stage<N, LPV, INV, 0, 1>::run(s, tw, lane, team, load, sst);
+      Stage<N, LPV, INV, 0, 1, CTA>::run(s, tw, lane, team, load, sst);
     } else {
-      Stage<N, LPV, INV, 0, 1>::run(s, tw, lane, team, load, store);
+      Stage<N, LPV, INV, 0, 1, CTA>::run(s, tw, lane, team, load, store);
     }
   }
   if constexpr (STAGE_STORE) {
-    team_sync<LPV>(team);
+    team_barrier<LPV, CTA>(team);
 #pragma unroll 2
     for (int k = lane; k < N; k += LPV) store(k, s[pad_idx(k)], 0);
   }

@@ -134,17 +134,22 @@ __host__ __device__ constexpr int col_len(int N, int V) {
   return l;
 }
 
-// Column-tile kernels: V adjacent columns per CTA, one team per column.
-template <int N>
+// Column-tile kernels: V adjacent columns per CTA, one team per column.  All
+// teams of a CTA run the same transform in lockstep, so the teams can have
+// the exact lane count N / R_max (no idle lanes) and synchronise with CTA-wide
+// barriers (CTA = true) whenever that count does not tile warps.
+template <int N, bool EXACT = true>
 struct ColCfg {
-  static constexpr int LPV = Plan<N>::LPV;
+  static constexpr bool CTA = EXACT && Plan<N>::LPV_X != Plan<N>::LPV;
+  static constexpr int LPV = CTA ? Plan<N>::LPV_X : Plan<N>::LPV;
   // multi-warp teams: up to 4 columns, at most 1024 threads per CTA
   static constexpr int VT = 1024 / LPV >= 4 ? 4 : (1024 / LPV >= 2 ? 2 : 1);
-  static constexpr int V0 = LPV < 32 ? (256 / LPV > 16 ? 256 / LPV : 16) : VT;
+  static constexpr int V0 = LPV < 32 ? (pow2_floor(256 / LPV) > 16 ? pow2_floor(256 / LPV) : 16) : VT;
   static constexpr int TW = tw_len(N);
   static constexpr size_t smem_for(int v) { return sizeof(float2) * ((size_t)TW + (size_t)v * col_len(N, v)); }
   static constexpr int V = smem_for(V0) <= 200 * 1024 ? V0 : (smem_for(V0 / 2) <= 200 * 1024 ? V0 / 2 : V0 / 4);
   static_assert(V >= 1 && V * LPV <= 1024, "column tile does not fit one CTA");
+  static_assert(!CTA || (V * LPV) % 32 == 0, "exact-size teams must fill whole warps");
   static constexpr int LEN = col_len(N, V);
   static constexpr int THREADS = V * LPV;
   static constexpr int MINB = minb_for(THREADS);

@@ -128,9 +128,9 @@ __global__ void __launch_bounds__(RowCfg<NZ>::THREADS, RowCfg<NZ>::MINB) k_mbs_z
 // column tiles along an axis of length N with element stride E: vectors
 // (outer o, inner i), element j at buf + o * ostride + i + j * E; in place
 template <int N, bool INV>
-__global__ void __launch_bounds__(ColCfg<N>::THREADS, ColCfg<N>::MINB) k_mbs_cols(MbsArgs a, long n_outer,
+__global__ void __launch_bounds__(ColCfg<N, false>::THREADS, ColCfg<N, false>::MINB) k_mbs_cols(MbsArgs a, long n_outer,
                                                                                 int inner, long ostride, long E) {
-  using C = ColCfg<N>;
+  using C = ColCfg<N, false>;
   constexpr int V = C::V, LEN = C::LEN;
   extern __shared__ float2 sm[];
   float2* tw = sm;
@@ -149,7 +149,7 @@ __global__ void __launch_bounds__(ColCfg<N>::THREADS, ColCfg<N>::MINB) k_mbs_col
     __syncthreads();
     auto load = [&](int j) -> float2 { return s[pad_idx(j)]; };
     auto store = [&](int k, float2 v, int) { s[pad_idx(k)] = v; };
-    team_fft<N, INV>(s, tw, lane, team, load, store);
+    team_fft<N, INV, C::LPV, C::CTA>(s, tw, lane, team, load, store);
     __syncthreads();
     for (int idx = threadIdx.x; idx < N * V; idx += blockDim.x) {
       const int r = idx / V, c = idx % V, i = i0 + c;
@@ -162,11 +162,15 @@ __global__ void __launch_bounds__(ColCfg<N>::THREADS, ColCfg<N>::MINB) k_mbs_col
 // k-space projection / Green's-function division between FFT_x and IFFT_x
 template <int NX>
 struct MbsXCfg {
-  using C = ColCfg<NX>;
+  using C = ColCfg<NX, false>;
   static constexpr int LPV = C::LPV;
-  // about 128 lanes per component (at least 4 columns), at most 1024 threads
-  static constexpr int V0 = LPV < 32 ? (128 / LPV > 4 ? 128 / LPV : 4) : 4;
+  static constexpr bool CTA = C::CTA;
+  // about 128 lanes per component (at least 4 columns), at most 1024 threads;
+  // exact-size teams (CTA) fill whole warps
+  static constexpr int V1 = LPV < 32 ? (pow2_floor(128 / LPV) > 4 ? pow2_floor(128 / LPV) : 4) : 4;
+  static constexpr int V0 = (CTA && (3 * V1 * LPV) % 32 != 0 && 3 * 2 * V1 * LPV <= 1024) ? 2 * V1 : V1;
   static constexpr int V = (3 * V0 * LPV <= 1024) ? V0 : ((3 * 2 * LPV <= 1024) ? 2 : 1);
+  static_assert(!CTA || (3 * V * LPV) % 32 == 0, "exact-size teams must fill whole warps");
   static constexpr int LEN = col_len(NX, V);
   static constexpr int THREADS = 3 * V * LPV;
   static constexpr int MINB = minb_for(THREADS);
@@ -179,7 +183,7 @@ __global__ void __launch_bounds__(MbsXCfg<NX>::THREADS, MbsXCfg<NX>::MINB) k_mbs
   constexpr int V = Q::V, LEN = Q::LEN, LPV = Q::LPV;
   extern __shared__ float2 sm[];
   float2* tw = sm;
-  float2* tile = sm + ColCfg<NX>::TW;  // [comp][V][LEN]
+  float2* tile = sm + ColCfg<NX, false>::TW;  // [comp][V][LEN]
   load_twiddles<NX>(tw, a.twg, threadIdx.x, blockDim.x);
   const int team = threadIdx.x / LPV, lane = threadIdx.x % LPV;  // team = comp * V + column
   float2* s = tile + team * LEN;
@@ -194,7 +198,7 @@ __global__ void __launch_bounds__(MbsXCfg<NX>::THREADS, MbsXCfg<NX>::MINB) k_mbs
     __syncthreads();
     auto load = [&](int j) -> float2 { return s[pad_idx(j)]; };
     auto store = [&](int k, float2 v, int) { s[pad_idx(k)] = v; };
-    team_fft<NX, false>(s, tw, lane, team, load, store);
+    team_fft<NX, false, LPV, Q::CTA>(s, tw, lane, team, load, store);
     __syncthreads();
     // k-space operator, cooperatively over (kx, column)
     for (int idx = threadIdx.x; idx < NX * V; idx += blockDim.x) {
@@ -230,7 +234,7 @@ __global__ void __launch_bounds__(MbsXCfg<NX>::THREADS, MbsXCfg<NX>::MINB) k_mbs
       *p2 = cadd(cmul(csub(y2, l2), it), cmul(l2, il));
     }
     __syncthreads();
-    team_fft<NX, true>(s, tw, lane, team, load, store);
+    team_fft<NX, true, LPV, Q::CTA>(s, tw, lane, team, load, store);
     __syncthreads();
     for (int c = 0; c < 3; ++c) {
       float2* dst = a.buf + (size_t)c * a.vox;

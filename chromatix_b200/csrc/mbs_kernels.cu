@@ -35,7 +35,7 @@ static cx_status launch_z_any(int mode, const MbsArgs& a, cudaStream_t st) {
 
 template <int N, bool INV>
 static cx_status launch_cols(const MbsArgs& a, long n_outer, int inner, long ostride, long E, cudaStream_t st) {
-  using C = ColCfg<N>;
+  using C = ColCfg<N, false>;
   auto k = k_mbs_cols<N, INV>;
   CX_CUDA_TRY(set_smem(k, C::SMEM));
   const long items = (long)((inner + C::V - 1) / C::V) * n_outer;

@@ -45,7 +45,7 @@ __global__ void __launch_bounds__(ColCfg<NY>::THREADS, ColCfg<NY>::MINB) k_opt_c
       }
       s[pad_idx(k)] = v;
     };
-    team_fft_ex<NY, false, false, true>(s, tw, lane, team, load, store);
+    team_fft_ex<NY, false, false, true, C::LPV, C::CTA>(s, tw, lane, team, load, store);
     __syncthreads();
     const int b = q / a.W, w = q % a.W;
     for (int idx = threadIdx.x; idx < a.oy_n * V; idx += blockDim.x) {

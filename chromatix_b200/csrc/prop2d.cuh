@@ -247,11 +247,11 @@ __global__ void __launch_bounds__(ColCfg<NY>::THREADS, ColCfg<NY>::MINB) k_prop_
       return (n >= a.pad_y && n < a.pad_y + a.ny) ? s[pad_idx(n)] : make_float2(0.f, 0.f);
     };
     auto store1 = [&](int k, float2 v, int) { s[pad_idx(k)] = valid ? cmul(v, prop_kernel(k, kx, a, pl)) : v; };
-    team_fft_ex<NY, false, false, true>(s, tw, lane, team, load1, store1);
-    team_sync<C::LPV>(team);
+    team_fft_ex<NY, false, false, true, C::LPV, C::CTA>(s, tw, lane, team, load1, store1);
+    team_barrier<C::LPV, C::CTA>(team);
     auto load2 = [&](int n) -> float2 { return s[pad_idx(n)]; };
     auto store2 = [&](int k, float2 v, int) { s[pad_idx(k)] = cscale(v, scale); };
-    team_fft<NY, true>(s, tw, lane, team, load2, store2);
+    team_fft<NY, true, C::LPV, C::CTA>(s, tw, lane, team, load2, store2);
     __syncthreads();
     for (int idx = threadIdx.x; idx < a.out_ny * V; idx += blockDim.x) {
       const int r = idx / V, c = idx % V, x = x0 + c;

@@ -237,7 +237,7 @@ __global__ void __launch_bounds__(ColCfg<NY>::THREADS, ColCfg<NY>::MINB) k_psf_c
         const float e = dens * cabs2(v);
         acc[k] = (w == 0) ? e : acc[k] + e;
       };
-      team_fft<NY, false>(s, tw, lane, team, load, store);
+      team_fft<NY, false, C::LPV, C::CTA>(s, tw, lane, team, load, store);
     }
     __syncthreads();
     float* outz = a.out + (size_t)(a.z0 + zl) * a.ny * a.nx;
