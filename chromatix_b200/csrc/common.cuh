@@ -55,6 +55,16 @@ __device__ __forceinline__ float2 expi_precise(double ph) {
   return make_float2((float)c, (float)s);
 }
 
+// Asynchronous 16-byte global -> shared copies (cp.async): the copy proceeds
+// while the thread goes on computing; cp_async_wait_all() waits for this
+// thread's copies, a barrier then publishes them to the other threads.
+__device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
+  const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
+
 // Cast helpers that block FMA contraction, for the float32 reference-order
 // evaluation mode.
 __device__ __forceinline__ float fm(float a, float b) { return __fmul_rn(a, b); }

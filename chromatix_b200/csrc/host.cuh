@@ -123,6 +123,31 @@ struct RowCfg {
   static constexpr size_t SMEM = sizeof(float2) * ((size_t)TW + (size_t)TEAMS * Plan<N>::LEN);
 };
 
+// Row kernels whose teams all run one transform per loop iteration (no
+// per-team early exit): exact lane counts with CTA-wide barriers where the
+// count does not tile warps, about 192 threads in whole warps.
+template <int N>
+struct RowCfgX {
+  static constexpr bool CTA = Plan<N>::LPV_X != Plan<N>::LPV;
+  static constexpr int LPV = CTA ? Plan<N>::LPV_X : Plan<N>::LPV;
+  static constexpr int T1 = 192 / LPV > 0 ? 192 / LPV : 1;
+  static constexpr int teams_for() {
+    int t = T1;
+    if (CTA) {
+      while ((t * LPV) % 32 != 0) ++t;
+    } else if (LPV > 32 && t > 15) {
+      t = 15;
+    }
+    return t;
+  }
+  static constexpr int TEAMS = teams_for();
+  static constexpr int THREADS = TEAMS * LPV;
+  static_assert(THREADS <= 1024, "row CTA too large");
+  static constexpr int MINB = minb_for(THREADS);
+  static constexpr int TW = tw_len(N);
+  static constexpr size_t SMEM = sizeof(float2) * ((size_t)TW + (size_t)TEAMS * Plan<N>::LEN);
+};
+
 // Column stride (float2) of a V-column tile: a warp transposing a tile
 // touches V columns x (32/V) rows, so the stride must put those 32 elements
 // in distinct bank pairs: stride = 16/V (mod 16) for V <= 16, odd above.

@@ -62,15 +62,60 @@ __device__ __forceinline__ float2 ms_transmittance(const MsArgs& a, float dn, fl
   return make_float2(m * c, m * s);
 }
 
+// shared memory of the row pass: the base row configuration plus, per team,
+// a prefetch area for the slice's dn and abs rows (and, in the adjoint, the
+// recorded forward field row)
+template <int NX, int MODE>
+struct MsRowCfg {
+  using C = RowCfg<NX>;
+  static constexpr int NXA = (NX + 3) & ~3;  // one row of floats, rounded to 16 bytes
+  static constexpr int PF = (MODE == MS_FWD || MODE == MS_BWD) ? 2 * NXA + (MODE == MS_BWD ? 2 * NXA : 0) : 0;
+  // cp.async needs 16-byte aligned shared destinations: the prefetch area
+  // starts at the next 16-byte boundary after the transform buffers, and PF
+  // (a multiple of 4 floats) keeps every team's area aligned
+  static constexpr size_t PF_OFF = ((sizeof(float2) * ((size_t)C::TW + (size_t)C::TEAMS * Plan<NX>::LEN)) + 15) & ~(size_t)15;
+  static_assert(PF % 4 == 0, "prefetch rows must keep 16-byte alignment");
+  static constexpr size_t SMEM = PF_OFF + sizeof(float) * (size_t)C::TEAMS * PF;
+};
+
+// Start copying dn / abs row yd of the slice (and the recorded field row) into
+// the team's prefetch area; returns false when the rows are not 16-byte
+// aligned (the caller then reads them from global memory)
+template <int NX, int MODE>
+__device__ __forceinline__ bool ms_prefetch(const MsArgs& a, float* pf, int yd, int y, int lane, int lpv) {
+  const size_t off = (size_t)a.slice * a.ny * a.nx + (size_t)yd * a.nx;
+  const float* dn = a.dn + off;
+  const float* ab = a.ab + off;
+  bool ok = (a.nx % 4 == 0) && ((reinterpret_cast<size_t>(dn) & 15) == 0) && ((reinterpret_cast<size_t>(ab) & 15) == 0);
+  const float2* u = nullptr;
+  if constexpr (MODE == MS_BWD) {
+    u = a.rec_u + (size_t)y * a.px;
+    ok = ok && (a.px % 2 == 0) && ((reinterpret_cast<size_t>(u) & 15) == 0);
+  }
+  if (!ok) return false;
+  constexpr int NXA = MsRowCfg<NX, MODE>::NXA;
+  for (int i = lane; i < a.nx / 4; i += lpv) {
+    cp_async16(pf + 4 * i, dn + 4 * i);
+    cp_async16(pf + NXA + 4 * i, ab + 4 * i);
+  }
+  if constexpr (MODE == MS_BWD) {
+    for (int i = lane; i < a.px / 2; i += lpv) cp_async16(pf + 2 * NXA + 4 * i, u + 2 * i);
+  }
+  cp_async_commit();
+  return true;
+}
+
 template <int NX, int MODE>
 __global__ void __launch_bounds__(RowCfg<NX>::THREADS, RowCfg<NX>::MINB) k_ms_rows(MsArgs a) {
   using C = RowCfg<NX>;
-  extern __shared__ float2 sm[];
+  extern __shared__ __align__(16) float2 sm[];
   float2* tw = sm;
   load_twiddles<NX>(tw, a.twg, threadIdx.x, blockDim.x);
   __syncthreads();
   const int team = threadIdx.x / C::LPV, lane = threadIdx.x % C::LPV;
   float2* s = sm + C::TW + team * Plan<NX>::LEN;
+  float* pf = reinterpret_cast<float*>(reinterpret_cast<char*>(sm) + MsRowCfg<NX, MODE>::PF_OFF) +
+              (size_t)team * MsRowCfg<NX, MODE>::PF;
   // MS_FINAL only produces the cropped rows
   const int r0 = MODE == MS_FINAL ? a.pad_y : 0;
   const int nrows = MODE == MS_FINAL ? a.ny : a.py;
@@ -111,35 +156,48 @@ __global__ void __launch_bounds__(RowCfg<NX>::THREADS, RowCfg<NX>::MINB) k_ms_ro
       continue;
     }
     if constexpr (MODE == MS_FWD || MODE == MS_BWD) {
+    // the slice's rows stream into shared memory while the inverse transform runs
+    const bool pre = yin && ms_prefetch<NX, MODE>(a, pf, yd, y, lane, C::LPV);
+    auto sst = [&](int k, float2 v, int) { s[pad_idx(k)] = v; };
+    team_fft<NX, true>(s, tw, lane, team, load_row, sst);
+    if (pre) cp_async_wait_all();
+    team_sync<C::LPV>(team);
     if constexpr (MODE == MS_FWD) {
       float2* rrow = a.record ? a.rec + (size_t)y * a.px : nullptr;
-      auto store1 = [&](int k, float2 v, int) {
+#pragma unroll 2
+      for (int k = lane; k < NX; k += C::LPV) {
+        float2 v = s[pad_idx(k)];
         const int xd = k - a.pad_x;
         if (yin && xd >= 0 && xd < a.nx) {
           const size_t idx = plane_d + (size_t)yd * a.nx + xd;
-          v = cmul(v, ms_transmittance(a, a.dn[idx], a.ab[idx]));
+          const float dnv = pre ? pf[xd] : a.dn[idx];
+          const float abv = pre ? pf[MsRowCfg<NX, MODE>::NXA + xd] : a.ab[idx];
+          v = cmul(v, ms_transmittance(a, dnv, abv));
         }
         if (a.record) rrow[k] = v;
         s[pad_idx(k)] = v;
-      };
-      team_fft_ex<NX, true, false, true>(s, tw, lane, team, load_row, store1);
+      }
     } else {  // MS_BWD
       const float2* urow = a.rec_u + (size_t)y * a.px;
-      auto store1 = [&](int k, float2 g, int) {
+      const float2* purow = reinterpret_cast<const float2*>(pf + 2 * MsRowCfg<NX, MODE>::NXA);
+#pragma unroll 2
+      for (int k = lane; k < NX; k += C::LPV) {
+        float2 g = s[pad_idx(k)];
         const int xd = k - a.pad_x;
         if (yin && xd >= 0 && xd < a.nx) {
           const size_t idx = plane_d + (size_t)yd * a.nx + xd;
-          const float2 u = urow[k];
+          const float2 u = pre ? purow[k] : urow[k];
           // w = g * conj(u)
           const float wr = g.x * u.x + g.y * u.y, wi = g.y * u.x - g.x * u.y;
           const size_t gi = (size_t)yd * a.nx + xd;
           a.gdn[gi] = (float)(kdz * (double)wi);
           a.gab[gi] = (float)(-kdz * (double)wr);
-          g = cmul(g, cconj(ms_transmittance(a, a.dn[idx], a.ab[idx])));
+          const float dnv = pre ? pf[xd] : a.dn[idx];
+          const float abv = pre ? pf[MsRowCfg<NX, MODE>::NXA + xd] : a.ab[idx];
+          g = cmul(g, cconj(ms_transmittance(a, dnv, abv)));
         }
         s[pad_idx(k)] = g;
-      };
-      team_fft_ex<NX, true, false, true>(s, tw, lane, team, load_row, store1);
+      }
     }
     team_sync<C::LPV>(team);
     auto load2 = [&](int n) -> float2 { return s[pad_idx(n)]; };

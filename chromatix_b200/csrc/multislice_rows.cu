@@ -6,11 +6,12 @@ namespace cx {
 template <int NX, int MODE>
 static cx_status launch_ms_rows_mode(const MsArgs& a, cudaStream_t st) {
   using C = RowCfg<NX>;
+  constexpr size_t SMEM = MsRowCfg<NX, MODE>::SMEM;
   auto k = k_ms_rows<NX, MODE>;
-  CX_CUDA_TRY(set_smem(k, C::SMEM));
+  CX_CUDA_TRY(set_smem(k, SMEM));
   const long rows = a.mode == MS_FINAL ? a.ny : a.py;
   const long items = (rows + C::TEAMS - 1) / C::TEAMS;
-  k<<<persistent_grid(k, C::THREADS, C::SMEM, items), C::THREADS, C::SMEM, st>>>(a);
+  k<<<persistent_grid(k, C::THREADS, SMEM, items), C::THREADS, SMEM, st>>>(a);
   CX_LAUNCH_CHECK();
   return CX_OK;
 }

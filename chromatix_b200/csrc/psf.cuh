@@ -112,7 +112,53 @@ __device__ __forceinline__ float2 psf_const(const PsfArgs& a, int w, const unsig
 // ---------------------------------------------------------------------------
 // pass A: analytic source -> row FFT, for the rows inside the pupil only
 // ---------------------------------------------------------------------------
-template <int NX, bool TAB>
+// accurate mode: the loader is M * CX * one FP64 row factor (see PsfArgs).
+// Every team runs one transform per iteration (rows past the end or outside
+// the pupil transform zeros and store nothing), so teams can have the exact
+// lane count and share CTA-wide barriers.
+template <int NX>
+__global__ void __launch_bounds__(RowCfgX<NX>::THREADS, RowCfgX<NX>::MINB) k_psf_rows_tab(PsfArgs a) {
+  using C = RowCfgX<NX>;
+  extern __shared__ float2 sm[];
+  float2* tw = sm;
+  load_twiddles<NX>(tw, a.twg, threadIdx.x, blockDim.x);
+  __syncthreads();
+  const int team = threadIdx.x / C::LPV, lane = threadIdx.x % C::LPV;
+  float2* s = sm + C::TW + team * Plan<NX>::LEN;
+  const long total = (long)a.zc * a.rowsum;
+  const double PI = 3.141592653589793238462643383279502884;
+  for (long base = (long)blockIdx.x * C::TEAMS; base < total; base += (long)gridDim.x * C::TEAMS) {
+    const long item0 = base + team;
+    const long item = item0 < total ? item0 : total - 1;
+    const int zl = (int)(item / a.rowsum);
+    const int rem = (int)(item % a.rowsum);
+    int w = 0;
+    while (w + 1 < a.W && rem >= a.prefix[w + 1]) ++w;
+    const PsfWv& p = a.wv[w];
+    const int y = a.ylo[w] + (rem - a.prefix[w]);
+    const bool live = item0 < total && y >= support_lo(a, w) && y < support_hi(a, w);
+    const double z = a.z[a.z0 + zl];
+    const double gyo = p.dy * ((double)y - (double)a.ny * 0.5) - a.offy;
+    const double qz = -PI * (z / a.f_obj) / p.L2;
+    const float2* mrow = a.M + a.mprefix[w] + (size_t)(y - a.ylo[w]) * a.ncols[w];
+    const float2* cxz = a.CX + (size_t)(a.z0 + zl) * a.csum + a.cprefix[w];
+    const int xlo = a.xlo[w], nc = live ? a.ncols[w] : 0;
+    const float2 cy = expi_precise(qz * gyo * gyo);
+    float2* dst = a.T + ((size_t)zl * a.rowsum + rem) * a.nx;
+    auto load = [&](int n) -> float2 {
+      const int c = add_mod(n, NX / 2, NX) - xlo;  // ifftshift along x, then the box column
+      if ((unsigned)c >= (unsigned)nc) return make_float2(0.f, 0.f);
+      return cmul(cmul(mrow[c], cxz[c]), cy);
+    };
+    auto store = [&](int k, float2 v, int) {
+      if (live) dst[k] = v;
+    };
+    team_fft<NX, false, C::LPV, C::CTA>(s, tw, lane, team, load, store);
+  }
+}
+
+// reference-order float32 mode: the source evaluated per pixel in the loader
+template <int NX>
 __global__ void __launch_bounds__(RowCfg<NX>::THREADS, RowCfg<NX>::MINB) k_psf_rows(PsfArgs a) {
   using C = RowCfg<NX>;
   extern __shared__ float2 sm[];
@@ -145,19 +191,6 @@ __global__ void __launch_bounds__(RowCfg<NX>::THREADS, RowCfg<NX>::MINB) k_psf_r
     const double gyo = gy - a.offy;
     float2* dst = a.T + ((size_t)zl * a.rowsum + rem) * a.nx;
     auto store = [&](int k, float2 v, int) { dst[k] = v; };
-    if constexpr (TAB) {
-      const float2* mrow = a.M + a.mprefix[w] + (size_t)(y - a.ylo[w]) * a.ncols[w];
-      const float2* cxz = a.CX + (size_t)(a.z0 + zl) * a.csum + a.cprefix[w];
-      const int xlo = a.xlo[w], nc = a.ncols[w];
-      const float2 cy = expi_precise(qz * gyo * gyo);
-      auto load = [&](int n) -> float2 {
-        const int c = add_mod(n, NX / 2, NX) - xlo;  // ifftshift along x, then the box column
-        if ((unsigned)c >= (unsigned)nc) return make_float2(0.f, 0.f);
-        return cmul(cmul(mrow[c], cxz[c]), cy);
-      };
-      team_fft<NX, false>(s, tw, lane, team, load, store);
-      continue;
-    }
     auto load = [&](int n) -> float2 {
       const int x = add_mod(n, NX / 2, NX);  // ifftshift along x
       if (!in_pupil(a, p, y, x)) return make_float2(0.f, 0.f);

@@ -5,12 +5,20 @@ namespace cx {
 
 template <int NX>
 static cx_status launch_psf_rows(const PsfArgs& a, cudaStream_t st) {
-  using C = RowCfg<NX>;
-  auto k = a.precision == CX_PREC_REF32 ? k_psf_rows<NX, false> : k_psf_rows<NX, true>;
-  CX_CUDA_TRY(set_smem(k, C::SMEM));
-  const long items = ((long)a.zc * a.rowsum + C::TEAMS - 1) / C::TEAMS;
-  const int grid = persistent_grid(k, C::THREADS, C::SMEM, items);
-  k<<<grid, C::THREADS, C::SMEM, st>>>(a);
+  const long rows = (long)a.zc * a.rowsum;
+  if (a.precision != CX_PREC_REF32) {
+    using C = RowCfgX<NX>;
+    auto k = k_psf_rows_tab<NX>;
+    CX_CUDA_TRY(set_smem(k, C::SMEM));
+    const int grid = persistent_grid(k, C::THREADS, C::SMEM, (rows + C::TEAMS - 1) / C::TEAMS);
+    k<<<grid, C::THREADS, C::SMEM, st>>>(a);
+  } else {
+    using C = RowCfg<NX>;
+    auto k = k_psf_rows<NX>;
+    CX_CUDA_TRY(set_smem(k, C::SMEM));
+    const int grid = persistent_grid(k, C::THREADS, C::SMEM, (rows + C::TEAMS - 1) / C::TEAMS);
+    k<<<grid, C::THREADS, C::SMEM, st>>>(a);
+  }
   CX_LAUNCH_CHECK();
   return CX_OK;
 }
