@@ -405,6 +405,42 @@ def psf_published_arm(args):
     print(json.dumps(line), flush=True)
 
 
+def rescaled_published_arm(args):
+    """The reference's published rescaled-propagation timings
+    (docs/examples/rescaled_propagation.ipynb, cells 4, 8, 19): 1024^2 plane
+    wave through a square aperture of width D/10 (dx = 2 lambda, lambda 0.532,
+    D = 1024 dx), z = 10 D, n = 1, pad 512 (2048^2 grid), band-limited ASM,
+    output_dx = dx / 4, shift (0, w/2), mode "same"; published 63.1 ms (Yu et
+    al. branch) and 75.9 ms (chirp-Z branch) on an unstated GPU."""
+    import torch
+
+    import chromatix_b200.functional as cf
+
+    dev = torch.device("cuda", 0)
+    lam = 0.532
+    dxi = 2 * lam
+    D = dxi * 1024
+    w = D / 10
+    z = 10 * D
+    field = cf.plane_wave((1024, 1024), dxi, lam, pupil=lambda f: cf.square_pupil(f, w), device=dev)
+    res = {}
+    for name, use_czt, published in (("yu", False, 63.1), ("czt", True, 75.9)):
+        def step():
+            return cf.asm_propagate(field, z, 1, (512, 512), mode="same", bandlimit=True,
+                                    output_dx=np.asarray(field.dx) / 4, shift_yx=(0.0, w / 2), use_czt=use_czt)
+
+        ms = _device_timer(torch, dev, args.steps, args.warmup)(step)
+        res[name] = {"ms": round(ms, 4), "published_ms": published, "speedup": round(published / ms, 1)}
+    line = _base_line("ms, rescaled ASM 1024^2 (pad 512) -> dx/4 (the reference's published example)",
+                      res["czt"]["ms"], "ms", args.steps, args.warmup, res["czt"]["ms"], "c64",
+                      {"workload": "asm_propagate 1024^2, pad 512, bandlimit, output_dx = dx/4, shift (0, w/2), "
+                                   "mode same; chirp-Z and Yu et al. branches", "l2": "flushed between timed steps"},
+                      higher_is_better=False, vs_baseline=round(75.9 / res["czt"]["ms"], 1),
+                      baseline={"ms": {"czt": 75.9, "yu": 63.1}, "hardware": "unstated GPU (notebook output)"},
+                      cases=res)
+    print(json.dumps(line), flush=True)
+
+
 def asm_arm(args):
     """Single-field angular-spectrum / Fresnel-transfer propagation: 512^2
     complex64 A exp(i phi), A ~ U[0.5, 1], phi ~ U[0, 2 pi), dx 0.3 um,
@@ -742,7 +778,7 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--accuracy", action="store_true", help="also report the error vs the FP64 oracle")
     ap.add_argument("--workload", default="psf",
-                    choices=["psf", "serve", "psf_published", "asm", "multislice", "mbs"],
+                    choices=["psf", "serve", "psf_published", "rescaled_published", "asm", "multislice", "mbs"],
                     help="psf: the batched 4f PSF stack (headline); the others print one line each for the "
                          "other configurations")
     ap.add_argument("--mbs-maxiter", type=int, default=4000)
@@ -759,6 +795,8 @@ def main():
         psf_published_arm(args)
     elif args.workload == "asm":
         asm_arm(args)
+    elif args.workload == "rescaled_published":
+        rescaled_published_arm(args)
     elif args.workload == "multislice":
         multislice_arm(args)
     elif args.workload == "mbs":

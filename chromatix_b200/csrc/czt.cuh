@@ -31,10 +31,23 @@ struct CztArgs {
   const float2* x;
   float2* y;
   const float2* twg;
+  // kind 1: chirp convolution (the Yu et al. rescaling of kernel_propagate,
+  // functional/propagation.py:445-458) instead of a chirp-Z transform:
+  //   y[k] = mag_out exp(i pi c_out (dx_out (k - k0_out) + org_out)^2)
+  //          * sum_j x[j] mag_in exp(i pi c_in (j - j0_in)^2) f[k + s - j],
+  // with the finite chirp filter f in chat (see the filter kernel)
+  int kind = 0;
+  double c_in = 0.0, j0_in = 0.0, mag_in = 1.0;
+  double c_out = 0.0, dx_out = 0.0, k0_out = 0.0, org_out = 0.0, mag_out = 1.0;
 };
 
-// a^(-j) w^(j^2/2)
+// a^(-j) w^(j^2/2)  (kind 1: the input factor of the chirp convolution)
 __device__ __forceinline__ float2 czt_in_chirp(const CztArgs& a, int j) {
+  if (a.kind == 1) {
+    const double d = (double)j - a.j0_in;
+    const float2 e = expi_reduced(3.141592653589793238462643383279502884 * a.c_in * d * d);
+    return make_float2((float)a.mag_in * e.x, (float)a.mag_in * e.y);
+  }
   const double jj = (double)j;
   const double lm = -a.la * jj + a.lw * 0.5 * jj * jj;
   const double ph = -a.ta * jj + a.tw * 0.5 * jj * jj;
@@ -43,8 +56,13 @@ __device__ __forceinline__ float2 czt_in_chirp(const CztArgs& a, int j) {
   return make_float2(m * e.x, m * e.y);
 }
 
-// w^(k^2/2) [w^(-N k) a^N] * scale
+// w^(k^2/2) [w^(-N k) a^N] * scale  (kind 1: the output factor of the chirp convolution)
 __device__ __forceinline__ float2 czt_out_chirp(const CztArgs& a, int k) {
+  if (a.kind == 1) {
+    const double g = a.dx_out * ((double)k - a.k0_out) + a.org_out;
+    const float2 e = expi_reduced(3.141592653589793238462643383279502884 * a.c_out * g * g);
+    return make_float2((float)a.mag_out * e.x, (float)a.mag_out * e.y);
+  }
   const double kk = (double)k;
   double lm = a.lw * 0.5 * kk * kk;
   double ph = a.tw * 0.5 * kk * kk;

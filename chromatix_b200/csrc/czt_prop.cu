@@ -16,9 +16,25 @@
 #include <cmath>
 #include <complex>
 
-#include "host.cuh"
+#include "czt.cuh"
 
 namespace cx {
+
+// finite chirp filter of the Yu et al. convolution along an axis of length n,
+// arranged for the chirp-Z pass: c[i] = exp(-i pi cf (i - ic)^2) / L on
+// i in [i0, i1), 0 elsewhere (FP64 phases; evaluated once per call)
+__global__ void k_yu_filter(float2* __restrict__ c, int L, double cf, double ic, int i0, int i1) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < L; i += gridDim.x * blockDim.x) {
+    float2 v = make_float2(0.f, 0.f);
+    if (i >= i0 && i < i1) {
+      const double d = (double)i - ic;
+      double sd, cd;
+      sincos(-3.141592653589793238462643383279502884 * cf * d * d, &sd, &cd);
+      v = make_float2((float)(cd / L), (float)(sd / L));
+    }
+    c[i] = v;
+  }
+}
 
 __global__ void k_czt_prop_tables(cx_plane* hp, cx_plane h, cx_fft_plane* fp, cx_fft_plane f) {
   if (threadIdx.x == 0) {
@@ -49,12 +65,23 @@ static cx_status czt_prop_layout(const cx_czt_prop_desc* d, CztPropLayout* L) {
     set_error("invalid rescaled-propagation descriptor (output sides >= 2, transfer or ASM kernel)");
     return CX_ERR_INVALID;
   }
-  if (d->bandlimit) {
-    set_error("cx_czt_propagate: band-limited propagators are not supported in the one-call path");
-    return CX_ERR_UNSUPPORTED;
+  if (d->bandlimit && d->kernel != CX_KERNEL_ASM) {
+    set_error("cx_czt_propagate: the band limit applies to the ASM kernel only");
+    return CX_ERR_INVALID;
+  }
+  if (d->method != 0 && d->method != 1) {
+    set_error("cx_czt_propagate: method must be 0 (chirp-Z) or 1 (Yu et al. convolution)");
+    return CX_ERR_INVALID;
   }
   L->py = d->ny + 2 * d->pad_y;
   L->px = d->nx + 2 * d->pad_x;
+  if (d->method == 1 && (d->my != L->py || d->mx != L->px)) {
+    // the convolution keeps the padded grid (its output chirp and the "same"
+    // convolution share one shape, propagation.py:452-458)
+    set_error("the Yu et al. rescaling needs output_shape == padded shape (%dx%d), got %dx%d", L->py, L->px,
+              d->my, d->mx);
+    return CX_ERR_INVALID;
+  }
   if (!size_supported(L->py) || !size_supported(L->px)) {
     set_error("padded grid %dx%d: FFT length not supported", L->py, L->px);
     return CX_ERR_UNSUPPORTED;
@@ -72,7 +99,8 @@ static cx_status czt_prop_layout(const cx_czt_prop_desc* d, CztPropLayout* L) {
   L->off_y = L->off_h + al256(plane);
   L->off_t = L->off_y + al256(plane);
   L->off_c = L->off_t + al256(t);
-  L->total = L->off_c + al256(2 * sizeof(float2) * (size_t)Lm);
+  // chirp-Z: one filter + spectrum (cx_czt's workspace); Yu: filter + spectrum per axis
+  L->total = L->off_c + al256((d->method == 1 ? 4 : 2) * sizeof(float2) * (size_t)Lm);
   return CX_OK;
 }
 
@@ -112,13 +140,25 @@ extern "C" cx_status cx_czt_propagate(const cx_czt_prop_desc* d, const void* u_i
   void* cws = ws + L.off_c;
   const size_t cws_bytes = L.total - L.off_c;
 
-  // propagator of the padded grid with the field's spacing; the output shift
-  // lives in the CZT grid, not in H (propagation.py:420-443)
+  // propagator of the padded grid with the field's spacing; with chirp-Z
+  // transforms the output shift lives in their grid, not in H (propagation.py:420-443)
   cx_plane h{};
   h.z = d->z;
   h.wavelength = d->wavelength;
   h.dy = d->dy_in;
   h.dx = d->dx_in;
+  if (d->bandlimit) {
+    h.bl_y0 = d->bl_y0;
+    h.bl_x0 = d->bl_x0;
+    h.bl_hy = d->bl_hy;
+    h.bl_hx = d->bl_hx;
+  }
+  if (d->method == 1 && d->kernel == CX_KERNEL_ASM) {
+    // without the chirp-Z grid the ASM shift term stays in the propagator
+    // (asm_propagate passes shift_yx unless use_czt, propagation.py:331-339)
+    h.shift_y = d->shift_y;
+    h.shift_x = d->shift_x;
+  }
   cx_fft_plane f{};
   f.pre_re = 1.0;
   f.post_re = 1.0;
@@ -135,6 +175,7 @@ extern "C" cx_status cx_czt_propagate(const cx_czt_prop_desc* d, const void* u_i
   hd.kernel = d->kernel;
   hd.precision = d->precision;
   hd.remove_evanescent = d->kernel == CX_KERNEL_ASM ? d->remove_evanescent : 0;
+  hd.bandlimit = d->bandlimit;
   hd.n_medium = d->n_medium;
   hd.ky0 = d->ky0;
   hd.kx0 = d->kx0;
@@ -170,6 +211,65 @@ extern "C" cx_status cx_czt_propagate(const cx_czt_prop_desc* d, const void* u_i
 
   const size_t in_plane = (size_t)d->ny * d->nx;
   const size_t out_plane = (size_t)d->my * d->mx;
+  // Yu et al.: per axis n = padded length, alpha = dx_out / df_in with df_in =
+  // 1 / (n dx_in); input factor (1/alpha) exp(i pi alpha df^2 (j - n//2)^2),
+  // filter exp(-i pi alpha df^2 (m - n//2)^2) on m in [0, n) placed for the
+  // "same" convolution (offset (n-1)//2), output factor
+  // dx_out exp(i pi / alpha (dx_out (k - n/2) + origin)^2)
+  CztArgs yu[2];
+  if (d->method == 1) {
+    const float2* twg = nullptr;
+    if ((s = ensure_twiddles(&twg)) != CX_OK) return s;
+    const int Ls[2] = {L.Ly, L.Lx};
+    for (int k = 0; k < 2; ++k) {
+      const int n = P[k];
+      const double df = 1.0 / ((double)n * dxi[k]);
+      const double al = dxo[k] / df;
+      const double cin = al * df * df;
+      const int sc = (n - 1) / 2;
+      float2* cfilt = reinterpret_cast<float2*>(static_cast<char*>(cws)) + (size_t)k * 2 * (L.Ly > L.Lx ? L.Ly : L.Lx);
+      float2* chat = cfilt + (L.Ly > L.Lx ? L.Ly : L.Lx);
+      k_yu_filter<<<(Ls[k] + 255) / 256, 256, 0, st>>>(cfilt, Ls[k], cin, (double)(n - 1 - sc + n / 2), n - 1 - sc,
+                                                       2 * n - 1 - sc);
+      CX_LAUNCH_CHECK();
+      if ((s = cx_fft1d(cfilt, chat, Ls[k], 1, 0, stream)) != CX_OK) return s;
+      CztArgs& a = yu[k];
+      a.n = n;
+      a.m = n;
+      a.L = Ls[k];
+      a.ta = a.tw = a.la = a.lw = 0.0;
+      a.modN = -1;
+      a.scale = 1.0;
+      a.chat = chat;
+      a.twg = twg;
+      a.kind = 1;
+      a.c_in = cin;
+      a.j0_in = (double)(n / 2);
+      a.mag_in = 1.0 / al;
+      a.c_out = 1.0 / al;
+      a.dx_out = dxo[k];
+      a.k0_out = n / 2.0;
+      a.org_out = sh[k];
+      a.mag_out = dxo[k];
+    }
+    // along y: column tiles over the px columns; along x: one team per row
+    yu[0].n_vec = L.px;
+    yu[0].inner = L.px;
+    yu[0].in_ostride = (long)L.py * L.px;
+    yu[0].in_istride = 1;
+    yu[0].in_estride = L.px;
+    yu[0].out_ostride = (long)L.py * L.px;
+    yu[0].out_istride = 1;
+    yu[0].out_estride = L.px;
+    yu[1].n_vec = L.py;
+    yu[1].inner = 1;
+    yu[1].in_ostride = L.px;
+    yu[1].in_istride = 1;
+    yu[1].in_estride = 1;
+    yu[1].out_ostride = L.px;
+    yu[1].out_istride = 1;
+    yu[1].out_estride = 1;
+  }
   for (int b = 0; b < d->n_fields; ++b) {
     const float2* ub = static_cast<const float2*>(u_in) + (size_t)b * in_plane;
     float2* ob = static_cast<float2*>(u_out) + (size_t)b * out_plane;
@@ -177,6 +277,15 @@ extern "C" cx_status cx_czt_propagate(const cx_czt_prop_desc* d, const void* u_i
     // workspace in T
     if ((s = cx_optical_fft_h(&od, fp, H, ub, Y, T, sizeof(float2) * (size_t)L.py * L.px, stream)) != CX_OK)
       return s;
+    if (d->method == 1) {
+      yu[0].x = Y;
+      yu[0].y = T;
+      if ((s = czt_dispatch_cols(yu[0].L, yu[0], st)) != CX_OK) return s;
+      yu[1].x = T;
+      yu[1].y = ob;
+      if ((s = czt_dispatch_rows(yu[1].L, yu[1], st)) != CX_OK) return s;
+      continue;
+    }
     // along y: (py, px) -> (my, px), column tiles
     cx_czt_desc cy{};
     cy.n = L.py;

@@ -311,7 +311,12 @@ cx_status cx_czt_noalloc(const cx_czt_desc* d, const void* x, void* y, cx_stream
  * along y and along x onto the (my, mx) output grid of spacing (dy_out,
  * dx_out) shifted by (shift_y, shift_x).  n_fields single-wavelength fields
  * (ny, nx) complex64 sharing every parameter; u_out (n_fields, my, mx).
- * Band-limited propagators are not supported here (CX_ERR_UNSUPPORTED). */
+ * bandlimit = 1 applies the Matsushima band-limit rectangle bl_* to the ASM
+ * propagator (the caller computes it, e.g. as _bandlimit_rect does).
+ * method 1 replaces the two CZTs by the Yu et al. rescaled convolution:
+ * fftconvolve(B, f, "same") of the chirped spectrum with a chirp filter,
+ * separable per axis, times the output chirp; shift_y/x is the output
+ * grid origin there. */
 typedef struct {
   int32_t ny, nx;          /* input shape */
   int32_t pad_y, pad_x;    /* zero padding on each side */
@@ -320,11 +325,13 @@ typedef struct {
   int32_t kernel;          /* CX_KERNEL_TRANSFER or CX_KERNEL_ASM */
   int32_t precision;       /* cx_precision */
   int32_t remove_evanescent, bandlimit;
-  int32_t reserved;
+  int32_t method;          /* 0: chirp-Z transforms (use_czt=True); 1: the Yu et al. chirp convolution
+                              (use_czt=False, propagation.py:445-458; output shape = padded shape) */
   double n_medium, z, wavelength;
   double dy_in, dx_in, dy_out, dx_out;
   double shift_y, shift_x;
   double ky0, kx0;
+  double bl_y0, bl_x0, bl_hy, bl_hx; /* band-limit rectangle (bandlimit = 1, ASM only; as in cx_plane) */
 } cx_czt_prop_desc;
 
 cx_status cx_czt_propagate_workspace_size(const cx_czt_prop_desc* d, size_t* bytes);

@@ -93,3 +93,46 @@ def test_rescaled_with_shift_and_same_mode():
     ref = O.asm_propagate(oracle_field(u, 0.3, 0.532), 25.0, 1.33, 16, **kw)
     assert out.u.shape == ref.u.shape
     assert rel(to_np(out.u), ref.u) < 1e-5
+
+
+@pytest.mark.parametrize("fn", ["asm_propagate", "transfer_propagate"])
+@pytest.mark.parametrize("zoom,pad,shift,mode", [(2.0, 64, (0.0, 0.0), "full"), (0.5, 32, (1.5, -2.0), "full"),
+                                                 (1.3, 0, (0.0, 0.0), "same"), (4.0, 48, (0.0, 0.0), "same")])
+def test_rescaled_yu_branch(fn, zoom, pad, shift, mode):
+    """kernel_propagate's use_czt=False branch (functional/propagation.py:445-458): the
+    chirp convolution against the FP64 oracle (scipy fftconvolve)."""
+    import chromatix_b200.functional as cf
+
+    u = rand_field((128, 96), seed=4)
+    dx = 0.3
+    kw = dict(output_dx=np.array([dx / zoom, dx / zoom]), use_czt=False, shift_yx=shift, mode=mode)
+    out = getattr(cf, fn)(cuda_field(u, dx, 0.532), 40.0, 1.33, pad, **kw)
+    ref = getattr(O, fn)(oracle_field(u, dx, 0.532), 40.0, 1.33, pad, **kw)
+    assert out.u.shape == ref.u.shape
+    assert rel(to_np(out.u), ref.u) < 1e-5
+    np.testing.assert_allclose(out.dx, ref.dx)
+
+
+def test_rescaled_yu_branch_rejects_other_output_shapes():
+    import chromatix_b200.functional as cf
+    from chromatix_b200._native import CxError
+
+    u = rand_field((64, 64), seed=5)
+    with pytest.raises(CxError):
+        cf.asm_propagate(cuda_field(u, 0.3, 0.532), 40.0, 1.33, 16, output_dx=np.array([0.15, 0.15]),
+                         output_shape=(64, 64), use_czt=False)
+
+
+@pytest.mark.parametrize("use_czt", [True, False])
+def test_rescaled_band_limited(use_czt):
+    """The band-limited (Matsushima) ASM propagator in both rescaled branches, as in
+    docs/examples/rescaled_propagation.ipynb."""
+    import chromatix_b200.functional as cf
+
+    u = rand_field((128, 128), seed=6)
+    kw = dict(output_dx=np.array([0.3 / 1.5] * 2), shift_yx=(3.0, -1.0), bandlimit=True, use_czt=use_czt,
+              mode="same")
+    out = cf.asm_propagate(cuda_field(u, 0.3, 0.532), 300.0, 1.0, 64, **kw)
+    ref = O.asm_propagate(oracle_field(u, 0.3, 0.532), 300.0, 1.0, 64, **kw)
+    assert out.u.shape == ref.u.shape
+    assert rel(to_np(out.u), ref.u) < 1e-5
