@@ -548,7 +548,7 @@ def mbs_arm(args):
 
     dev = torch.device("cuda", 0)
     rng = np.random.default_rng(0)
-    n_in, sp, lam = 256, 0.1, 0.5
+    n_in, sp, lam = args.mbs_side, 0.1, 0.5
     ax = (torch.arange(n_in, device=dev, dtype=torch.float32) - n_in // 2) * sp
     n = torch.full((n_in, n_in, n_in), 1.33, device=dev)
     for _ in range(200):
@@ -578,7 +578,7 @@ def mbs_arm(args):
     per_it = loop_ms / it
     line = _base_line("Mvoxel-iterations/s, modified Born series", round(vox * it / (ms * 1e-3) / 1e6, 1),
                       "Mvoxel-iterations/s", it, 0, ms, "c64 (FP64 residual)",
-                      {"workload": "MBS 256^3 + 32-voxel absorbing boundary (320^3), 200 spheres, spacing 0.1, "
+                      {"workload": f"MBS {n_in}^3 + 32-voxel absorbing boundary ({X}^3), 200 spheres, spacing 0.1, "
                                    "lambda 0.5, current sheet, to relative residual < 1e-5", "l2": "inputs larger than L2"},
                       iterations=it, residual_rel=info["residual_rel"], converged=info["residual_rel"] < 1e-5,
                       ms_per_iteration=round(per_it, 4), iteration_loop_ms=round(loop_ms, 2),
@@ -782,6 +782,7 @@ def main():
                     help="psf: the batched 4f PSF stack (headline); the others print one line each for the "
                          "other configurations")
     ap.add_argument("--mbs-maxiter", type=int, default=4000)
+    ap.add_argument("--mbs-side", type=int, default=256, help="mbs: interior grid side (+64 boundary voxels)")
     ap.add_argument("--rate", type=float, default=2000.0, help="serve: mean arrivals per second")
     ap.add_argument("--serve-seconds", type=float, default=2.0, help="serve: length of the arrival stream")
     args = ap.parse_args()

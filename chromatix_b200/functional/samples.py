@@ -129,6 +129,37 @@ def _autograd_fn():
 _MS_FN = None
 
 
+def _multislice_stack(field: Field, absorption_stack, dn_stack, n, thickness_per_slice, pad_width, kykx,
+                      remove_evanescent, bandlimit, precision) -> Field:
+    """``return_stack=True`` (functional/samples.py:253-260): the field after
+    every slice, without the final defocus, cropped; the plane index becomes
+    the innermost batch axis.  Each slice is one call of the fused slice loop
+    on the padded grid (differentiable like the whole stack)."""
+    from ..core.field import crop, pad
+
+    torch = nat.torch_mod()
+    dn = dn_stack if isinstance(dn_stack, torch.Tensor) else torch.as_tensor(np.asarray(dn_stack, np.float32))
+    ab = absorption_stack if isinstance(absorption_stack, torch.Tensor) else torch.as_tensor(
+        np.asarray(absorption_stack, np.float32))
+    dn = dn.to(device=field.device, dtype=torch.float32)
+    ab = ab.to(device=field.device, dtype=torch.float32)
+    if tuple(dn.shape) != tuple(ab.shape):
+        raise AssertionError("absorption_stack and dn_stack must have equal shapes")
+    p = int(pad_width)
+    # center_pad of the stacks (samples.py:224-225): zero index change and absorption in the padding
+    dn = torch.nn.functional.pad(dn, (p, p, p, p))
+    ab = torch.nn.functional.pad(ab, (p, p, p, p))
+    f = pad(field, p)
+    planes = []
+    for i in range(dn.shape[0]):
+        f = multislice_thick_sample(f, ab[i:i + 1], dn[i:i + 1], n, thickness_per_slice, 0, kykx=kykx,
+                                    reverse_propagate_distance=0.0, remove_evanescent=remove_evanescent,
+                                    bandlimit=bandlimit, precision=precision)
+        planes.append(f.u)
+    axis = -4 if field.chromatic else -3
+    return crop(field.replace(u=torch.stack(planes, dim=planes[0].ndim + axis + 1)), p)
+
+
 def multislice_thick_sample(field: Field, absorption_stack, dn_stack, n, thickness_per_slice, pad_width: int,
                             NA=None, propagator=None, kykx=(0.0, 0.0), reverse_propagate_distance=None,
                             return_stack: bool = False, remove_evanescent: bool = False, bandlimit: bool = False,
@@ -154,7 +185,8 @@ def multislice_thick_sample(field: Field, absorption_stack, dn_stack, n, thickne
     if propagator is not None:
         raise NotImplementedError("a custom propagator is not supported by the fused slice kernel")
     if return_stack:
-        raise NotImplementedError("return_stack is not supported by the fused slice kernel")
+        return _multislice_stack(field, absorption_stack, dn_stack, n, thickness_per_slice, pad_width, kykx,
+                                 remove_evanescent, bandlimit, precision)
     dev = field.device
     dn = dn_stack if isinstance(dn_stack, torch.Tensor) else torch.as_tensor(np.asarray(dn_stack, np.float32))
     ab = absorption_stack if isinstance(absorption_stack, torch.Tensor) else torch.as_tensor(

@@ -121,3 +121,20 @@ def test_field_gradient_and_batch():
     (out.u.abs() ** 2).sum().backward()
     # the map is unitary up to absorption: d/du sum|u_out|^2 = 2 A^H A u, nonzero
     assert float(ut.grad.abs().sum()) > 0
+
+
+def test_return_stack_planes_match_partial_stacks():
+    """return_stack (functional/samples.py:253-260): plane k of the stack is the
+    field after the first k slices (no final defocus), cropped."""
+    import chromatix_b200.functional as cf
+
+    ny, nx, D, pad = 48, 64, 5, 8
+    u = rand_field((ny, nx), seed=9)
+    dn, ab = _sample(D, ny, nx, seed=10)
+    fc = cuda_field(u, 0.1, 0.532)
+    st = cf.multislice_thick_sample(fc, ab, dn, 1.33, 0.2, pad, return_stack=True)
+    assert tuple(st.u.shape) == (D, ny, nx)
+    for k in (1, 3, 5):
+        ref = O.multislice_thick_sample(oracle_field(u, 0.1, 0.532), ab[:k], dn[:k], 1.33, 0.2, pad,
+                                        reverse_propagate_distance=0.0)
+        assert rel(to_np(st.u[k - 1]), ref.u) < 1e-5
