@@ -434,13 +434,18 @@ struct Stage {
       const int j = (EXACT || lane + it * LPV < NBF) ? lane + it * LPV : NBF - 1;
       {
 #pragma unroll
-        for (int r = 0; r < R; ++r) {
-          const int n = j + r * NBF;
-          if constexpr (FIRST) {
-            v[it][r] = load(n);
-          } else {
-            v[it][r] = s[pad_idx(n)];
-          }
+        if constexpr (FIRST) {
+#pragma unroll
+          for (int r = 0; r < R; ++r) v[it][r] = load(j + r * NBF);
+        } else if constexpr (NBF % 16 == 0) {
+          // pad_idx(j + r NBF) = pad_idx(j) + r (NBF + NBF/16): one address,
+          // immediate offsets
+          const float2* sp = s + pad_idx(j);
+#pragma unroll
+          for (int r = 0; r < R; ++r) v[it][r] = sp[r * (NBF + NBF / 16)];
+        } else {
+#pragma unroll
+          for (int r = 0; r < R; ++r) v[it][r] = s[pad_idx(j + r * NBF)];
         }
         if constexpr (!FIRST) {
           const int k = j % NS;
@@ -469,8 +474,20 @@ struct Stage {
         if (EXACT || j < NBF) {
           const int k = j % NS;
           const int base = (j - k) * R + k;
+          if constexpr (NS % 16 == 0) {
+            float2* sp = s + pad_idx(base);
 #pragma unroll
-          for (int r = 0; r < R; ++r) s[pad_idx(base + r * NS)] = v[it][r];
+            for (int r = 0; r < R; ++r) sp[r * (NS + NS / 16)] = v[it][r];
+          } else if constexpr (NS == 1 && 16 % R == 0) {
+            // base = j R is a multiple of R, so base + r (r < R) stays in one
+            // run of 16 and pad_idx(base + r) = pad_idx(base) + r
+            float2* sp = s + pad_idx(base);
+#pragma unroll
+            for (int r = 0; r < R; ++r) sp[r] = v[it][r];
+          } else {
+#pragma unroll
+            for (int r = 0; r < R; ++r) s[pad_idx(base + r * NS)] = v[it][r];
+          }
         }
       }
       team_barrier<LPV, CTA>(team);

@@ -45,7 +45,14 @@ __device__ __forceinline__ float2 mbs_disc(const MbsArgs& a, float2 v, float2 e)
   return cmul(v, f);
 }
 
-// lines along z: one team per (component, ix, iy)
+// lines along z: one team per (ix, iy) line, the three components in turn,
+// so the line's permittivity is read from HBM once (kept in shared memory)
+template <int NZ>
+struct MbsZCfg {
+  using C = RowCfg<NZ>;
+  static constexpr size_t SMEM = C::SMEM + sizeof(float2) * (size_t)C::TEAMS * NZ;
+};
+
 template <int NZ, int MODE>
 __global__ void __launch_bounds__(RowCfg<NZ>::THREADS, RowCfg<NZ>::MINB) k_mbs_z(MbsArgs a) {
   using C = RowCfg<NZ>;
@@ -55,48 +62,55 @@ __global__ void __launch_bounds__(RowCfg<NZ>::THREADS, RowCfg<NZ>::MINB) k_mbs_z
   __syncthreads();
   const int team = threadIdx.x / C::LPV, lane = threadIdx.x % C::LPV;
   float2* s = sm + C::TW + team * Plan<NZ>::LEN;
-  const long lines = 3L * a.X * a.Y;
+  float2* se = sm + C::TW + C::TEAMS * Plan<NZ>::LEN + team * NZ;  // the line's permittivity
+  const long lines = (long)a.X * a.Y;
   const float inv_n = 1.0f / ((float)a.X * (float)a.Y * (float)a.Z);
   double dsum = 0.0, nsum = 0.0;
   for (long base = (long)blockIdx.x * C::TEAMS; base < lines; base += (long)gridDim.x * C::TEAMS) {
-    const long line = base + team;
-    if (line >= lines) continue;
-    const long comp = line / ((long)a.X * a.Y);
-    const long xy = line % ((long)a.X * a.Y);
-    const size_t off = (size_t)comp * a.vox + (size_t)xy * a.Z;
-    const float2* erow = a.eps + (size_t)xy * a.Z;
-    float2* brow = a.buf + off;
-    if constexpr (MODE == MBS_Z_DISC || MODE == MBS_Z_SCALE) {
-      const float2* xrow = a.x + off;
-      auto load = [&](int k) -> float2 {
-        return MODE == MBS_Z_DISC ? mbs_disc(a, xrow[k], erow[k]) : cmul(a.s, xrow[k]);
-      };
-      auto store = [&](int k, float2 v, int) { brow[k] = v; };
-      team_fft_ex<NZ, false, true, false>(s, tw, lane, team, load, store);
-    } else {
-      auto load = [&](int k) -> float2 { return brow[k]; };
-      if constexpr (MODE == MBS_ZI_STEP) {
+    const long xy = base + team;
+    if (xy >= lines) continue;
+    if constexpr (MODE != MBS_Z_SCALE) {
+      const float2* erow = a.eps + (size_t)xy * a.Z;
+      team_sync<C::LPV>(team);  // the previous line's reads of se are complete
+      for (int k = lane; k < NZ; k += C::LPV) se[k] = erow[k];
+      team_sync<C::LPV>(team);
+    }
+#pragma unroll 1
+    for (int comp = 0; comp < 3; ++comp) {
+      const size_t off = (size_t)comp * a.vox + (size_t)xy * a.Z;
+      float2* brow = a.buf + off;
+      if constexpr (MODE == MBS_Z_DISC || MODE == MBS_Z_SCALE) {
         const float2* xrow = a.x + off;
-        const float2* prow = a.prec_y + off;
-        float2* orow = a.x_new + off;
-        auto store = [&](int k, float2 g, int) {
-          const float2 xo = xrow[k];
-          const float2 gk = cscale(g, inv_n);
-          const float2 vx = mbs_disc(a, cadd(gk, xo), erow[k]);
-          const float2 xn = cadd(cadd(prow[k], vx), xo);
-          orow[k] = xn;
-          const float2 dd = csub(xn, xo);
-          dsum += (double)dd.x * dd.x + (double)dd.y * dd.y;
-          nsum += (double)xn.x * xn.x + (double)xn.y * xn.y;
+        auto load = [&](int k) -> float2 {
+          return MODE == MBS_Z_DISC ? mbs_disc(a, xrow[k], se[k]) : cmul(a.s, xrow[k]);
         };
-        team_fft_ex<NZ, true, false, true>(s, tw, lane, team, load, store);
-      } else {  // MBS_ZI_PREC: prec_y = -V(G)
-        float2* orow = a.x_new + off;
-        auto store = [&](int k, float2 g, int) {
-          const float2 v = mbs_disc(a, cscale(g, inv_n), erow[k]);
-          orow[k] = make_float2(-v.x, -v.y);
-        };
-        team_fft_ex<NZ, true, false, true>(s, tw, lane, team, load, store);
+        auto store = [&](int k, float2 v, int) { brow[k] = v; };
+        team_fft_ex<NZ, false, true, false>(s, tw, lane, team, load, store);
+      } else {
+        auto load = [&](int k) -> float2 { return brow[k]; };
+        if constexpr (MODE == MBS_ZI_STEP) {
+          const float2* xrow = a.x + off;
+          const float2* prow = a.prec_y + off;
+          float2* orow = a.x_new + off;
+          auto store = [&](int k, float2 g, int) {
+            const float2 xo = xrow[k];
+            const float2 gk = cscale(g, inv_n);
+            const float2 vx = mbs_disc(a, cadd(gk, xo), se[k]);
+            const float2 xn = cadd(cadd(prow[k], vx), xo);
+            orow[k] = xn;
+            const float2 dd = csub(xn, xo);
+            dsum += (double)dd.x * dd.x + (double)dd.y * dd.y;
+            nsum += (double)xn.x * xn.x + (double)xn.y * xn.y;
+          };
+          team_fft_ex<NZ, true, false, true>(s, tw, lane, team, load, store);
+        } else {  // MBS_ZI_PREC: prec_y = -V(G)
+          float2* orow = a.x_new + off;
+          auto store = [&](int k, float2 g, int) {
+            const float2 v = mbs_disc(a, cscale(g, inv_n), se[k]);
+            orow[k] = make_float2(-v.x, -v.y);
+          };
+          team_fft_ex<NZ, true, false, true>(s, tw, lane, team, load, store);
+        }
       }
     }
   }
@@ -200,38 +214,45 @@ __global__ void __launch_bounds__(MbsXCfg<NX>::THREADS, MbsXCfg<NX>::MINB) k_mbs
     auto store = [&](int k, float2 v, int) { s[pad_idx(k)] = v; };
     team_fft<NX, false, LPV, Q::CTA>(s, tw, lane, team, load, store);
     __syncthreads();
-    // k-space operator, cooperatively over (kx, column)
-    for (int idx = threadIdx.x; idx < NX * V; idx += blockDim.x) {
-      const int kx = idx / V, c = idx % V;
+    // k-space operator, cooperatively over (kx, column): blockDim.x is a
+    // multiple of V, so each thread keeps one column c and its (ky, kz)
+    {
+      const int c = threadIdx.x % V;
       const long i = i0 + c;
-      if (i >= inner) continue;
-      const int iy = (int)(i / a.Z), iz = (int)(i % a.Z);
-      const float kxv = a.kfx * (float)freq_index(kx, a.X);
+      const bool col_ok = i < inner;
+      const long ii = col_ok ? i : 0;
+      const int iy = (int)(ii / a.Z), iz = (int)(ii - (long)iy * a.Z);
       const float kyv = a.kfy * (float)freq_index(iy, a.Y);
       const float kzv = a.kfz * (float)freq_index(iz, a.Z);
-      const float ksq = kxv * kxv + kyv * kyv + kzv * kzv;
-      float2* p0 = tile + (0 * V + c) * LEN + pad_idx(kx);
-      float2* p1 = tile + (1 * V + c) * LEN + pad_idx(kx);
-      float2* p2 = tile + (2 * V + c) * LEN + pad_idx(kx);
-      const float2 y0 = *p0, y1 = *p1, y2 = *p2;
-      // longitudinal part k (k . y) / |k|^2 (zero at k = 0)
-      float2 l0 = make_float2(0.f, 0.f), l1 = l0, l2 = l0;
-      if (ksq != 0.f) {
-        const float2 proj = make_float2((kxv * y0.x + kyv * y1.x + kzv * y2.x) / ksq,
-                                        (kxv * y0.y + kyv * y1.y + kzv * y2.y) / ksq);
-        l0 = cscale(proj, kxv);
-        l1 = cscale(proj, kyv);
-        l2 = cscale(proj, kzv);
-      }
-      // 1 / (kb2 - s ksq) and 1 / kb2
-      const float2 dt = make_float2(a.kb2.x - a.s.x * ksq, a.kb2.y - a.s.y * ksq);
-      const float dn = dt.x * dt.x + dt.y * dt.y;
-      const float2 it = make_float2(dt.x / dn, -dt.y / dn);
+      const float kyz = kyv * kyv + kzv * kzv;
+      // 1 / kb2 (longitudinal part), a per-call constant
       const float bn = a.kb2.x * a.kb2.x + a.kb2.y * a.kb2.y;
       const float2 il = make_float2(a.kb2.x / bn, -a.kb2.y / bn);
-      *p0 = cadd(cmul(csub(y0, l0), it), cmul(l0, il));
-      *p1 = cadd(cmul(csub(y1, l1), it), cmul(l1, il));
-      *p2 = cadd(cmul(csub(y2, l2), it), cmul(l2, il));
+      for (int kx = threadIdx.x / V; col_ok && kx < NX; kx += blockDim.x / V) {
+        const float kxv = a.kfx * (float)freq_index(kx, a.X);
+        const float ksq = kxv * kxv + kyz;
+        float2* p0 = tile + (0 * V + c) * LEN + pad_idx(kx);
+        float2* p1 = tile + (1 * V + c) * LEN + pad_idx(kx);
+        float2* p2 = tile + (2 * V + c) * LEN + pad_idx(kx);
+        const float2 y0 = *p0, y1 = *p1, y2 = *p2;
+        // longitudinal part k (k . y) / |k|^2 (zero at k = 0)
+        float2 l0 = make_float2(0.f, 0.f), l1 = l0, l2 = l0;
+        if (ksq != 0.f) {
+          const float r = __frcp_rn(ksq);
+          const float2 proj = make_float2((kxv * y0.x + kyv * y1.x + kzv * y2.x) * r,
+                                          (kxv * y0.y + kyv * y1.y + kzv * y2.y) * r);
+          l0 = cscale(proj, kxv);
+          l1 = cscale(proj, kyv);
+          l2 = cscale(proj, kzv);
+        }
+        // 1 / (kb2 - s ksq) = conj(dt) / |dt|^2
+        const float2 dt = make_float2(a.kb2.x - a.s.x * ksq, a.kb2.y - a.s.y * ksq);
+        const float rd = __frcp_rn(dt.x * dt.x + dt.y * dt.y);
+        const float2 it = make_float2(dt.x * rd, -dt.y * rd);
+        *p0 = cadd(cmul(csub(y0, l0), it), cmul(l0, il));
+        *p1 = cadd(cmul(csub(y1, l1), it), cmul(l1, il));
+        *p2 = cadd(cmul(csub(y2, l2), it), cmul(l2, il));
+      }
     }
     __syncthreads();
     team_fft<NX, true, LPV, Q::CTA>(s, tw, lane, team, load, store);

@@ -11,10 +11,11 @@ namespace cx {
 template <int N, int MODE>
 static cx_status launch_z(const MbsArgs& a, cudaStream_t st) {
   using C = RowCfg<N>;
+  constexpr size_t SMEM = MbsZCfg<N>::SMEM;
   auto k = k_mbs_z<N, MODE>;
-  CX_CUDA_TRY(set_smem(k, C::SMEM));
-  const long items = (3L * a.X * a.Y + C::TEAMS - 1) / C::TEAMS;
-  k<<<persistent_grid(k, C::THREADS, C::SMEM, items), C::THREADS, C::SMEM, st>>>(a);
+  CX_CUDA_TRY(set_smem(k, SMEM));
+  const long items = ((long)a.X * a.Y + C::TEAMS - 1) / C::TEAMS;
+  k<<<persistent_grid(k, C::THREADS, SMEM, items), C::THREADS, SMEM, st>>>(a);
   CX_LAUNCH_CHECK();
   return CX_OK;
 }
