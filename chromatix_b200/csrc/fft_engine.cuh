@@ -412,7 +412,9 @@ __device__ __forceinline__ void apply_twiddles(const float2* tw, int m, float2* 
 // ---------------------------------------------------------------------------
 // the stage recursion
 // ---------------------------------------------------------------------------
-template <int N, int LPV, bool INV, int SI, int NS, bool CTA = false>
+// ZM (first stage only): bit r set = inputs j + r N/R_0 are known to be zero
+// for every j, so they are compile-time zeros and their arithmetic folds away
+template <int N, int LPV, bool INV, int SI, int NS, bool CTA = false, unsigned ZM = 0u>
 struct Stage {
   static constexpr int S = Plan<N>::S;
   static constexpr int R = Plan<N>::radix(SI);
@@ -436,7 +438,7 @@ struct Stage {
 #pragma unroll
         if constexpr (FIRST) {
 #pragma unroll
-          for (int r = 0; r < R; ++r) v[it][r] = load(j + r * NBF);
+          for (int r = 0; r < R; ++r) v[it][r] = ((ZM >> r) & 1u) ? make_float2(0.f, 0.f) : load(j + r * NBF);
         } else if constexpr (NBF % 16 == 0) {
           // pad_idx(j + r NBF) = pad_idx(j) + r (NBF + NBF/16): one address,
           // immediate offsets
@@ -497,8 +499,8 @@ struct Stage {
 };
 
 // terminate recursion past the last stage (never instantiated at run time)
-template <int N, int LPV, bool INV, int NS, bool CTA>
-struct Stage<N, LPV, INV, 16, NS, CTA> {
+template <int N, int LPV, bool INV, int NS, bool CTA, unsigned ZM>
+struct Stage<N, LPV, INV, 16, NS, CTA, ZM> {
   template <class Load, class Store>
   __device__ static void run(float2*, const float2*, int, int, Load&, Store&) {}
 };
@@ -510,9 +512,20 @@ struct Stage<N, LPV, INV, 16, NS, CTA> {
 // lanes of the team must call this (inactive lanes still take part in the
 // team barriers).  Outputs are unnormalised (numpy convention for the
 // forward transform; the inverse omits the 1/N).
-template <int N, bool INV, int LPV = Plan<N>::LPV, bool CTA = false, class Load, class Store>
+template <int N, bool INV, int LPV = Plan<N>::LPV, bool CTA = false, unsigned ZM = 0u, class Load, class Store>
 __device__ __forceinline__ void team_fft(float2* s, const float2* tw, int lane, int team, Load& load, Store& store) {
-  Stage<N, LPV, INV, 0, 1, CTA>::run(s, tw, lane, team, load, store);
+  Stage<N, LPV, INV, 0, 1, CTA, ZM>::run(s, tw, lane, team, load, store);
+}
+
+// Zero mask for team_fft when the input vector is nonzero only on
+// [0, h) and [N - h, N) with h <= Q N / R_0 (a centred support after an
+// ifftshift): first-stage inputs r in [Q, R_0 - Q) are zero.
+template <int N, int Q>
+__host__ __device__ constexpr unsigned edge_zero_mask() {
+  constexpr int R0 = Plan<N>::P.r[0];
+  unsigned m = 0u;
+  for (int r = Q; r < R0 - Q; ++r) m |= 1u << r;
+  return m;
 }
 
 // Same transform with the load and/or store functor applied in a compact,

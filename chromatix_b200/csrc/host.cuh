@@ -126,11 +126,11 @@ struct RowCfg {
 // Row kernels whose teams all run one transform per loop iteration (no
 // per-team early exit): exact lane counts with CTA-wide barriers where the
 // count does not tile warps, about 192 threads in whole warps.
-template <int N>
+template <int N, int TARGET = 192>
 struct RowCfgX {
   static constexpr bool CTA = Plan<N>::LPV_X != Plan<N>::LPV;
   static constexpr int LPV = CTA ? Plan<N>::LPV_X : Plan<N>::LPV;
-  static constexpr int T1 = 192 / LPV > 0 ? 192 / LPV : 1;
+  static constexpr int T1 = TARGET / LPV > 0 ? TARGET / LPV : 1;
   static constexpr int teams_for() {
     int t = T1;
     if (CTA) {

@@ -117,8 +117,11 @@ __device__ __forceinline__ float2 psf_const(const PsfArgs& a, int w, const unsig
 // the pupil transform zeros and store nothing), so teams can have the exact
 // lane count and share CTA-wide barriers.
 template <int NX>
-__global__ void __launch_bounds__(RowCfgX<NX>::THREADS, RowCfgX<NX>::MINB) k_psf_rows_tab(PsfArgs a) {
-  using C = RowCfgX<NX>;
+using PsfRowCfg = RowCfgX<NX>;
+
+template <int NX, int Q>
+__global__ void __launch_bounds__(PsfRowCfg<NX>::THREADS, PsfRowCfg<NX>::MINB) k_psf_rows_tab(PsfArgs a) {
+  using C = PsfRowCfg<NX>;
   extern __shared__ float2 sm[];
   float2* tw = sm;
   load_twiddles<NX>(tw, a.twg, threadIdx.x, blockDim.x);
@@ -153,7 +156,7 @@ __global__ void __launch_bounds__(RowCfgX<NX>::THREADS, RowCfgX<NX>::MINB) k_psf
     auto store = [&](int k, float2 v, int) {
       if (live) dst[k] = v;
     };
-    team_fft<NX, false, C::LPV, C::CTA>(s, tw, lane, team, load, store);
+    team_fft<NX, false, C::LPV, C::CTA, (Q > 0 ? edge_zero_mask<NX, Q>() : 0u)>(s, tw, lane, team, load, store);
   }
 }
 
@@ -231,7 +234,9 @@ struct PsfColCfg {
   static constexpr size_t SMEM = ((C::SMEM + 15) & ~(size_t)15) + sizeof(float) * (size_t)C::V * ACC;
 };
 
-template <int NY>
+// Q > 0: every wavelength's pupil rows map to FFT rows within Q N/R_0 of the
+// ends (checked on the host), so the first stage skips the zero inputs
+template <int NY, int Q>
 __global__ void __launch_bounds__(ColCfg<NY>::THREADS, ColCfg<NY>::MINB) k_psf_cols(PsfArgs a) {
   using C = ColCfg<NY>;
   constexpr int V = C::V, LEN = C::LEN, ACC = PsfColCfg<NY>::ACC;
@@ -270,7 +275,7 @@ __global__ void __launch_bounds__(ColCfg<NY>::THREADS, ColCfg<NY>::MINB) k_psf_c
         const float e = dens * cabs2(v);
         acc[k] = (w == 0) ? e : acc[k] + e;
       };
-      team_fft<NY, false, C::LPV, C::CTA>(s, tw, lane, team, load, store);
+      team_fft<NY, false, C::LPV, C::CTA, (Q > 0 ? edge_zero_mask<NY, Q>() : 0u)>(s, tw, lane, team, load, store);
     }
     __syncthreads();
     float* outz = a.out + (size_t)(a.z0 + zl) * a.ny * a.nx;
@@ -286,6 +291,21 @@ __global__ void __launch_bounds__(ColCfg<NY>::THREADS, ColCfg<NY>::MINB) k_psf_c
 
 // accurate-mode source tables M and CX (see PsfArgs), after the count pass
 __global__ void k_psf_tables(PsfArgs a);
+
+// The pupil boxes of every wavelength (rows [ylo, ylo + nrows) or columns
+// [xlo, xlo + ncols) of a length-n axis) map, after the ifftshift, to FFT
+// indices within q n / r0 of both ends
+inline bool psf_edges_within(const PsfArgs& a, bool rows, int n, int r0, int q) {
+  const long lim = (long)q * (n / r0);
+  for (int w = 0; w < a.W; ++w) {
+    const long lo = rows ? a.ylo[w] : a.xlo[w];
+    const long hi = lo + (rows ? a.nrows[w] : a.ncols[w]);  // exclusive
+    if (hi - n / 2 > lim || n / 2 - lo > lim) return false;
+  }
+  return true;
+}
+
+constexpr int PSF_EDGE_Q = 3;
 
 cx_status psf_dispatch_rows(int n, const PsfArgs& a, cudaStream_t st);
 cx_status psf_dispatch_cols(int n, const PsfArgs& a, cudaStream_t st);

@@ -6,7 +6,8 @@ namespace cx {
 template <int NY>
 static cx_status launch_psf_cols(const PsfArgs& a, cudaStream_t st) {
   using C = ColCfg<NY>;
-  auto k = k_psf_cols<NY>;
+  auto k = psf_edges_within(a, true, NY, Plan<NY>::P.r[0], PSF_EDGE_Q) ? k_psf_cols<NY, PSF_EDGE_Q>
+                                                                        : k_psf_cols<NY, 0>;
   CX_CUDA_TRY(set_smem(k, PsfColCfg<NY>::SMEM));
   const long items = (long)((a.nx + C::V - 1) / C::V) * a.zc;
   const int grid = persistent_grid(k, C::THREADS, PsfColCfg<NY>::SMEM, items);
