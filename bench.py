@@ -59,6 +59,18 @@ def inputs(seed=0):
     return z, phase, dx
 
 
+def max_over_ranks(values, dist=None, device=None):
+    """Element-wise maximum of per-rank timings over all ranks (identity
+    without a process group); every rank gets the result."""
+    if dist is None:
+        return [float(v) for v in values]
+    import torch
+
+    t = torch.tensor([float(v) for v in values], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return [float(v) for v in t.cpu()]
+
+
 # ---------------------------------------------------------------------------
 # clocks
 # ---------------------------------------------------------------------------
@@ -193,10 +205,7 @@ def gpu_arm(args):
     # on the launching stream: one chunk of the same workload
     kern = dominant_kernel_time(dev, z, phase_d, dx)
 
-    if dist:
-        t = torch.tensor([ms, ms_e2e], device=dev, dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms, ms_e2e = float(t[0]), float(t[1])
+    ms, ms_e2e = max_over_ranks([ms, ms_e2e], dist, dev)
     value = PX_PER_STEP * world / (ms * 1e-3) / 1e6
     e2e_value = PX_PER_STEP * world / (ms_e2e * 1e-3) / 1e6
 
