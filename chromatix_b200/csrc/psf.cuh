@@ -305,7 +305,14 @@ inline bool psf_edges_within(const PsfArgs& a, bool rows, int n, int r0, int q) 
   return true;
 }
 
-constexpr int PSF_EDGE_Q = 3;
+// the narrowest first-stage band (in units of N / R_0 from each end) that
+// holds every wavelength's pupil box: 3, 4 or 6, else 0 (dense)
+inline int psf_edge_q(const PsfArgs& a, bool rows, int n, int r0) {
+  if (r0 < 16) return 0;
+  for (int q : {3, 4, 6})
+    if (psf_edges_within(a, rows, n, r0, q)) return q;
+  return 0;
+}
 
 cx_status psf_dispatch_rows(int n, const PsfArgs& a, cudaStream_t st);
 cx_status psf_dispatch_cols(int n, const PsfArgs& a, cudaStream_t st);

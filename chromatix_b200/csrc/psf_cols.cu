@@ -6,8 +6,8 @@ namespace cx {
 template <int NY>
 static cx_status launch_psf_cols(const PsfArgs& a, cudaStream_t st) {
   using C = ColCfg<NY>;
-  auto k = psf_edges_within(a, true, NY, Plan<NY>::P.r[0], PSF_EDGE_Q) ? k_psf_cols<NY, PSF_EDGE_Q>
-                                                                        : k_psf_cols<NY, 0>;
+  const int q = psf_edge_q(a, true, NY, Plan<NY>::P.r[0]);
+  auto k = q == 3 ? k_psf_cols<NY, 3> : q == 4 ? k_psf_cols<NY, 4> : q == 6 ? k_psf_cols<NY, 6> : k_psf_cols<NY, 0>;
   CX_CUDA_TRY(set_smem(k, PsfColCfg<NY>::SMEM));
   const long items = (long)((a.nx + C::V - 1) / C::V) * a.zc;
   const int grid = persistent_grid(k, C::THREADS, PsfColCfg<NY>::SMEM, items);

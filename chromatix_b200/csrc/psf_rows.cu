@@ -8,8 +8,11 @@ static cx_status launch_psf_rows(const PsfArgs& a, cudaStream_t st) {
   const long rows = (long)a.zc * a.rowsum;
   if (a.precision != CX_PREC_REF32) {
     using C = PsfRowCfg<NX>;
-    auto k = psf_edges_within(a, false, NX, Plan<NX>::P.r[0], PSF_EDGE_Q) ? k_psf_rows_tab<NX, PSF_EDGE_Q>
-                                                                          : k_psf_rows_tab<NX, 0>;
+    const int q = psf_edge_q(a, false, NX, Plan<NX>::P.r[0]);
+    auto k = q == 3   ? k_psf_rows_tab<NX, 3>
+             : q == 4 ? k_psf_rows_tab<NX, 4>
+             : q == 6 ? k_psf_rows_tab<NX, 6>
+                      : k_psf_rows_tab<NX, 0>;
     CX_CUDA_TRY(set_smem(k, C::SMEM));
     const int grid = persistent_grid(k, C::THREADS, C::SMEM, (rows + C::TEAMS - 1) / C::TEAMS);
     k<<<grid, C::THREADS, C::SMEM, st>>>(a);
