@@ -414,6 +414,38 @@ def psf_published_arm(args):
     print(json.dumps(line), flush=True)
 
 
+def microscope_published_arm(args):
+    """The reference's published imaging benchmark (docs/parallelism.md:118-181):
+    Microscope(Optical4FSystemPSF(1536^2, spacing 0.3 um, phase zeros),
+    BasicSensor(resampling_method=None, reduce_axis=0), f = 100 um, n = 1.33,
+    NA 0.8, lambda 0.532 um) on a (128, 1536, 1536) volume of ones at z =
+    linspace(-4, 4, 128); published 172.86 ms on one A100.  The tube lens focal
+    length is not given there (older API); f_tube = f = 100 um here."""
+    import torch
+
+    from chromatix_b200.systems import BasicSensor, Microscope, Optical4FSystemPSF
+
+    dev = torch.device("cuda", 0)
+    shape, spacing = (1536, 1536), 0.3
+    n_z = 128
+    z = torch.linspace(-4, 4, n_z, dtype=torch.float64, device=dev)
+    volume = torch.ones((n_z,) + shape, dtype=torch.float32, device=dev)
+    phase = torch.zeros(shape, dtype=torch.float32, device=dev)
+    scope = Microscope(Optical4FSystemPSF(shape, spacing, 100.0, phase),
+                       BasicSensor(shape, spacing, resampling_method=None, reduce_axis=0), 100.0, 1.33, 0.8, 0.532)
+    with ClockSampler(0) as clk:
+        ms = _device_timer(torch, dev, args.steps, args.warmup)(lambda: scope(volume, z))
+    published = 172.86
+    line = _base_line("ms, Microscope image of a 128 x 1536^2 volume (the reference's published benchmark)",
+                      round(ms, 3), "ms", args.steps, args.warmup, ms, "c64/f32",
+                      {"workload": "Microscope(Optical4FSystemPSF 1536^2, BasicSensor reduce_axis=0), 128 planes, "
+                                   "NA 0.8, f 100 um, lambda 0.532, volume of ones", "l2": "flushed between timed steps"},
+                      higher_is_better=False, vs_baseline=round(published / ms, 1),
+                      baseline={"ms": published, "hardware": "1x A100 (docs/parallelism.md:182)"},
+                      clocks=clk.summary())
+    print(json.dumps(line), flush=True)
+
+
 def rescaled_published_arm(args):
     """The reference's published rescaled-propagation timings
     (docs/examples/rescaled_propagation.ipynb, cells 4, 8, 19): 1024^2 plane
@@ -787,7 +819,8 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--accuracy", action="store_true", help="also report the error vs the FP64 oracle")
     ap.add_argument("--workload", default="psf",
-                    choices=["psf", "serve", "psf_published", "rescaled_published", "asm", "multislice", "mbs"],
+                    choices=["psf", "serve", "psf_published", "rescaled_published", "microscope_published", "asm",
+                             "multislice", "mbs"],
                     help="psf: the batched 4f PSF stack (headline); the others print one line each for the "
                          "other configurations")
     ap.add_argument("--mbs-maxiter", type=int, default=4000)
@@ -807,6 +840,8 @@ def main():
         asm_arm(args)
     elif args.workload == "rescaled_published":
         rescaled_published_arm(args)
+    elif args.workload == "microscope_published":
+        microscope_published_arm(args)
     elif args.workload == "multislice":
         multislice_arm(args)
     elif args.workload == "mbs":

@@ -339,6 +339,23 @@ cx_status cx_czt_propagate(const cx_czt_prop_desc* d, const void* u_in, void* u_
                            size_t workspace_bytes, cx_stream_t stream);
 
 /* ---------------------------------------------------------------------------
+ * Incoherent imaging: fourier_convolution (ops/ops.py:9-86, axes (-2, -1),
+ * mode "same", fast_fft_shape) of a sample stack with a PSF stack, plane by
+ * plane, and the sensor's sum over the planes (functional/sensors.py:85-86,
+ * systems/microscopes.py:271-297).  sample, psf: (n_planes, h, w) float32;
+ * out: (h, w) float32 if reduce, else (n_planes, h, w).  Transform size
+ * (next power of two of 2h, of 2w), at most 4096 per axis (w >= 2).
+ * ------------------------------------------------------------------------- */
+typedef struct {
+  int32_t n_planes, h, w;
+  int32_t reduce; /* 1: sum over the planes (BasicSensor(reduce_axis=0)) */
+} cx_conv_desc;
+
+cx_status cx_conv2d_workspace_size(const cx_conv_desc* d, size_t* bytes);
+cx_status cx_conv2d_same(const cx_conv_desc* d, const float* sample, const float* psf, float* out, void* workspace,
+                         size_t workspace_bytes, cx_stream_t stream);
+
+/* ---------------------------------------------------------------------------
  * Modified Born series (experimental/modified_born_series/solver.py:42-146)
  * Grid (X, Y, Z); fields are three component planes (3, X, Y, Z) complex64;
  * eps (X, Y, Z) complex64.  s = 1 / (1.1 i R) and kb2 = shift * s + 1 are the

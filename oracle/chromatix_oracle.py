@@ -1054,6 +1054,66 @@ def mbs_source_field(current_density, k0):
 
 
 # ---------------------------------------------------------------------------
+# incoherent imaging  (ops/ops.py, functional/sensors.py, systems/microscopes.py)
+# ---------------------------------------------------------------------------
+
+
+def next_order(val: int) -> int:
+    """``next_order`` (utils/utils.py:11-12): the next power of two."""
+    return int(2 ** np.ceil(np.log2(val)))
+
+
+def fourier_convolution(image, kernel, axes=(0, 1), fast_fft_shape=True, mode="same"):
+    """``fourier_convolution`` (ops/ops.py:9-86): rfftn/irfftn of real inputs at
+    the (next power of two of the) summed shape, cropped to ``image``'s shape
+    from offset (k - 1) // 2 for mode "same"."""
+    image = np.asarray(image)
+    kernel = np.asarray(kernel)
+    axes = [a if a >= 0 else image.ndim + a for a in axes]
+    padded = [image.shape[a] + kernel.shape[a] for a in axes]
+    fast = [next_order(k) for k in padded] if fast_fft_shape else padded
+    if np.iscomplexobj(image) or np.iscomplexobj(kernel):
+        conv = np.fft.ifftn(np.fft.fftn(image, s=fast, axes=axes) * np.fft.fftn(kernel, s=fast, axes=axes),
+                            s=fast, axes=axes)
+    else:
+        conv = np.fft.irfftn(np.fft.rfftn(image, s=fast, axes=axes) * np.fft.rfftn(kernel, s=fast, axes=axes),
+                             s=fast, axes=axes)
+    if mode == "same":
+        sl = tuple(slice((k - 1) // 2, (k - 1) // 2 + i) if idx in axes else slice(i)
+                   for idx, (i, k) in enumerate(zip(image.shape, kernel.shape)))
+        conv = conv[sl]
+    return conv
+
+
+def basic_sensor_reduce(intensity, reduce_axis=None):
+    """``basic_sensor`` (functional/sensors.py:14-92) without resampling or
+    shot noise: the optional sum over ``reduce_axis``."""
+    return np.sum(intensity, axis=reduce_axis) if reduce_axis is not None else intensity
+
+
+def optical_4f_required_spacing(height, output_spacing, f_tube, n, wavelength):
+    """``Optical4FSystemPSF.compute_required_spacing`` (systems/microscopes.py:357-365)."""
+    return f_tube * np.asarray(wavelength, np.float64) / (n * height * output_spacing)
+
+
+def microscope_image(sample, shape, spacing, f_tube, phase, f, n, NA, spectrum, z, reduce_axis=0,
+                     prec: Prec = FP64):
+    """``Microscope(Optical4FSystemPSF, BasicSensor(resampling_method=None))``
+    called on ``sample`` (systems/microscopes.py:197-213, 271-297, 334-355):
+    PSF intensity of the 4f system at every z, one plane-wise 2D Fourier
+    convolution per z (axes (-2, -1)), the sensor's sum over ``reduce_axis``.
+    padding_ratio = 0 and taper_width = 0 (the defaults)."""
+    spec = build_spectrum(spectrum, prec)
+    dx = optical_4f_required_spacing(shape[0], spacing, f_tube, n, spec.wavelength)
+    dxw = dx if spec.wavelength.size > 1 else float(dx.reshape(-1)[0])
+    fld = objective_point_source(shape, dxw, spectrum, z, f, n, NA, prec=prec)
+    fld = ff_lens(phase_change(fld, phase), f_tube, n)
+    psf = fld.intensity
+    image = fourier_convolution(sample, psf, axes=(-2, -1))
+    return basic_sensor_reduce(image, reduce_axis), psf
+
+
+# ---------------------------------------------------------------------------
 # misc helpers used by tests / baselines
 # ---------------------------------------------------------------------------
 

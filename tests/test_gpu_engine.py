@@ -6,7 +6,8 @@ import pytest
 from tests.helpers import to_np
 
 SIZES = [2, 3, 4, 5, 6, 7, 8, 10, 12, 14, 16, 20, 24, 28, 32, 40, 48, 56, 64, 80, 96, 112, 128, 160, 192, 224, 256,
-         320, 384, 448, 512, 640, 768, 896, 1024, 1280, 1536, 1792, 2048, 2560, 3072, 3584, 4096]
+         320, 384, 448, 512, 640, 768, 896, 1024, 1280, 1536, 1792, 2048, 2560, 3072, 3584, 4096,
+         4608, 5120, 6144, 7168, 8192]  # the last five: 1D / chirp-Z lengths only
 
 
 @pytest.mark.gpu
@@ -39,3 +40,16 @@ def test_fft1d_unsupported_length_is_an_error():
     x = torch.zeros(11 * 13, dtype=torch.complex64, device="cuda")
     with pytest.raises(nat.CxError):
         nat.check(nat.lib().cx_fft1d(nat.ptr(x), nat.ptr(x), 143, 1, 0, nat.stream_handle()))
+
+
+@pytest.mark.gpu
+def test_fft1d_empty_batch_is_a_no_op():
+    import torch
+
+    from chromatix_b200 import _native as nat
+
+    x = torch.zeros(8, dtype=torch.complex64, device="cuda")
+    y = torch.full_like(x, 3.0)
+    nat.check(nat.lib().cx_fft1d(nat.ptr(x), nat.ptr(y), 8, 0, 0, nat.stream_handle()))
+    torch.cuda.synchronize()
+    assert torch.all(y == 3.0)

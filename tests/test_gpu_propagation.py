@@ -188,3 +188,15 @@ def test_unsupported_sizes_fail_loudly():
     u = rand_field((11, 13), seed=10)
     with pytest.raises(nat.CxError):
         cf.asm_propagate(cuda_field(u, 0.1, 0.5), 1.0, 1.0, 0)
+
+
+def test_largest_grid_4096():
+    """The largest compiled 2D length: a 2048^2 field padded to 4096^2 (ASM, full)."""
+    import chromatix_b200.functional as cf
+
+    u = rand_field((2048, 2048), seed=21)
+    out = cf.asm_propagate(cuda_field(u, 0.3, 0.532), 200.0, 1.33, 1024)
+    O.set_fft_workers(8)
+    ref = O.asm_propagate(oracle_field(u, 0.3, 0.532), 200.0, 1.33, 1024)
+    assert out.u.shape == ref.u.shape == (4096, 4096)
+    assert rel(to_np(out.u), ref.u) < 1e-5
