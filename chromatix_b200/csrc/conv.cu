@@ -4,104 +4,42 @@
 
 namespace cx {
 
-template <int M>
-static cx_status launch_rows(const ConvArgs& a, cudaStream_t st) {
-  using C = RowCfg<M>;
-  auto k = k_conv_rows<M>;
-  CX_CUDA_TRY(set_smem(k, C::SMEM));
-  const long items = ((long)a.zc * 2 * a.h + C::TEAMS - 1) / C::TEAMS;
-  k<<<persistent_grid(k, C::THREADS, C::SMEM, items), C::THREADS, C::SMEM, st>>>(a);
-  CX_LAUNCH_CHECK();
-  return CX_OK;
-}
+#define CX_CONV_LIST_(N) N,
+static constexpr int kConvP[] = {CX_CONV_P_SIZES(CX_CONV_LIST_)};
+static constexpr int kConvM[] = {CX_CONV_M_SIZES(CX_CONV_LIST_)};
+#undef CX_CONV_LIST_
 
-template <int P>
-static cx_status launch_cols(const ConvArgs& a, cudaStream_t st) {
-  using Q = ConvColCfg<P>;
-  auto k = k_conv_cols<P>;
-  CX_CUDA_TRY(set_smem(k, Q::SMEM));
-  const long items = (a.NC + Q::V - 1) / Q::V;
-  k<<<persistent_grid(k, Q::THREADS, Q::SMEM, items), Q::THREADS, Q::SMEM, st>>>(a);
-  CX_LAUNCH_CHECK();
-  return CX_OK;
-}
-
-template <int P>
-static cx_status launch_fin_cols(const ConvArgs& a, cudaStream_t st) {
-  using C = RowCfg<P>;
-  auto k = k_conv_fin_cols<P>;
-  CX_CUDA_TRY(set_smem(k, C::SMEM));
-  const long items = ((long)a.NC + C::TEAMS - 1) / C::TEAMS;
-  k<<<persistent_grid(k, C::THREADS, C::SMEM, items), C::THREADS, C::SMEM, st>>>(a);
-  CX_LAUNCH_CHECK();
-  return CX_OK;
-}
-
-template <int M>
-static cx_status launch_fin_rows(const ConvArgs& a, cudaStream_t st) {
-  using Q = ConvFinCfg<M>;
-  auto k = k_conv_fin_rows<M>;
-  CX_CUDA_TRY(set_smem(k, Q::SMEM));
-  const long items = (a.h + Q::V - 1) / Q::V;
-  k<<<persistent_grid(k, Q::THREADS, Q::SMEM, items), Q::THREADS, Q::SMEM, st>>>(a);
-  CX_LAUNCH_CHECK();
-  return CX_OK;
-}
-
-#define CX_CONV_DISPATCH_(NAME, FN, VAR)                 \
-  cx_status NAME(int VAR, const ConvArgs& a, cudaStream_t st) { \
-    switch (VAR) {                                       \
-      CX_CONV_SIZES(CX_CONV_CASE_)                       \
-    }                                                    \
-    set_error("convolution length %d is not supported", VAR); \
-    return CX_ERR_UNSUPPORTED;                           \
+// smallest length >= need in an ascending list (times `mul`), powers of two
+// only on request; 0 if none
+template <size_t K>
+static int conv_len(const int (&list)[K], int mul, long need, bool pow2) {
+  for (size_t i = 0; i < K; ++i) {
+    const long L = (long)list[i] * mul;
+    if (L >= need && (!pow2 || (L & (L - 1)) == 0)) return (int)L;
   }
-
-#define CX_CONV_CASE_(N) \
-  case N:                \
-    return launch_rows<N>(a, st);
-CX_CONV_DISPATCH_(conv_dispatch_rows, launch_rows, m)
-#undef CX_CONV_CASE_
-#define CX_CONV_CASE_(N) \
-  case N:                \
-    return launch_cols<N>(a, st);
-CX_CONV_DISPATCH_(conv_dispatch_cols, launch_cols, p)
-#undef CX_CONV_CASE_
-#define CX_CONV_CASE_(N) \
-  case N:                \
-    return launch_fin_cols<N>(a, st);
-CX_CONV_DISPATCH_(conv_dispatch_fin_cols, launch_fin_cols, p)
-#undef CX_CONV_CASE_
-#define CX_CONV_CASE_(N) \
-  case N:                \
-    return launch_fin_rows<N>(a, st);
-CX_CONV_DISPATCH_(conv_dispatch_fin_rows, launch_fin_rows, m)
-#undef CX_CONV_CASE_
-
-static int next_pow2(long v) {
-  long p = 1;
-  while (p < v) p <<= 1;
-  return (int)p;
+  return 0;
 }
 
-// row-spectrum chunk budget (planes of both stacks per chunk)
-static constexpr size_t kConvChunkBytes = (size_t)256 << 20;
+// Row-spectrum chunk budget (zc planes of both stacks per chunk): large, so
+// that the column pass accumulates many planes in registers per St update;
+// its loads of the row spectra overlap the transforms.
+static constexpr size_t kConvChunkBytes = (size_t)1 << 30;
 
 static cx_status conv_plan(const cx_conv_desc* d, ConvArgs* a, int* zc, size_t* t_bytes, size_t* total) {
-  if (!d || d->n_planes <= 0 || d->h < 1 || d->w < 2) {
-    set_error("invalid convolution descriptor (n_planes >= 1, h >= 1, w >= 2)");
+  if (!d || d->n_planes <= 0 || d->h < 1 || d->w < 1) {
+    set_error("invalid convolution descriptor (n_planes >= 1, h >= 1, w >= 1)");
     return CX_ERR_INVALID;
   }
   a->h = d->h;
   a->w = d->w;
-  a->P = next_pow2(2L * d->h);
-  a->Q = next_pow2(2L * d->w);
-  a->M = a->Q / 2;
-  a->NC = a->M + 1;
-  if (a->P < 2 || a->P > 4096 || a->Q > 4096) {
-    set_error("convolution of %dx%d needs transforms of %dx%d; at most 4096 per axis", d->h, d->w, a->P, a->Q);
+  a->P = conv_len(kConvP, 1, 2L * d->h, d->pow2_lengths != 0);
+  a->Q = conv_len(kConvM, 2, 2L * d->w, d->pow2_lengths != 0);
+  if (a->P == 0 || a->Q == 0) {
+    set_error("convolution of %dx%d needs transforms longer than 4096 per axis", d->h, d->w);
     return CX_ERR_UNSUPPORTED;
   }
+  a->M = a->Q / 2;
+  a->NC = a->M + 1;
   a->c0y = (d->h - 1) / 2;
   a->c0x = (d->w - 1) / 2;
   a->scale = (float)(2.0 / ((double)a->P * (double)a->Q));

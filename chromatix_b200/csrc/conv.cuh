@@ -25,8 +25,32 @@
 
 namespace cx {
 
-// power-of-two transform lengths of the convolution (next_order of 2 h, 2 w)
-#define CX_CONV_SIZES(X) X(2) X(4) X(8) X(16) X(32) X(64) X(128) X(256) X(512) X(1024) X(2048) X(4096)
+// Transform lengths.  Any P >= h_a + h_b - 1 gives the same linear
+// convolution after the "same" crop (the reference's next power of two
+// included), so the column length P is the smallest even engine length
+// >= 2 h and the row length Q = 2 M the smallest >= 2 w whose half M is an
+// engine length; powers of two on request.
+#define CX_CONV_P_SIZES(X)                                                                                   \
+  X(2) X(4) X(6) X(8) X(10) X(12) X(14) X(16) X(20) X(24) X(28) X(32) X(40) X(48) X(56) X(64) X(80) X(96)    \
+  X(112) X(128) X(160) X(192) X(224) X(256) X(320) X(384) X(448) X(512) X(640) X(768) X(896) X(1024) X(1280) \
+  X(1536) X(1792) X(2048) X(2560) X(3072) X(3584) X(4096)
+#define CX_CONV_M_SIZES(X)                                                                                  \
+  X(2) X(3) X(4) X(5) X(6) X(7) X(8) X(10) X(12) X(14) X(16) X(20) X(24) X(28) X(32) X(40) X(48) X(56) X(64) \
+  X(80) X(96) X(112) X(128) X(160) X(192) X(224) X(256) X(320) X(384) X(448) X(512) X(640) X(768) X(896)    \
+  X(1024) X(1280) X(1536) X(1792) X(2048)
+
+// First-stage zero mask for an input that is nonzero only on [0, N / 2):
+// with an even first radix R_0 the inputs r >= R_0 / 2 of every first-stage
+// butterfly (indices j + r N / R_0 >= N / 2) are zero.  Odd first radices
+// (odd N) get no mask.
+template <int N>
+__host__ __device__ constexpr unsigned lower_half_mask() {
+  constexpr int R0 = Plan<N>::P.r[0];
+  unsigned m = 0u;
+  if (R0 % 2 == 0)
+    for (int r = R0 / 2; r < R0; ++r) m |= 1u << r;
+  return m;
+}
 
 struct ConvArgs {
   int h, w, P, Q, M, NC;  // image shape, transform lengths, M = Q / 2, NC = M + 1
@@ -54,10 +78,13 @@ __global__ void __launch_bounds__(RowCfg<M>::THREADS, RowCfg<M>::MINB) k_conv_ro
   load_twiddles<M>(tw, a.twg, threadIdx.x, blockDim.x);
   __syncthreads();
   constexpr int OFF_Q = tw_offset(QN);
+  static_assert(OFF_Q >= 0, "row length Q = 2 M has no twiddle table");
   const float2* wq = a.twg + OFF_Q;  // exp(-2 pi i k / Q), k < Q
   const int team = threadIdx.x / C::LPV, lane = threadIdx.x % C::LPV;
   float2* s = sm + C::TW + team * Plan<M>::LEN;
   const long total = (long)a.zc * 2 * a.h;
+  const bool even_w = (a.w % 2) == 0 &&
+                      ((reinterpret_cast<uintptr_t>(a.a) | reinterpret_cast<uintptr_t>(a.b)) & 7u) == 0;
   for (long base = (long)blockIdx.x * C::TEAMS; base < total; base += (long)gridDim.x * C::TEAMS) {
     const long item = base + team;
     if (item >= total) continue;
@@ -65,12 +92,15 @@ __global__ void __launch_bounds__(RowCfg<M>::THREADS, RowCfg<M>::MINB) k_conv_ro
     const int stack = (int)((item / a.h) % 2);
     const int zl = (int)(item / (2L * a.h));
     const float* xr = (stack == 0 ? a.a : a.b) + ((size_t)(a.z0 + zl) * a.h + y) * a.w;
+    // even w and 8-byte aligned stacks: aligned rows, one float2 load per pair
     auto load = [&](int n) -> float2 {
       const int x = 2 * n;
+      if (even_w) return x < a.w ? __ldg(reinterpret_cast<const float2*>(xr + x)) : make_float2(0.f, 0.f);
       return make_float2(x < a.w ? xr[x] : 0.f, x + 1 < a.w ? xr[x + 1] : 0.f);
     };
     auto sst = [&](int k, float2 v, int) { s[pad_idx(k)] = v; };
-    team_fft<M, false>(s, tw, lane, team, load, sst);
+    // z[n] = 0 for n >= ceil(w / 2), and Q >= 2 w puts that below M / 2
+    team_fft<M, false, C::LPV, false, lower_half_mask<M>()>(s, tw, lane, team, load, sst);
     team_sync<C::LPV>(team);
     float2* dst = a.T + (size_t)item * a.NC;
     for (int k = lane; k <= M; k += C::LPV) {
@@ -85,8 +115,14 @@ __global__ void __launch_bounds__(RowCfg<M>::THREADS, RowCfg<M>::MINB) k_conv_ro
 }
 
 // ---------------------------------------------------------------------------
-// columns: per NC-column tile, for each plane FFT_P(sample column) and
-// FFT_P(PSF column), products accumulated per lane, added into St
+// columns: work units (column tile of V spectrum columns, plane), split in
+// equal contiguous ranges over the CTAs (no last-wave tail).  Per unit:
+// FFT_P of the sample column and of the PSF column, product accumulated per
+// lane; the accumulators go to St (float2 atomicAdd) when the range leaves a
+// tile.  The next unit's columns are copied into a staging area with
+// cp.async while the current unit's transforms run (two copy groups, one
+// per stack, double-buffered against the transforms):
+//   wait A(u), FFT A(u), issue A(u+1) | wait B(u), FFT B(u) + acc, issue B(u+1)
 // ---------------------------------------------------------------------------
 template <int P>
 struct ConvColCfg {
@@ -94,82 +130,118 @@ struct ConvColCfg {
   static constexpr int LPV = C0::LPV;
   static constexpr bool CTA = C0::CTA;
   static constexpr int TW = tw_len(P);
+  static constexpr int HS = P / 2;  // staging rows per column (h <= P / 2)
+  // twiddles, two transform tiles, staging [stack][column][HS]
   static constexpr size_t smem_for(int v) {
-    return sizeof(float2) * ((size_t)TW + 2 * (size_t)v * col_len(P, v));
+    return sizeof(float2) * ((size_t)TW + 2 * (size_t)v * col_len(P, v) + 2 * (size_t)v * HS);
   }
   static constexpr int V0 = C0::V;
-  static constexpr int V = smem_for(V0) <= 200 * 1024 ? V0 : (smem_for(V0 / 2) <= 200 * 1024 ? V0 / 2 : V0 / 4);
+  // within 200 KB, and at most 384 threads so that the transform plus the
+  // per-lane accumulators (about 150 registers at P >= 1024) fit without
+  // spilling; exact-size teams keep whole warps
+  static constexpr int pick_v() {
+    int v = V0;
+    while (v > 1 && smem_for(v) > 200 * 1024) v /= 2;
+    while (v > 1 && v * LPV > 384 && (!CTA || ((v / 2) * LPV) % 32 == 0)) v /= 2;
+    return v;
+  }
+  static constexpr int V = pick_v();
   static_assert(V >= 1 && (!CTA || (V * LPV) % 32 == 0), "convolution column tile");
   static constexpr int LEN = col_len(P, V);
   static constexpr int THREADS = V * LPV;
   static constexpr int MINB = 1;
   static constexpr size_t SMEM = smem_for(V);
-  // rows >= h <= P / 2 are zero: the upper half of the first-stage inputs
-  static constexpr unsigned ZM = [] {
-    constexpr int R0 = Plan<P>::P.r[0];
-    unsigned m = 0u;
-    for (int r = R0 / 2; r < R0; ++r) m |= 1u << r;
-    return R0 >= 2 ? m : 0u;
-  }();
+  static_assert(SMEM <= 227 * 1024, "convolution column tile exceeds shared memory");
+  // rows >= h are zero and P >= 2 h
+  static constexpr unsigned ZM = lower_half_mask<P>();
 };
 
 template <int P>
 __global__ void __launch_bounds__(ConvColCfg<P>::THREADS, ConvColCfg<P>::MINB) k_conv_cols(ConvArgs a) {
   using Q = ConvColCfg<P>;
-  constexpr int V = Q::V, LEN = Q::LEN, LPV = Q::LPV;
-  constexpr int RL = Plan<P>::R_LAST, NBFL = P / RL, SLOTS = Plan<P>::OUT_SLOTS;
-  static_assert(SLOTS == ((NBFL + LPV - 1) / LPV) * RL, "slot layout");
+  constexpr int V = Q::V, LEN = Q::LEN, LPV = Q::LPV, HS = Q::HS;
+  // store slots of the last stage with this kernel's lane count:
+  // slot = it R_last + r for output j + r NBF_last, j = lane + it LPV
+  constexpr int RL = Plan<P>::R_LAST, NBFL = P / RL, SLOTS = ((NBFL + LPV - 1) / LPV) * RL;
   extern __shared__ float2 sm[];
   float2* tw = sm;
   float2* tA = sm + Q::TW;
   float2* tB = tA + V * LEN;
+  float2* stg = tB + V * LEN;  // [stack][V][HS]
   load_twiddles<P>(tw, a.twg, threadIdx.x, blockDim.x);
   const int team = threadIdx.x / LPV, lane = threadIdx.x % LPV;
   float2* sA = tA + team * LEN;
   float2* sB = tB + team * LEN;
-  const int tiles = (a.NC + V - 1) / V;
-  for (int t = blockIdx.x; t < tiles; t += gridDim.x) {
-    const int kc0 = t * V;
-    float2 acc[SLOTS];
-#pragma unroll
-    for (int i = 0; i < SLOTS; ++i) acc[i] = make_float2(0.f, 0.f);
-    for (int zl = 0; zl < a.zc; ++zl) {
-      __syncthreads();
-      const float2* TA = a.T + (size_t)(2 * zl) * a.h * a.NC;
-      load_col_tile<V, LEN>(tA, TA, a.NC, kc0, a.NC, 0, a.h, [](int r) { return r; });
-      load_col_tile<V, LEN>(tB, TA + (size_t)a.h * a.NC, a.NC, kc0, a.NC, 0, a.h, [](int r) { return r; });
-      __syncthreads();
-      auto ldA = [&](int n) -> float2 { return n < a.h ? sA[pad_idx(n)] : make_float2(0.f, 0.f); };
-      auto stA = [&](int k, float2 v, int) { sA[pad_idx(k)] = v; };
-      team_fft<P, false, LPV, Q::CTA, Q::ZM>(sA, tw, lane, team, ldA, stA);
-      team_barrier<LPV, Q::CTA>(team);
-      auto ldB = [&](int n) -> float2 { return n < a.h ? sB[pad_idx(n)] : make_float2(0.f, 0.f); };
-      auto stAcc = [&](int k, float2 v, int slot) { acc[slot] = cadd(acc[slot], cmul(sA[pad_idx(k)], v)); };
-      team_fft<P, false, LPV, Q::CTA, Q::ZM>(sB, tw, lane, team, ldB, stAcc);
+  const float2* gA = stg + team * HS;
+  const float2* gB = stg + (V + team) * HS;
+  const long zc = a.zc;
+  const long units = (long)((a.NC + V - 1) / V) * zc;
+  const long u0 = units * blockIdx.x / gridDim.x, u1 = units * (blockIdx.x + 1) / gridDim.x;
+  if (u0 >= u1) return;  // whole CTA, before any barrier
+  // copy the stack's V columns of unit u into the staging area (columns
+  // past NC are not loaded: their transforms are computed and discarded)
+  auto prefetch = [&](long u, int stack) {
+    const int kc0 = (int)(u / zc) * V, zl = (int)(u % zc);
+    const float2* src = a.T + (size_t)(2 * zl + stack) * a.h * a.NC + kc0;
+    float2* dst = stg + stack * V * HS;
+    const int n = a.h * V;
+    for (int i = threadIdx.x; i < n; i += blockDim.x) {
+      const int y = i / V, c = i % V;
+      if (kc0 + c < a.NC) cp_async8(dst + c * HS + y, src + (size_t)y * a.NC + c);
     }
-    // St[kc][k] += acc: the slot of output k = j + r NBF_last, j = lane + it LPV
-    const int kc = kc0 + team;
-    if (kc < a.NC) {
-      float2* col = a.St + (size_t)kc * a.P;
+  };
+  float2 acc[SLOTS];
 #pragma unroll
-      for (int slot = 0; slot < SLOTS; ++slot) {
-        const int it = slot / RL, r = slot % RL;
-        const int j = lane + it * LPV;
-        if (j < NBFL) {
-          const int k = j + r * NBFL;
-          col[k] = cadd(col[k], acc[slot]);
+  for (int i = 0; i < SLOTS; ++i) acc[i] = make_float2(0.f, 0.f);
+  prefetch(u0, 0);
+  cp_async_commit();
+  prefetch(u0, 1);
+  cp_async_commit();
+  for (long u = u0; u < u1; ++u) {
+    const int t = (int)(u / zc);
+    cp_async_wait_group<1>();  // A(u) (B(u) may be in flight)
+    __syncthreads();
+    auto ldA = [&](int n) -> float2 { return n < a.h ? gA[n] : make_float2(0.f, 0.f); };
+    auto stA = [&](int k, float2 v, int) { sA[pad_idx(k)] = v; };
+    team_fft<P, false, LPV, Q::CTA, Q::ZM>(sA, tw, lane, team, ldA, stA);
+    __syncthreads();  // every team is past its reads of the A staging
+    if (u + 1 < u1) prefetch(u + 1, 0);
+    cp_async_commit();
+    cp_async_wait_group<1>();  // B(u)
+    __syncthreads();
+    auto ldB = [&](int n) -> float2 { return n < a.h ? gB[n] : make_float2(0.f, 0.f); };
+    auto stAcc = [&](int k, float2 v, int slot) { acc[slot] = cadd(acc[slot], cmul(sA[pad_idx(k)], v)); };
+    team_fft<P, false, LPV, Q::CTA, Q::ZM>(sB, tw, lane, team, ldB, stAcc);
+    __syncthreads();  // B staging and the A tile are free
+    if (u + 1 < u1) prefetch(u + 1, 1);
+    cp_async_commit();
+    if (u + 1 == u1 || (u + 1) / zc != t) {
+      // St[kc][k] += acc for output k = j + r NBF_last of slot it R_last + r
+      const int kc = t * V + team;
+      if (kc < a.NC) {
+        float2* col = a.St + (size_t)kc * a.P;
+#pragma unroll
+        for (int slot = 0; slot < SLOTS; ++slot) {
+          const int it = slot / RL, r = slot % RL;
+          const int j = lane + it * LPV;
+          if (j < NBFL) atomicAdd(col + j + r * NBFL, acc[slot]);
         }
       }
+#pragma unroll
+      for (int i = 0; i < SLOTS; ++i) acc[i] = make_float2(0.f, 0.f);
     }
   }
+  cp_async_wait_all();
 }
 
 // ---------------------------------------------------------------------------
 // final, columns: inverse FFT_P of each spectrum column (contiguous in St),
 // only the crop rows written, transposed into U (NC, h)
 // ---------------------------------------------------------------------------
+// no blocks-per-SM bound: the long transforms' unrolled stores need up to
+// about 170 registers
 template <int P>
-__global__ void __launch_bounds__(RowCfg<P>::THREADS, RowCfg<P>::MINB) k_conv_fin_cols(ConvArgs a) {
+__global__ void __launch_bounds__(RowCfg<P>::THREADS, 1) k_conv_fin_cols(ConvArgs a) {
   using C = RowCfg<P>;
   extern __shared__ float2 sm[];
   float2* tw = sm;
@@ -206,6 +278,7 @@ struct ConvFinCfg {
   static constexpr int THREADS = V * LPV;
   static constexpr int MINB = minb_for(THREADS);
   static constexpr size_t SMEM = sizeof(float2) * ((size_t)TW + (size_t)V * LEN);
+  static_assert(SMEM <= 227 * 1024, "convolution row tile exceeds shared memory");
 };
 
 template <int M>
@@ -218,6 +291,7 @@ __global__ void __launch_bounds__(ConvFinCfg<M>::THREADS, ConvFinCfg<M>::MINB) k
   float2* tile = sm + Q::TW;
   load_twiddles<M>(tw, a.twg, threadIdx.x, blockDim.x);
   constexpr int OFF_Q = tw_offset(QN);
+  static_assert(OFF_Q >= 0, "row length Q = 2 M has no twiddle table");
   const float2* wq = a.twg + OFF_Q;  // exp(-2 pi i k / Q)
   const int team = threadIdx.x / LPV, lane = threadIdx.x % LPV;
   float2* s = tile + team * LEN;

@@ -1,12 +1,17 @@
 """``fourier_convolution`` (ops/ops.py:9-86) on the GPU.
 
 Real inputs of equal shape convolved plane by plane over their last two axes
-(``axes=(-2, -1)``), mode "same", transforms padded to the next power of two
-of the summed shape (``fast_fft_shape=True``) -- the configuration the
-``Microscope`` uses -- run as one native call (``cx_conv2d_same``): r2c
-row passes, column passes with the product accumulated per plane, and the
-c2r back, all fused.  ``reduce=True`` also sums over the leading plane axis
+(``axes=(-2, -1)``), mode "same" -- the configuration the ``Microscope``
+uses -- run as one native call (``cx_conv2d_same``): r2c row passes, column
+passes with the product accumulated per plane, and the c2r back, all fused.
+``reduce=True`` also sums over the leading plane axis
 (``BasicSensor(reduce_axis=0)``) inside the same call.
+
+Transform lengths: the reference pads to the next power of two of the summed
+shape (``fast_fft_shape=True``) or to the summed shape itself; every length
+>= 2 n - 1 gives the same linear convolution after the crop, so both settings
+run at the smallest engine lengths >= 2 n (1536 -> 3072 instead of 4096).
+``lengths="pow2"`` keeps the reference's power-of-two lengths.
 """
 
 from __future__ import annotations
@@ -17,7 +22,7 @@ from .. import _native as nat
 
 
 class cx_conv_desc(nat.ctypes.Structure):
-    _fields_ = [(k, nat.c_int32) for k in ("n_planes", "h", "w", "reduce")]
+    _fields_ = [(k, nat.c_int32) for k in ("n_planes", "h", "w", "reduce", "pow2_lengths")]
 
 
 def _lib():
@@ -34,16 +39,19 @@ def _lib():
 
 
 def fourier_convolution(image, kernel, *, axes=(-2, -1), fast_fft_shape: bool = True, mode: str = "same",
-                        reduce: bool = False):
+                        reduce: bool = False, lengths: str = "smallest"):
     """Convolution ``kernel * image`` over the last two axes by the Fourier
     convolution theorem (ops/ops.py:9-86); ``reduce`` sums the result over
-    all leading axes."""
+    all leading axes.  ``lengths``: "smallest" (smallest engine lengths
+    >= 2 n) or "pow2" (next powers of two); the result is the same."""
     torch = nat.torch_mod()
     ax = tuple(a % image.ndim for a in axes)
     if ax != (image.ndim - 2, image.ndim - 1):
         raise NotImplementedError("convolution over the last two axes only")
-    if not fast_fft_shape or mode != "same":
-        raise NotImplementedError("fast_fft_shape=True and mode='same' only")
+    if mode != "same":
+        raise NotImplementedError("mode='same' only")
+    if lengths not in ("smallest", "pow2"):
+        raise ValueError(f"lengths must be 'smallest' or 'pow2', got {lengths!r}")
     if image.ndim != kernel.ndim:
         raise AssertionError(f"Input ({image.ndim}D) and kernel ({kernel.ndim}D) must have same number of dimensions")
     if tuple(image.shape) != tuple(kernel.shape):
@@ -56,7 +64,7 @@ def fourier_convolution(image, kernel, *, axes=(-2, -1), fast_fft_shape: bool = 
     h, w = a.shape[-2:]
     lead = tuple(a.shape[:-2])
     planes = int(np.prod(lead)) if lead else 1
-    d = cx_conv_desc(n_planes=planes, h=h, w=w, reduce=1 if reduce else 0)
+    d = cx_conv_desc(n_planes=planes, h=h, w=w, reduce=1 if reduce else 0, pow2_lengths=1 if lengths == "pow2" else 0)
     L = _lib()
     wsb = nat.c_size_t(0)
     nat.check(L.cx_conv2d_workspace_size(d, wsb))

@@ -85,7 +85,8 @@ class BasicSensor:
 
     def __call__(self, sensor_input, input_spacing=None, resample: bool = True, key=None):
         torch = nat.torch_mod()
-        image = sensor_input.intensity if hasattr(sensor_input, "intensity") else sensor_input
+        # a field's intensity is a computed property: read it once
+        image = sensor_input if isinstance(sensor_input, torch.Tensor) else sensor_input.intensity
         if self.reduce_axis is not None:
             image = torch.sum(image, dim=self.reduce_axis)
         return self._parallel_sum(image)
@@ -96,7 +97,8 @@ class Microscope:
     (systems/microscopes.py:16-297)."""
 
     def __init__(self, system_psf: Callable, sensor: BasicSensor, f, n, NA, spectrum, padding_ratio=0,
-                 taper_width=0, convolution_axes=(-2, -1), fast_fft_shape: bool = True, *, device="cuda"):
+                 taper_width=0, convolution_axes=(-2, -1), fast_fft_shape: bool = True, *, device="cuda",
+                 fft_lengths: str = "smallest"):
         if taper_width:
             raise NotImplementedError("taper_width > 0 is not part of this build")
         self.system_psf = system_psf
@@ -108,13 +110,18 @@ class Microscope:
         self.convolution_axes = tuple(convolution_axes)
         self.fast_fft_shape = fast_fft_shape
         self.device = device
+        # "smallest" engine lengths >= 2 n or "pow2" (the reference's
+        # fast_fft_shape lengths): the same image either way
+        self.fft_lengths = fft_lengths
 
     def psf(self, *args: Any, **kwargs: Any):
         return self.system_psf(self, *args, **kwargs)
 
     def __call__(self, sample, *args: Any, key=None, **kwargs: Any):
+        torch = nat.torch_mod()
         system_psf = self.psf(*args, **kwargs)
-        psf = system_psf.intensity if hasattr(system_psf, "intensity") else system_psf
+        # the PSF field's intensity runs the fused PSF pipeline: evaluate it once
+        psf = system_psf if isinstance(system_psf, torch.Tensor) else system_psf.intensity
         return self.image(sample, psf, key=key)
 
     def image(self, sample, psf, key=None):
@@ -129,7 +136,8 @@ class Microscope:
                  and s.resampling_method is None)
         if fused:
             image = fourier_convolution(sample, psf, axes=self.convolution_axes,
-                                        fast_fft_shape=self.fast_fft_shape, reduce=True)
+                                        fast_fft_shape=self.fast_fft_shape, reduce=True, lengths=self.fft_lengths)
             return s._parallel_sum(image)
-        image = fourier_convolution(sample, psf, axes=self.convolution_axes, fast_fft_shape=self.fast_fft_shape)
+        image = fourier_convolution(sample, psf, axes=self.convolution_axes, fast_fft_shape=self.fast_fft_shape,
+                                    lengths=self.fft_lengths)
         return s(image, s.spacing, resample=False, key=key)

@@ -343,12 +343,16 @@ cx_status cx_czt_propagate(const cx_czt_prop_desc* d, const void* u_in, void* u_
  * mode "same", fast_fft_shape) of a sample stack with a PSF stack, plane by
  * plane, and the sensor's sum over the planes (functional/sensors.py:85-86,
  * systems/microscopes.py:271-297).  sample, psf: (n_planes, h, w) float32;
- * out: (h, w) float32 if reduce, else (n_planes, h, w).  Transform size
- * (next power of two of 2h, of 2w), at most 4096 per axis (w >= 2).
+ * out: (h, w) float32 if reduce, else (n_planes, h, w).  Any transform
+ * size >= 2h - 1 by 2w - 1 gives the same linear convolution after the
+ * crop: the smallest supported lengths >= 2h, 2w are used (even, 2..4096
+ * per axis), or the next powers of two (the reference's fast_fft_shape
+ * lengths) with pow2_lengths = 1.
  * ------------------------------------------------------------------------- */
 typedef struct {
   int32_t n_planes, h, w;
-  int32_t reduce; /* 1: sum over the planes (BasicSensor(reduce_axis=0)) */
+  int32_t reduce;       /* 1: sum over the planes (BasicSensor(reduce_axis=0)) */
+  int32_t pow2_lengths; /* 1: transform lengths are powers of two */
 } cx_conv_desc;
 
 cx_status cx_conv2d_workspace_size(const cx_conv_desc* d, size_t* bytes);

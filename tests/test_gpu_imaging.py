@@ -11,8 +11,16 @@ from tests.helpers import rel, to_np
 pytestmark = pytest.mark.gpu
 
 
-@pytest.mark.parametrize("shape", [(3, 40, 56), (2, 37, 29), (1, 64, 64), (4, 5, 2), (2, 96, 130)])
-def test_fourier_convolution_matches_oracle(shape):
+# shapes cover power-of-two and 3/5/7-smooth transform lengths, odd half row
+# lengths (w = 5, 7: M = 5, 7, no first-stage zero mask), single rows and
+# columns
+SHAPES = [(3, 40, 56), (2, 37, 29), (1, 64, 64), (4, 5, 2), (2, 96, 130), (2, 9, 7), (3, 6, 5), (2, 1, 1),
+          (3, 1, 7), (2, 7, 1), (1, 100, 140), (2, 700, 300), (1, 190, 1800)]
+
+
+@pytest.mark.parametrize("lengths", ["smallest", "pow2"])
+@pytest.mark.parametrize("shape", SHAPES)
+def test_fourier_convolution_matches_oracle(shape, lengths):
     import torch
 
     from chromatix_b200.ops import fourier_convolution
@@ -22,11 +30,34 @@ def test_fourier_convolution_matches_oracle(shape):
     k = rng.uniform(0, 1, shape).astype(np.float32)
     ad, kd = torch.as_tensor(a, device="cuda"), torch.as_tensor(k, device="cuda")
     ref = O.fourier_convolution(a.astype(np.float64), k.astype(np.float64), axes=(-2, -1))
-    out = fourier_convolution(ad, kd)
+    out = fourier_convolution(ad, kd, lengths=lengths)
     assert tuple(out.shape) == shape
     assert rel(to_np(out), ref) < 1e-5
-    red = fourier_convolution(ad, kd, reduce=True)
+    red = fourier_convolution(ad, kd, reduce=True, lengths=lengths)
     assert rel(to_np(red), ref.sum(0)) < 1e-5
+
+
+def test_fourier_convolution_published_plane_size():
+    """1536^2 planes (the reference's imaging benchmark): 3072-point
+    transforms against the FP64 oracle's 4096-point ones, and the plane sum
+    of 24 planes (more than one row-spectrum chunk) against the per-plane
+    images summed in FP64."""
+    import torch
+
+    from chromatix_b200.ops import fourier_convolution
+
+    rng = np.random.default_rng(1536)
+    shape = (24, 1536, 1536)
+    a = torch.rand(shape, device="cuda", generator=torch.Generator("cuda").manual_seed(1))
+    k = torch.rand(shape, device="cuda", generator=torch.Generator("cuda").manual_seed(2))
+    per = fourier_convolution(a, k)
+    red = fourier_convolution(a, k, reduce=True)
+    assert rel(to_np(red), to_np(per).astype(np.float64).sum(0)) < 1e-5
+    for i in rng.choice(24, 2, replace=False):
+        ref = O.fourier_convolution(to_np(a[i]).astype(np.float64), to_np(k[i]).astype(np.float64), axes=(-2, -1))
+        assert rel(to_np(per[i]), ref) < 1e-5
+    pow2 = fourier_convolution(a[:3], k[:3], reduce=True, lengths="pow2")
+    assert rel(to_np(pow2), to_np(per[:3]).astype(np.float64).sum(0)) < 1e-5
 
 
 def test_fourier_convolution_rejects_unsupported_forms():
@@ -41,6 +72,11 @@ def test_fourier_convolution_rejects_unsupported_forms():
         fourier_convolution(a, a, mode="full")
     with pytest.raises(NotImplementedError):
         fourier_convolution(a.to(torch.complex64), a.to(torch.complex64))
+    with pytest.raises(ValueError):
+        fourier_convolution(a, a, lengths="exact")
+    big = torch.zeros((1, 2049, 8), device="cuda")
+    with pytest.raises(Exception, match="longer than 4096"):
+        fourier_convolution(big, big)
 
 
 def test_microscope_image_matches_oracle():

@@ -22,3 +22,33 @@ def test_basic_sensor_reduce_and_next_order():
     x = np.arange(24.0).reshape(2, 3, 4)
     np.testing.assert_array_equal(O.basic_sensor_reduce(x, 0), x.sum(0))
     assert O.next_order(3072) == 4096 and O.next_order(4096) == 4096 and O.next_order(3) == 4
+
+
+def test_microscope_reads_the_psf_intensity_once():
+    """Microscope.__call__ (systems/microscopes.py:232-269) evaluates the PSF
+    field's intensity -- the whole PSF pipeline -- exactly once per image."""
+    import torch
+
+    from chromatix_b200.systems import BasicSensor, Microscope
+
+    class CountingField:
+        reads = 0
+
+        @property
+        def intensity(self):
+            CountingField.reads += 1
+            return torch.ones((4, 8, 8))
+
+    class HostMicroscope(Microscope):
+        def image(self, sample, psf, key=None):  # the convolution itself runs on the GPU only
+            return psf.sum(0)
+
+    scope = HostMicroscope(lambda microscope, *a: CountingField(),
+                           BasicSensor((8, 8), 0.3, resampling_method=None, reduce_axis=0), 100.0, 1.33, 0.8, 0.532)
+    out = scope(torch.zeros((4, 8, 8)), np.linspace(-1, 1, 4))
+    assert CountingField.reads == 1
+    assert tuple(out.shape) == (8, 8)
+    # the sensor reads a field's intensity once too
+    CountingField.reads = 0
+    assert tuple(BasicSensor((8, 8), 0.3, resampling_method=None, reduce_axis=0)(CountingField()).shape) == (8, 8)
+    assert CountingField.reads == 1
