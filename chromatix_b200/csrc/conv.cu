@@ -26,24 +26,45 @@ static int conv_len(const int (&list)[K], int mul, long need, bool pow2) {
 static constexpr size_t kConvChunkBytes = (size_t)1 << 30;
 
 static cx_status conv_plan(const cx_conv_desc* d, ConvArgs* a, int* zc, size_t* t_bytes, size_t* total) {
-  if (!d || d->n_planes <= 0 || d->h < 1 || d->w < 1) {
-    set_error("invalid convolution descriptor (n_planes >= 1, h >= 1, w >= 1)");
+  if (!d || d->n_planes <= 0 || d->h < 1 || d->w < 1 || d->kh < 1 || d->kw < 1) {
+    set_error("invalid convolution descriptor (n_planes, h, w, kh, kw >= 1)");
     return CX_ERR_INVALID;
   }
   a->h = d->h;
   a->w = d->w;
-  a->P = conv_len(kConvP, 1, 2L * d->h, d->pow2_lengths != 0);
-  a->Q = conv_len(kConvM, 2, 2L * d->w, d->pow2_lengths != 0);
+  a->kh = d->kh;
+  a->kw = d->kw;
+  const int H = d->h > d->kh ? d->h : d->kh;
+  a->HB = H;
+
+  const int W = d->w > d->kw ? d->w : d->kw;
+  // >= h + kh - 1 (linear convolution) and >= 2 max(h, kh): the inputs then
+  // fill at most the first half of every transform (first-stage zero masks)
+  a->P = conv_len(kConvP, 1, 2L * H, d->pow2_lengths != 0);
+  a->Q = conv_len(kConvM, 2, 2L * W, d->pow2_lengths != 0);
   if (a->P == 0 || a->Q == 0) {
-    set_error("convolution of %dx%d needs transforms longer than 4096 per axis", d->h, d->w);
+    set_error("convolution of %dx%d with %dx%d needs transforms longer than 4096 per axis", d->h, d->w, d->kh,
+              d->kw);
     return CX_ERR_UNSUPPORTED;
   }
   a->M = a->Q / 2;
   a->NC = a->M + 1;
-  a->c0y = (d->h - 1) / 2;
-  a->c0x = (d->w - 1) / 2;
+  // T tiles: the column pass's width V (a power of two), at least 4 columns
+  // so that a row's run in a tile fills a 32-byte sector
+  const int cv = conv_col_tile(a->P);
+  if (cv < 1 || (cv & (cv - 1)) != 0) {
+    set_error("internal: column tile width %d for length %d", cv, a->P);
+    return CX_ERR_UNSUPPORTED;
+  }
+  const int vt = cv > 4 ? cv : 4;
+  a->vt_shift = 0;
+  while ((1 << a->vt_shift) < vt) ++a->vt_shift;
+  a->NT = (a->NC + vt - 1) / vt;
+  a->b_plane = d->kernel_broadcast ? 0 : (long)d->kh * d->kw;
+  a->c0y = (d->kh - 1) / 2;
+  a->c0x = (d->kw - 1) / 2;
   a->scale = (float)(2.0 / ((double)a->P * (double)a->Q));
-  const size_t plane_t = sizeof(float2) * 2 * (size_t)d->h * a->NC;
+  const size_t plane_t = sizeof(float2) * 2 * (size_t)a->HB * a->NT * vt;
   int c = (int)(kConvChunkBytes / plane_t);
   if (c < 1) c = 1;
   if (c > d->n_planes) c = d->n_planes;
@@ -70,14 +91,14 @@ extern "C" cx_status cx_conv2d_workspace_size(const cx_conv_desc* d, size_t* byt
   return CX_OK;
 }
 
-extern "C" cx_status cx_conv2d_same(const cx_conv_desc* d, const float* sample, const float* psf, float* out,
+extern "C" cx_status cx_conv2d_same(const cx_conv_desc* d, const float* sample, const float* kernel, float* out,
                                     void* workspace, size_t workspace_bytes, cx_stream_t stream) {
   ConvArgs a;
   int zc = 0;
   size_t tb = 0, total = 0;
   cx_status s = conv_plan(d, &a, &zc, &tb, &total);
   if (s != CX_OK) return s;
-  if (!sample || !psf || !out || !workspace) {
+  if (!sample || !kernel || !out || !workspace) {
     set_error("null pointer argument");
     return CX_ERR_INVALID;
   }
@@ -92,7 +113,7 @@ extern "C" cx_status cx_conv2d_same(const cx_conv_desc* d, const float* sample, 
   a.St = reinterpret_cast<float2*>(ws + tb);
   a.U = reinterpret_cast<float2*>(ws + tb + (((sizeof(float2) * (size_t)a.NC * a.P) + 255) & ~(size_t)255));
   a.a = sample;
-  a.b = psf;
+  a.b = kernel;
   const size_t st_bytes = sizeof(float2) * (size_t)a.NC * a.P;
   const size_t img = (size_t)d->h * d->w;
   // reduce: one accumulated spectrum for all planes; otherwise one per plane

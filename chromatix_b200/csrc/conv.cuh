@@ -53,21 +53,30 @@ __host__ __device__ constexpr unsigned lower_half_mask() {
 }
 
 struct ConvArgs {
-  int h, w, P, Q, M, NC;  // image shape, transform lengths, M = Q / 2, NC = M + 1
+  int h, w;               // image (sample) plane shape = output shape
+  int kh, kw;             // kernel (PSF) plane shape
+  int HB;                 // rows per tile block of T: max(h, kh)
+  int NT, vt_shift;       // column tiles of T and their width VT = 1 << vt_shift (>= 4, a multiple of the column pass's V)
+  int P, Q, M, NC;        // transform lengths, M = Q / 2, NC = M + 1
   int z0, zc;             // plane chunk
   const float* a;         // sample (n_planes, h, w)
-  const float* b;         // PSF (n_planes, h, w)
-  float2* T;              // row spectra (zc, 2, h, NC)
+  const float* b;         // kernel (n_planes, kh, kw), or one (kh, kw) plane
+  long b_plane;           // kernel plane stride in floats (0: one kernel for all planes)
+  float2* T;              // row spectra by column tile (zc, 2, NT, HB, VT): stack 0 rows < h, stack 1 rows < kh
   float2* St;             // accumulated spectrum, transposed (NC, P)
   float2* U;              // column inverse of the crop rows, transposed (NC, h)
   float* out;             // image (h, w)
-  int c0y, c0x;           // "same" crop offsets
+  int c0y, c0x;           // "same" crop offsets ((kh - 1) / 2, (kw - 1) / 2)
   float scale;            // 2 / (P Q)
   const float2* twg;
 };
 
 // ---------------------------------------------------------------------------
-// rows: r2c of the zc planes of both stacks (items: plane, stack, row)
+// rows: r2c of the zc planes of both stacks (items: plane, stack, row).  T is
+// stored by column tile, (zc, 2, NT, HB, VT) with VT = max(4, the column
+// pass's tile width): a row's run in a tile is >= 32 bytes, so every lane
+// group writes whole sectors (partial sectors make the L2 read them back
+// from DRAM) and the column pass copies its columns from one block.
 // ---------------------------------------------------------------------------
 template <int M>
 __global__ void __launch_bounds__(RowCfg<M>::THREADS, RowCfg<M>::MINB) k_conv_rows(ConvArgs a) {
@@ -82,34 +91,39 @@ __global__ void __launch_bounds__(RowCfg<M>::THREADS, RowCfg<M>::MINB) k_conv_ro
   const float2* wq = a.twg + OFF_Q;  // exp(-2 pi i k / Q), k < Q
   const int team = threadIdx.x / C::LPV, lane = threadIdx.x % C::LPV;
   float2* s = sm + C::TW + team * Plan<M>::LEN;
-  const long total = (long)a.zc * 2 * a.h;
-  const bool even_w = (a.w % 2) == 0 &&
-                      ((reinterpret_cast<uintptr_t>(a.a) | reinterpret_cast<uintptr_t>(a.b)) & 7u) == 0;
+  const int vs = a.vt_shift, vm = (1 << a.vt_shift) - 1;
+  const size_t tile_stride = (size_t)a.HB << vs;
+  // items: (plane, stack, row), h sample rows then kh kernel rows per plane
+  const int rows = a.h + a.kh;
+  const long total = (long)a.zc * rows;
   for (long base = (long)blockIdx.x * C::TEAMS; base < total; base += (long)gridDim.x * C::TEAMS) {
     const long item = base + team;
     if (item >= total) continue;
-    const int y = (int)(item % a.h);
-    const int stack = (int)((item / a.h) % 2);
-    const int zl = (int)(item / (2L * a.h));
-    const float* xr = (stack == 0 ? a.a : a.b) + ((size_t)(a.z0 + zl) * a.h + y) * a.w;
-    // even w and 8-byte aligned stacks: aligned rows, one float2 load per pair
+    const int zl = (int)(item / rows), r = (int)(item % rows);
+    const int stack = r < a.h ? 0 : 1;
+    const int y = stack == 0 ? r : r - a.h;
+    const int w = stack == 0 ? a.w : a.kw;
+    const float* xr = stack == 0 ? a.a + ((size_t)(a.z0 + zl) * a.h + y) * a.w
+                                 : a.b + (size_t)(a.z0 + zl) * a.b_plane + (size_t)y * a.kw;
+    // even width on an 8-byte boundary: one float2 load per input pair
+    const bool pairs = (w % 2) == 0 && (reinterpret_cast<uintptr_t>(xr) & 7u) == 0;
     auto load = [&](int n) -> float2 {
       const int x = 2 * n;
-      if (even_w) return x < a.w ? __ldg(reinterpret_cast<const float2*>(xr + x)) : make_float2(0.f, 0.f);
-      return make_float2(x < a.w ? xr[x] : 0.f, x + 1 < a.w ? xr[x + 1] : 0.f);
+      if (pairs) return x < w ? __ldg(reinterpret_cast<const float2*>(xr + x)) : make_float2(0.f, 0.f);
+      return make_float2(x < w ? xr[x] : 0.f, x + 1 < w ? xr[x + 1] : 0.f);
     };
     auto sst = [&](int k, float2 v, int) { s[pad_idx(k)] = v; };
-    // z[n] = 0 for n >= ceil(w / 2), and Q >= 2 w puts that below M / 2
+    // z[n] = 0 for n >= ceil(w / 2), and Q >= 2 max(w, kw) puts that below M / 2
     team_fft<M, false, C::LPV, false, lower_half_mask<M>()>(s, tw, lane, team, load, sst);
     team_sync<C::LPV>(team);
-    float2* dst = a.T + (size_t)item * a.NC;
+    float2* dst = a.T + (size_t)(2 * zl + stack) * a.NT * tile_stride + ((size_t)y << vs);
     for (int k = lane; k <= M; k += C::LPV) {
       const float2 zk = s[pad_idx(k == M ? 0 : k)];
       const float2 zm = cconj(s[pad_idx(k == 0 ? 0 : M - k)]);
       const float2 e = cscale(cadd(zk, zm), 0.5f);
       const float2 d = csub(zk, zm);
       const float2 o = make_float2(0.5f * d.y, -0.5f * d.x);  // (zk - zm) / (2i)
-      dst[k] = cadd(e, cmul(wq[k], o));
+      dst[(size_t)(k >> vs) * tile_stride + (k & vm)] = cadd(e, cmul(wq[k], o));
     }
   }
 }
@@ -130,11 +144,10 @@ struct ConvColCfg {
   static constexpr int LPV = C0::LPV;
   static constexpr bool CTA = C0::CTA;
   static constexpr int TW = tw_len(P);
-  static constexpr int HS = P / 2;  // staging rows per column (h <= P / 2)
-  // twiddles, two transform tiles, staging [stack][column][HS]
-  static constexpr size_t smem_for(int v) {
-    return sizeof(float2) * ((size_t)TW + 2 * (size_t)v * col_len(P, v) + 2 * (size_t)v * HS);
-  }
+  static constexpr int HS = P / 2;  // staging rows per column (h, kh <= P / 2)
+  // twiddles | two transform tiles | staging [stack][column][HS]
+  static constexpr int stg_off(int v) { return TW + 2 * v * col_len(P, v); }
+  static constexpr size_t smem_for(int v) { return sizeof(float2) * ((size_t)stg_off(v) + 2 * (size_t)v * HS); }
   static constexpr int V0 = C0::V;
   // within 200 KB, and at most 384 threads so that the transform plus the
   // per-lane accumulators (about 150 registers at P >= 1024) fit without
@@ -152,7 +165,7 @@ struct ConvColCfg {
   static constexpr int MINB = 1;
   static constexpr size_t SMEM = smem_for(V);
   static_assert(SMEM <= 227 * 1024, "convolution column tile exceeds shared memory");
-  // rows >= h are zero and P >= 2 h
+  // rows >= h (kh) are zero and P >= 2 max(h, kh)
   static constexpr unsigned ZM = lower_half_mask<P>();
 };
 
@@ -167,7 +180,7 @@ __global__ void __launch_bounds__(ConvColCfg<P>::THREADS, ConvColCfg<P>::MINB) k
   float2* tw = sm;
   float2* tA = sm + Q::TW;
   float2* tB = tA + V * LEN;
-  float2* stg = tB + V * LEN;  // [stack][V][HS]
+  float2* stg = sm + Q::stg_off(V);  // [stack][V][HS]
   load_twiddles<P>(tw, a.twg, threadIdx.x, blockDim.x);
   const int team = threadIdx.x / LPV, lane = threadIdx.x % LPV;
   float2* sA = tA + team * LEN;
@@ -178,16 +191,20 @@ __global__ void __launch_bounds__(ConvColCfg<P>::THREADS, ConvColCfg<P>::MINB) k
   const long units = (long)((a.NC + V - 1) / V) * zc;
   const long u0 = units * blockIdx.x / gridDim.x, u1 = units * (blockIdx.x + 1) / gridDim.x;
   if (u0 >= u1) return;  // whole CTA, before any barrier
-  // copy the stack's V columns of unit u into the staging area (columns
-  // past NC are not loaded: their transforms are computed and discarded)
+  // copy the stack's V columns of unit u (V of the VT columns of one T tile
+  // block) into the staging area, one run per column; the columns past NC
+  // of the last tile are never written by the row pass: their transforms
+  // are computed and discarded
+  const int vts = a.vt_shift;
   auto prefetch = [&](long u, int stack) {
-    const int kc0 = (int)(u / zc) * V, zl = (int)(u % zc);
-    const float2* src = a.T + (size_t)(2 * zl + stack) * a.h * a.NC + kc0;
+    const int c0 = (int)(u / zc) * V, zl = (int)(u % zc);
+    const float2* src = a.T + (((size_t)(2 * zl + stack) * a.NT + (c0 >> vts)) * a.HB << vts) +
+                        (c0 & ((1 << vts) - 1));
     float2* dst = stg + stack * V * HS;
-    const int n = a.h * V;
+    const int n = (stack == 0 ? a.h : a.kh) * V;
     for (int i = threadIdx.x; i < n; i += blockDim.x) {
       const int y = i / V, c = i % V;
-      if (kc0 + c < a.NC) cp_async8(dst + c * HS + y, src + (size_t)y * a.NC + c);
+      cp_async8(dst + c * HS + y, src + ((size_t)y << vts) + c);
     }
   };
   float2 acc[SLOTS];
@@ -209,7 +226,7 @@ __global__ void __launch_bounds__(ConvColCfg<P>::THREADS, ConvColCfg<P>::MINB) k
     cp_async_commit();
     cp_async_wait_group<1>();  // B(u)
     __syncthreads();
-    auto ldB = [&](int n) -> float2 { return n < a.h ? gB[n] : make_float2(0.f, 0.f); };
+    auto ldB = [&](int n) -> float2 { return n < a.kh ? gB[n] : make_float2(0.f, 0.f); };
     auto stAcc = [&](int k, float2 v, int slot) { acc[slot] = cadd(acc[slot], cmul(sA[pad_idx(k)], v)); };
     team_fft<P, false, LPV, Q::CTA, Q::ZM>(sB, tw, lane, team, ldB, stAcc);
     __syncthreads();  // B staging and the A tile are free
@@ -337,6 +354,7 @@ __global__ void __launch_bounds__(ConvFinCfg<M>::THREADS, ConvFinCfg<M>::MINB) k
 }
 
 cx_status conv_dispatch_rows(int m, const ConvArgs& a, cudaStream_t st);
+int conv_col_tile(int p);  // the column pass's tile width V for length p (0: unsupported)
 cx_status conv_dispatch_cols(int p, const ConvArgs& a, cudaStream_t st);
 cx_status conv_dispatch_fin_cols(int p, const ConvArgs& a, cudaStream_t st);
 cx_status conv_dispatch_fin_rows(int m, const ConvArgs& a, cudaStream_t st);

@@ -39,6 +39,17 @@ cx_status conv_dispatch_cols(int p, const ConvArgs& a, cudaStream_t st) {
   return CX_ERR_UNSUPPORTED;
 }
 
+int conv_col_tile(int p) {
+  switch (p) {
+#define CX_CONV_CASE_(N) \
+  case N:                \
+    return ConvColCfg<N>::V;
+    CX_CONV_P_SIZES(CX_CONV_CASE_)
+#undef CX_CONV_CASE_
+  }
+  return 0;
+}
+
 cx_status conv_dispatch_fin_cols(int p, const ConvArgs& a, cudaStream_t st) {
   switch (p) {
 #define CX_CONV_CASE_(N) \

@@ -10,7 +10,7 @@ static cx_status launch_rows(const ConvArgs& a, cudaStream_t st) {
   using C = RowCfg<M>;
   auto k = k_conv_rows<M>;
   CX_CUDA_TRY(set_smem(k, C::SMEM));
-  const long items = ((long)a.zc * 2 * a.h + C::TEAMS - 1) / C::TEAMS;
+  const long items = ((long)a.zc * (a.h + a.kh) + C::TEAMS - 1) / C::TEAMS;
   k<<<persistent_grid(k, C::THREADS, C::SMEM, items), C::THREADS, C::SMEM, st>>>(a);
   CX_LAUNCH_CHECK();
   return CX_OK;

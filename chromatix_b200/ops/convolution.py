@@ -1,11 +1,12 @@
 """``fourier_convolution`` (ops/ops.py:9-86) on the GPU.
 
-Real inputs of equal shape convolved plane by plane over their last two axes
+Real inputs convolved plane by plane over their last two axes
 (``axes=(-2, -1)``), mode "same" -- the configuration the ``Microscope``
 uses -- run as one native call (``cx_conv2d_same``): r2c row passes, column
 passes with the product accumulated per plane, and the c2r back, all fused.
-``reduce=True`` also sums over the leading plane axis
-(``BasicSensor(reduce_axis=0)``) inside the same call.
+The kernel has its own plane shape and either the image's leading axes or
+none (one 2D kernel for every plane).  ``reduce=True`` also sums over the
+leading plane axes (``BasicSensor(reduce_axis=0)``) inside the same call.
 
 Transform lengths: the reference pads to the next power of two of the summed
 shape (``fast_fft_shape=True``) or to the summed shape itself; every length
@@ -22,7 +23,8 @@ from .. import _native as nat
 
 
 class cx_conv_desc(nat.ctypes.Structure):
-    _fields_ = [(k, nat.c_int32) for k in ("n_planes", "h", "w", "reduce", "pow2_lengths")]
+    _fields_ = [(k, nat.c_int32) for k in ("n_planes", "h", "w", "kh", "kw", "kernel_broadcast", "reduce",
+                                           "pow2_lengths")]
 
 
 def _lib():
@@ -54,17 +56,23 @@ def fourier_convolution(image, kernel, *, axes=(-2, -1), fast_fft_shape: bool = 
         raise ValueError(f"lengths must be 'smallest' or 'pow2', got {lengths!r}")
     if image.ndim != kernel.ndim:
         raise AssertionError(f"Input ({image.ndim}D) and kernel ({kernel.ndim}D) must have same number of dimensions")
-    if tuple(image.shape) != tuple(kernel.shape):
-        raise NotImplementedError("image and kernel of equal shape only")
+    if image.ndim < 2:
+        raise NotImplementedError("convolution over two axes only")
+    lead = tuple(image.shape[:-2])
+    klead = tuple(kernel.shape[:-2])
+    broadcast = all(k == 1 for k in klead)
+    if klead != lead and not broadcast:
+        raise NotImplementedError("the kernel's leading axes must equal the image's or be all 1")
     if torch.is_complex(image) or torch.is_complex(kernel):
         raise NotImplementedError("real inputs only (the rfftn branch)")
     nat.require_cuda(image, "image")
     a = image.to(torch.float32).contiguous()
     b = kernel.to(device=a.device, dtype=torch.float32).contiguous()
     h, w = a.shape[-2:]
-    lead = tuple(a.shape[:-2])
+    kh, kw = b.shape[-2:]
     planes = int(np.prod(lead)) if lead else 1
-    d = cx_conv_desc(n_planes=planes, h=h, w=w, reduce=1 if reduce else 0, pow2_lengths=1 if lengths == "pow2" else 0)
+    d = cx_conv_desc(n_planes=planes, h=h, w=w, kh=kh, kw=kw, kernel_broadcast=1 if broadcast else 0,
+                     reduce=1 if reduce else 0, pow2_lengths=1 if lengths == "pow2" else 0)
     L = _lib()
     wsb = nat.c_size_t(0)
     nat.check(L.cx_conv2d_workspace_size(d, wsb))

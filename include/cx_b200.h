@@ -340,23 +340,27 @@ cx_status cx_czt_propagate(const cx_czt_prop_desc* d, const void* u_in, void* u_
 
 /* ---------------------------------------------------------------------------
  * Incoherent imaging: fourier_convolution (ops/ops.py:9-86, axes (-2, -1),
- * mode "same", fast_fft_shape) of a sample stack with a PSF stack, plane by
- * plane, and the sensor's sum over the planes (functional/sensors.py:85-86,
- * systems/microscopes.py:271-297).  sample, psf: (n_planes, h, w) float32;
- * out: (h, w) float32 if reduce, else (n_planes, h, w).  Any transform
- * size >= 2h - 1 by 2w - 1 gives the same linear convolution after the
- * crop: the smallest supported lengths >= 2h, 2w are used (even, 2..4096
- * per axis), or the next powers of two (the reference's fast_fft_shape
- * lengths) with pow2_lengths = 1.
+ * mode "same") of a sample stack with a kernel (PSF) stack, plane by plane,
+ * and the sensor's sum over the planes (functional/sensors.py:85-86,
+ * systems/microscopes.py:271-297).  sample: (n_planes, h, w) float32;
+ * kernel: (n_planes, kh, kw) float32, or one (kh, kw) plane for all planes
+ * (kernel_broadcast = 1); out: (h, w) float32 if reduce, else
+ * (n_planes, h, w), cropped from offset ((kh - 1) / 2, (kw - 1) / 2) of the
+ * full convolution.  Any transform size >= h + kh - 1 by w + kw - 1 gives
+ * the same linear convolution after the crop: the smallest supported even
+ * lengths >= 2 max(h, kh), 2 max(w, kw) are used (2..4096 per axis), or the
+ * smallest powers of two >= those with pow2_lengths = 1.
  * ------------------------------------------------------------------------- */
 typedef struct {
   int32_t n_planes, h, w;
-  int32_t reduce;       /* 1: sum over the planes (BasicSensor(reduce_axis=0)) */
-  int32_t pow2_lengths; /* 1: transform lengths are powers of two */
+  int32_t kh, kw;
+  int32_t kernel_broadcast; /* 1: one (kh, kw) kernel for every plane */
+  int32_t reduce;           /* 1: sum over the planes (BasicSensor(reduce_axis=0)) */
+  int32_t pow2_lengths;     /* 1: transform lengths are powers of two */
 } cx_conv_desc;
 
 cx_status cx_conv2d_workspace_size(const cx_conv_desc* d, size_t* bytes);
-cx_status cx_conv2d_same(const cx_conv_desc* d, const float* sample, const float* psf, float* out, void* workspace,
+cx_status cx_conv2d_same(const cx_conv_desc* d, const float* sample, const float* kernel, float* out, void* workspace,
                          size_t workspace_bytes, cx_stream_t stream);
 
 /* ---------------------------------------------------------------------------

@@ -60,6 +60,48 @@ def test_fourier_convolution_published_plane_size():
     assert rel(to_np(pow2), to_np(per[:3]).astype(np.float64).sum(0)) < 1e-5
 
 
+@pytest.mark.parametrize("ha,hb,fast", [(512, 256, True), (513, 253, False)])
+def test_fourier_convolution_reference_cases(ha, hb, fast):
+    """The reference's own cases (tests/test_convolution.py:8-41): a kernel
+    smaller than the image, scipy's "same" convolution, atol 1e-3 there; the
+    FP64 oracle and relative L2 1e-5 here."""
+    import torch
+
+    from chromatix_b200.ops import fourier_convolution
+
+    rng = np.random.default_rng(ha)
+    a, b = rng.standard_normal((ha, ha)), rng.standard_normal((hb, hb))
+    out = fourier_convolution(torch.as_tensor(a, dtype=torch.float32, device="cuda"),
+                              torch.as_tensor(b, dtype=torch.float32, device="cuda"), fast_fft_shape=fast)
+    ref = O.fourier_convolution(a, b, fast_fft_shape=fast)
+    assert tuple(out.shape) == (ha, ha)
+    assert np.allclose(to_np(out), ref, atol=1e-3)
+    assert rel(to_np(out), ref) < 1e-5
+
+
+@pytest.mark.parametrize("lengths", ["smallest", "pow2"])
+@pytest.mark.parametrize("shape,kshape", [((3, 40, 56), (3, 9, 13)), ((2, 21, 17), (2, 40, 33)),
+                                          ((4, 30, 31), (1, 7, 8)), ((2, 1, 9), (2, 5, 1))])
+def test_fourier_convolution_unequal_kernels(shape, kshape, lengths):
+    """Kernels smaller and larger than the image, per plane or one for all
+    planes (broadcast), with and without the plane sum."""
+    import torch
+
+    from chromatix_b200.ops import fourier_convolution
+
+    rng = np.random.default_rng(sum(shape) + sum(kshape))
+    a = rng.standard_normal(shape).astype(np.float32)
+    k = rng.uniform(-1, 1, kshape).astype(np.float32)
+    kb = np.broadcast_to(k, shape[:1] + kshape[1:]).astype(np.float64)
+    ref = np.stack([O.fourier_convolution(a[i].astype(np.float64), kb[i]) for i in range(shape[0])])
+    ad, kd = torch.as_tensor(a, device="cuda"), torch.as_tensor(k, device="cuda")
+    out = fourier_convolution(ad, kd, lengths=lengths)
+    assert tuple(out.shape) == shape
+    assert rel(to_np(out), ref) < 1e-5
+    red = fourier_convolution(ad, kd, reduce=True, lengths=lengths)
+    assert rel(to_np(red), ref.sum(0)) < 1e-5
+
+
 def test_fourier_convolution_rejects_unsupported_forms():
     import torch
 
@@ -67,7 +109,9 @@ def test_fourier_convolution_rejects_unsupported_forms():
 
     a = torch.zeros((2, 16, 16), device="cuda")
     with pytest.raises(NotImplementedError):
-        fourier_convolution(a, torch.zeros((2, 8, 8), device="cuda"))
+        fourier_convolution(a, torch.zeros((3, 8, 8), device="cuda"))
+    with pytest.raises(AssertionError):
+        fourier_convolution(a, torch.zeros((8, 8), device="cuda"))
     with pytest.raises(NotImplementedError):
         fourier_convolution(a, a, mode="full")
     with pytest.raises(NotImplementedError):

@@ -18,6 +18,19 @@ def test_fourier_convolution_matches_scipy_same():
     assert O.rel_l2(c, ref) < 1e-12
 
 
+def test_fourier_convolution_reference_cases():
+    """The reference's own cases (tests/test_convolution.py:8-41): a 512^2
+    image with a 256^2 kernel at power-of-two lengths and 513^2 with 253^2 at
+    the summed lengths, against scipy's "same" convolution (atol 1e-3 there)."""
+    rng = np.random.default_rng(1)
+    for (ha, hb), fast in [((512, 256), True), ((513, 253), False)]:
+        a, b = rng.standard_normal((ha, ha)), rng.standard_normal((hb, hb))
+        c = O.fourier_convolution(a, b, fast_fft_shape=fast)
+        ref = fftconvolve(a, b, mode="same")
+        assert c.shape == a.shape
+        assert np.allclose(c, ref, atol=1e-3) and O.rel_l2(c, ref) < 1e-12
+
+
 def test_basic_sensor_reduce_and_next_order():
     x = np.arange(24.0).reshape(2, 3, 4)
     np.testing.assert_array_equal(O.basic_sensor_reduce(x, 0), x.sum(0))
