@@ -1,8 +1,9 @@
 """Field containers with the reference's scalar-field semantics.
 
-``ScalarField`` (monochromatic, ``u`` of shape ``(... y x)``) and
-``ChromaticScalarField`` (``(... y x wv)``, wavelength innermost) mirror
-core/field.py:49-740.  ``u`` is a CUDA ``complex64`` tensor; ``dx``,
+``ScalarField`` (monochromatic, ``u`` of shape ``(... y x)``),
+``ChromaticScalarField`` (``(... y x wv)``, wavelength innermost) and
+``VectorField`` (monochromatic, ``(... y x 3)``, components z, y, x) mirror
+core/field.py:49-811.  ``u`` is a CUDA ``complex64`` tensor; ``dx``,
 ``origin`` and the spectrum are float64 host arrays (they become per-plane
 launch parameters).  Grids are returned as float32 device tensors, like the
 reference's float32 jax arrays.
@@ -64,6 +65,7 @@ class Field:
     """Base of the scalar field containers (core/field.py:49-531)."""
 
     chromatic = False
+    vectorial = False
 
     def __init__(self, u, dx, origin, spectrum: Spectrum):
         torch = _torch()
@@ -79,7 +81,7 @@ class Field:
     # ---------------------------------------------------------------- layout
     @property
     def spatial_dims(self):
-        return (-3, -2) if self.chromatic else (-2, -1)
+        return (-3, -2) if (self.chromatic or self.vectorial) else (-2, -1)
 
     @property
     def shape(self):
@@ -251,12 +253,16 @@ class Field:
 
     @classmethod
     def build(cls, u, dx, spectrum) -> "Field":
-        """``Field.build`` (core/field.py:364-384), scalar fields only."""
+        """``Field.build`` (core/field.py:364-384): (y x) scalar, (y x 3)
+        vector, (y x wv) chromatic scalar; chromatic vector fields are not
+        part of this build."""
         spec = Spectrum.build(spectrum)
         ndim = u.ndim
         if isinstance(spec, MonoSpectrum):
+            if ndim == 3:
+                return VectorField(u, dx, 0.0, spec)
             if ndim != 2:
-                raise NotImplementedError("vectorial fields are not part of this build")
+                raise NotImplementedError(f"a monochromatic field has 2 (scalar) or 3 (vector) dimensions, got {ndim}")
             return ScalarField(u, dx, 0.0, spec)
         if ndim != 3:
             raise NotImplementedError("vectorial fields are not part of this build")
@@ -369,6 +375,43 @@ class ChromaticScalarField(Field):
             raise AssertionError("Expected last dimension of u to be same as wavelengths.")
 
 
+class VectorField(Field):
+    """Monochromatic vector field, ``u`` of shape (... y x 3) with the
+    components (z, y, x) innermost (core/field.py:743-811)."""
+
+    chromatic = False
+    vectorial = True
+
+    def __init__(self, u, dx, origin, spectrum):
+        spec = spectrum if isinstance(spectrum, Spectrum) else MonoSpectrum(float(spectrum))
+        super().__init__(u, _broadcast_dx(dx, 1).reshape(2),
+                         np.broadcast_to(np.asarray(origin, dtype=np.float64), (2,)).copy(), spec)
+        if self.u.ndim < 3:
+            raise AssertionError(f"Expected 3-dimensional field, got shape {tuple(self.u.shape)}.")
+        if self.u.shape[-1] != 3:
+            raise AssertionError(f"Expected last dimension of u to be 3, got {self.u.shape[-1]}")
+
+    @property
+    def intensity(self):
+        """sum over the components of |u|^2 (core/field.py:808-811), by the
+        native readout kernel."""
+        torch = _torch()
+        nat.require_cuda(self.u, "Field.u")
+        u = self.u.contiguous()
+        out = torch.empty(u.shape[:-1], dtype=torch.float32, device=u.device)
+        dens = nat.upload(np.ones(3), u.device)
+        nat.check(nat.lib().cx_intensity(nat.ptr(u), out.numel(), 3, nat.ptr(dens), nat.ptr(out),
+                                         nat.stream_handle(u.device)))
+        return out
+
+    @property
+    def power(self):
+        """area * sum over (y, x) of the intensity (core/field.py:801-806)."""
+        torch = _torch()
+        pd = self.intensity.sum(dim=(-2, -1), dtype=torch.float64)
+        return (float(np.prod(self.dx_wv[0])) * pd[..., None, None, None]).to(torch.float32)
+
+
 def pad(field: Field, pad_width, cval: float = 0.0) -> Field:
     """``pad`` (core/field.py:534-549): zero (or ``cval``) padding of y and x."""
     torch = _torch()
@@ -376,10 +419,11 @@ def pad(field: Field, pad_width, cval: float = 0.0) -> Field:
         pad_width = (int(pad_width), int(pad_width))
     py, px = int(pad_width[0]), int(pad_width[1])
     u = field.u
-    if field.chromatic:
+    inner = field.chromatic or field.vectorial  # wavelength / component axis innermost
+    if inner:
         u = u.movedim(-1, -3)
     u = torch.nn.functional.pad(u, (px, px, py, py), value=complex(cval) if cval else 0.0)
-    if field.chromatic:
+    if inner:
         u = u.movedim(-3, -1).contiguous()
     return field.replace(u=u)
 

@@ -1,7 +1,7 @@
 """Drop-in subset of ``chromatix.functional`` for the FFT-propagation hot path."""
 
 from .convenience import optical_fft
-from .lenses import df_lens, ff_lens, thin_lens
+from .lenses import df_lens, ff_lens, high_na_ff_lens, thin_lens
 from .phase_masks import phase_change, spectrally_modulate_phase
 from .propagation import (
     asm_propagate,

@@ -339,6 +339,31 @@ cx_status cx_czt_propagate(const cx_czt_prop_desc* d, const void* u_in, void* u_
                            size_t workspace_bytes, cx_stream_t stream);
 
 /* ---------------------------------------------------------------------------
+ * High-NA lens: high_na_ff_lens (functional/lenses.py:98-156) of n_fields
+ * monochromatic fields (ny, nx) complex64, scalar, or vectorial (ny, nx, 3)
+ * with components (z, y, x) converted to the spherical basis first
+ * (cartesian_to_spherical, core/field.py:897-940).  The defocus
+ * exp(i k sz f) / sz on the pupil's frequency grid (k = 2 pi n / lambda,
+ * sz = sqrt(max(1 - NA^2 |f_grid lambda / n|^2, 0)), 0 where sz = 0), then the
+ * zoomed FFT over [-zoom pi, zoom pi] with the end point onto (my, mx),
+ * zoom = 2 NA my output_dx / ((nx - 1) lambda).  u_out: (n_fields, my, mx[, 3]).
+ * ------------------------------------------------------------------------- */
+typedef struct {
+  int32_t n_fields;
+  int32_t ny, nx;          /* pupil grid (nx >= 2) */
+  int32_t my, mx;          /* output grid (>= 2 each) */
+  int32_t vectorial;       /* 0: scalar; 1: vector field, 3 components innermost */
+  double f, n_medium, NA, wavelength;
+  double dy, dx;           /* pupil spacing */
+  double origin_y, origin_x; /* pupil grid origin (vector basis change) */
+  double output_dx;        /* output pixel pitch (both axes) */
+} cx_high_na_desc;
+
+cx_status cx_high_na_ff_lens_workspace_size(const cx_high_na_desc* d, size_t* bytes);
+cx_status cx_high_na_ff_lens(const cx_high_na_desc* d, const void* u_in, void* u_out, void* workspace,
+                             size_t workspace_bytes, cx_stream_t stream);
+
+/* ---------------------------------------------------------------------------
  * Incoherent imaging: fourier_convolution (ops/ops.py:9-86, axes (-2, -1),
  * mode "same") of a sample stack with a kernel (PSF) stack, plane by plane,
  * and the sensor's sum over the planes (functional/sensors.py:85-86,

@@ -900,6 +900,72 @@ def zoomed_fft(x, k_start, k_end, output_shape, axes=(-2, -1), include_end=True,
     return cztn(x, output_shape, tuple(a for _ in output_shape), w, axes, prec)
 
 
+def pupil_grid(shape, dx, origin=(0.0, 0.0)):
+    """Spatial grid of a monochromatic field (core/field.py:23-33, 759-770):
+    dx * (i - N/2) + origin, shape (y x 2), FP64."""
+    ny, nx = shape
+    dy, dxx = (float(dx), float(dx)) if np.ndim(dx) == 0 else (float(dx[0]), float(dx[1]))
+    gy = (np.arange(ny) - ny / 2) * dy + origin[0]
+    gx = (np.arange(nx) - nx / 2) * dxx + origin[1]
+    GY, GX = np.meshgrid(gy, gx, indexing="ij")
+    return np.stack([GY, GX], axis=-1)
+
+
+def cartesian_to_spherical(u, grid, n, NA, f):
+    """``cartesian_to_spherical`` (core/field.py:897-940): the pupil field of a
+    vector field ``u`` (y x 3, components z, y, x) in the spherical basis of a
+    lens of focal length f (Eq. 6 of arXiv:2502.03170), returned as (z, y, x)."""
+    pupil_radius = f * NA / n
+    radius_sq = np.sum(grid**2, axis=-1)
+    mask = radius_sq <= pupil_radius**2
+    sin_theta2 = radius_sq * mask / f**2
+    cos_theta = np.sqrt(1 - sin_theta2)
+    sin_theta = np.sqrt(sin_theta2)
+    phi = np.arctan2(grid[..., 0], grid[..., 1])
+    cos_phi, sin_phi = np.cos(phi), np.sin(phi)
+    sin_2phi = 2 * sin_phi * cos_phi
+    cos_2phi = cos_phi**2 - sin_phi**2
+    fx, fy = u[..., 2], u[..., 1]
+    e_x = ((cos_theta + 1.0) + (cos_theta - 1.0) * cos_2phi) * fx + (cos_theta - 1.0) * sin_2phi * fy
+    e_y = ((cos_theta + 1.0) - (cos_theta - 1.0) * cos_2phi) * fy + (cos_theta - 1.0) * sin_2phi * fx
+    e_z = -2.0 * sin_theta * (cos_phi * fx + sin_phi * fy)
+    return np.stack([e_z, e_y, e_x], axis=-1) / 2
+
+
+def high_na_ff_lens(u, dx, wavelength, f, n, NA, output_shape=None, output_dx=None, origin=(0.0, 0.0)):
+    """``high_na_ff_lens`` (functional/lenses.py:98-156) of a monochromatic
+    square field: ``u`` (y x) scalar or (y x 3) vectorial.  The defocus
+    exp(i k sz f) / sz on the pupil's frequency grid, then a zoomed FFT over
+    [-zoom pi, zoom pi] with the end point, zoom = 2 NA fov_out / ((N - 1)
+    lambda).  Returns (u_out, output_dx)."""
+    u = np.asarray(u, dtype=np.complex128)
+    vectorial = u.ndim == 3
+    shape = u.shape[:2]
+    if vectorial:
+        spherical_u = cartesian_to_spherical(u, pupil_grid(shape, dx, origin), n, NA, f)
+    else:
+        spherical_u = u
+    if output_dx is None:
+        output_dx = float(dx) if np.ndim(dx) == 0 else float(dx[0])
+    if output_shape is None:
+        output_shape = shape
+    fov_out = output_shape[0] * output_dx
+    zoom_factor = 2 * NA * fov_out / ((u.shape[1] - 1) * wavelength)
+    fg = freq_grid(shape, np.broadcast_to(np.asarray(dx, np.float64), (2,)).reshape(1, 2), FP64, False)
+    s_grid = fg * wavelength / n
+    sz_sq = 1 - NA**2 * np.sum(s_grid**2, axis=-1)
+    sz = np.sqrt(np.maximum(sz_sq, 0.0))
+    k = 2 * np.pi * n / wavelength
+    with np.errstate(divide="ignore", invalid="ignore"):
+        defocus = np.where(sz != 0.0, np.exp(1j * k * sz * f) / sz, 0.0)
+    if vectorial:
+        defocus = defocus[..., None]
+    axes = (0, 1)
+    out = zoomed_fft(spherical_u * defocus, -zoom_factor * np.pi, zoom_factor * np.pi, tuple(output_shape),
+                     axes=axes, include_end=True)
+    return out, output_dx
+
+
 # ---------------------------------------------------------------------------
 # modified Born series  (experimental/modified_born_series/)
 # ---------------------------------------------------------------------------
