@@ -61,6 +61,8 @@ static cx_status ms_plan(const cx_ms_desc* d, MsPlan* p) {
   a.ky0 = d->ky0;
   a.kx0 = d->kx0;
   a.na_f2 = -1.0;
+  a.precise = 0;
+  a.conj_h = 0;
   a.planes = nullptr;
   a.H = nullptr;
   return ensure_twiddles(&a.twg);
@@ -89,6 +91,7 @@ static MsArgs ms_args(const cx_ms_desc* d, const MsPlan& p) {
   a.dz = d->dz;
   a.kdz_f = (float)(6.283185307179586476925286766559 * d->dz / d->wavelength);
   a.twg = p.col.twg;
+  a.load_scale = 1.f;
   return a;
 }
 

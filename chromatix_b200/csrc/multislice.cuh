@@ -21,7 +21,9 @@
 
 namespace cx {
 
-enum MsMode { MS_LOAD = 0, MS_FWD = 1, MS_BWD = 2, MS_FINAL = 3 };
+// MS_FLUOR: the fluorescent forward step (samples.py:387-404), transmittance
+// and source before the propagation: v <- v exp(i k dz dn_i) + fl_i exp(i ph_i)
+enum MsMode { MS_LOAD = 0, MS_FWD = 1, MS_BWD = 2, MS_FINAL = 3, MS_FLUOR = 4 };
 
 struct MsArgs {
   int ny, nx, pad_y, pad_x, py, px;
@@ -39,6 +41,9 @@ struct MsArgs {
   float* gab;           // MS_BWD: dL/d abs_i (ny, nx)
   float2* dst;          // MS_FINAL: (ny, nx) crop of the padded grid
   const float2* twg;  // device twiddle tables (ensure_twiddles)
+  const float* fl;      // MS_FLUOR: (D, ny, nx) fluorescence amplitude
+  const float* ph;      // MS_FLUOR: (D, ny, nx) random phases
+  float load_scale;     // MS_LOAD: factor on the source (1 / px when a row pass follows the load)
 };
 
 // thin-sample transmittance t = exp(i 2 pi dz / lam (dn + i abs))
@@ -69,7 +74,9 @@ template <int NX, int MODE>
 struct MsRowCfg {
   using C = RowCfg<NX>;
   static constexpr int NXA = (NX + 3) & ~3;  // one row of floats, rounded to 16 bytes
-  static constexpr int PF = (MODE == MS_FWD || MODE == MS_BWD) ? 2 * NXA + (MODE == MS_BWD ? 2 * NXA : 0) : 0;
+  static constexpr int PF = (MODE == MS_FWD || MODE == MS_BWD || MODE == MS_FLUOR)
+                                ? 2 * NXA + (MODE == MS_BWD ? 2 * NXA : 0) + (MODE == MS_FLUOR ? NXA : 0)
+                                : 0;
   // cp.async needs 16-byte aligned shared destinations: the prefetch area
   // starts at the next 16-byte boundary after the transform buffers, and PF
   // (a multiple of 4 floats) keeps every team's area aligned
@@ -85,8 +92,11 @@ template <int NX, int MODE>
 __device__ __forceinline__ bool ms_prefetch(const MsArgs& a, float* pf, int yd, int y, int lane, int lpv) {
   const size_t off = (size_t)a.slice * a.ny * a.nx + (size_t)yd * a.nx;
   const float* dn = a.dn + off;
-  const float* ab = a.ab + off;
+  // MS_FLUOR: the second and third rows are the fluorescence and the phases
+  const float* ab = (MODE == MS_FLUOR ? a.fl : a.ab) + off;
   bool ok = (a.nx % 4 == 0) && ((reinterpret_cast<size_t>(dn) & 15) == 0) && ((reinterpret_cast<size_t>(ab) & 15) == 0);
+  const float* ph = MODE == MS_FLUOR ? a.ph + off : nullptr;
+  if constexpr (MODE == MS_FLUOR) ok = ok && ((reinterpret_cast<size_t>(ph) & 15) == 0);
   const float2* u = nullptr;
   if constexpr (MODE == MS_BWD) {
     u = a.rec_u + (size_t)y * a.px;
@@ -97,6 +107,7 @@ __device__ __forceinline__ bool ms_prefetch(const MsArgs& a, float* pf, int yd, 
   for (int i = lane; i < a.nx / 4; i += lpv) {
     cp_async16(pf + 4 * i, dn + 4 * i);
     cp_async16(pf + NXA + 4 * i, ab + 4 * i);
+    if constexpr (MODE == MS_FLUOR) cp_async16(pf + 2 * NXA + 4 * i, ph + 4 * i);
   }
   if constexpr (MODE == MS_BWD) {
     for (int i = lane; i < a.px / 2; i += lpv) cp_async16(pf + 2 * NXA + 4 * i, u + 2 * i);
@@ -136,7 +147,7 @@ __global__ void __launch_bounds__(RowCfg<NX>::THREADS, RowCfg<NX>::MINB) k_ms_ro
       float2* rrow = a.rec ? a.rec + (size_t)y * a.px : nullptr;
       auto load = [&](int n) -> float2 {
         const int xs = n - a.ox;
-        const float2 v = (rin && xs >= 0 && xs < a.sx) ? srow[xs] : make_float2(0.f, 0.f);
+        const float2 v = (rin && xs >= 0 && xs < a.sx) ? cscale(srow[xs], a.load_scale) : make_float2(0.f, 0.f);
         if (a.record) rrow[n] = v;
         return v;
       };
@@ -155,14 +166,32 @@ __global__ void __launch_bounds__(RowCfg<NX>::THREADS, RowCfg<NX>::MINB) k_ms_ro
       team_fft<NX, true>(s, tw, lane, team, load_row, store);
       continue;
     }
-    if constexpr (MODE == MS_FWD || MODE == MS_BWD) {
+    if constexpr (MODE == MS_FWD || MODE == MS_BWD || MODE == MS_FLUOR) {
     // the slice's rows stream into shared memory while the inverse transform runs
     const bool pre = yin && ms_prefetch<NX, MODE>(a, pf, yd, y, lane, C::LPV);
     auto sst = [&](int k, float2 v, int) { s[pad_idx(k)] = v; };
     team_fft<NX, true>(s, tw, lane, team, load_row, sst);
     if (pre) cp_async_wait_all();
     team_sync<C::LPV>(team);
-    if constexpr (MODE == MS_FWD) {
+    if constexpr (MODE == MS_FLUOR) {
+      constexpr int NXA = MsRowCfg<NX, MODE>::NXA;
+#pragma unroll 2
+      for (int k = lane; k < NX; k += C::LPV) {
+        float2 v = s[pad_idx(k)];
+        const int xd = k - a.pad_x;
+        if (yin && xd >= 0 && xd < a.nx) {
+          const size_t idx = plane_d + (size_t)yd * a.nx + xd;
+          const float dnv = pre ? pf[xd] : a.dn[idx];
+          const float flv = pre ? pf[NXA + xd] : a.fl[idx];
+          const float phv = pre ? pf[2 * NXA + xd] : a.ph[idx];
+          float sp, cp;
+          sincosf(phv, &sp, &cp);
+          v = cmul(v, ms_transmittance(a, dnv, 0.f));
+          v = make_float2(v.x + flv * cp, v.y + flv * sp);
+        }
+        s[pad_idx(k)] = v;
+      }
+    } else if constexpr (MODE == MS_FWD) {
       float2* rrow = a.record ? a.rec + (size_t)y * a.px : nullptr;
 #pragma unroll 2
       for (int k = lane; k < NX; k += C::LPV) {

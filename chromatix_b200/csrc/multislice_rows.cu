@@ -25,6 +25,8 @@ static cx_status launch_ms_rows(const MsArgs& a, cudaStream_t st) {
       return launch_ms_rows_mode<NX, MS_FWD>(a, st);
     case MS_BWD:
       return launch_ms_rows_mode<NX, MS_BWD>(a, st);
+    case MS_FLUOR:
+      return launch_ms_rows_mode<NX, MS_FLUOR>(a, st);
     default:
       return launch_ms_rows_mode<NX, MS_FINAL>(a, st);
   }

@@ -43,12 +43,14 @@ __device__ __forceinline__ float2 prop_kernel_accurate(int ky, int kx, const Pro
   if (!a.precise && a.kernel == CX_KERNEL_ASM && K <= 8.0 && !a.bandlimit && pl.shift_y == 0.0 &&
       pl.shift_x == 0.0) {
     // Short distances (thin slices): every phase term is below 8 rad, so FP32
-    // evaluation keeps the phase error below ~2e-6 rad -- inside the accuracy
-    // budget -- at a fraction of the FP64 cost.
-    const float fy = (float)freq_index(ky, a.py) * (float)(1.0 / ((double)a.py * pl.dy)) - (float)a.ky0;
-    const float fx = (float)freq_index(kx, a.px) * (float)(1.0 / ((double)a.px * pl.dx)) - (float)a.kx0;
-    const float q = (float)(pl.wavelength / a.n_med);
-    const float kern = 1.0f - (q * q) * (fy * fy + fx * fx);
+    // square root and sin / cos keep the phase error below ~1e-6 rad -- inside
+    // the accuracy budget -- at a fraction of the FP64 cost.  kern = 1 - q^2 f^2
+    // is formed in FP64: in FP32 it cancels near the evanescent boundary
+    // (kern -> 0), where sqrt(kern) magnifies the rounding into ~1e-4 rad.
+    const double fy = (double)freq_index(ky, a.py) / ((double)a.py * pl.dy) - a.ky0;
+    const double fx = (double)freq_index(kx, a.px) / ((double)a.px * pl.dx) - a.kx0;
+    const double q = pl.wavelength / a.n_med;
+    const float kern = (float)(1.0 - (q * q) * (fy * fy + fx * fx));
     float amp = 1.f, ph = 0.f;
     if (kern >= 0.f || a.remove_evanescent) {
       ph = (float)K * sqrtf(fmaxf(kern, 0.f));

@@ -17,5 +17,5 @@ from .propagation import (
     transform_propagate_sas,
 )
 from .pupils import circular_pupil, square_pupil, super_gaussian_pupil, tukey_pupil
-from .samples import multislice_thick_sample, thin_sample
+from .samples import fluorescent_multislice_thick_sample, multislice_thick_sample, thin_sample
 from .sources import objective_point_source, plane_wave

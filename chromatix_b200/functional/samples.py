@@ -7,7 +7,7 @@ import numpy as np
 from .. import _native as nat
 from ..core.field import Field
 
-__all__ = ["thin_sample", "multislice_thick_sample"]
+__all__ = ["thin_sample", "multislice_thick_sample", "fluorescent_multislice_thick_sample"]
 
 
 def thin_sample(field: Field, absorption, dn, thickness) -> Field:
@@ -221,3 +221,98 @@ def multislice_thick_sample(field: Field, absorption_stack, dn_stack, n, thickne
     outs = [_MS_FN.apply(u2[b], dn, ab, desc_bytes) for b in range(u2.shape[0])]
     out = torch.stack(outs).reshape(u.shape)
     return field.replace(u=out)
+
+
+class cx_fluor_desc(nat.ctypes.Structure):
+    _fields_ = ([(k, nat.c_int32) for k in ("ny", "nx", "pad", "n_slices", "num_samples", "remove_evanescent",
+                                            "bandlimit", "reserved")] +
+                [("seed", nat.ctypes.c_uint64)] +
+                [(k, nat.c_double) for k in ("n_medium", "wavelength", "dy", "dx", "dz", "ky0", "kx0")])
+
+
+def _fluor_lib():
+    L = nat.lib()
+    if not hasattr(L, "_cx_fluor_sig"):
+        P = nat.ctypes.POINTER(cx_fluor_desc)
+        V = nat.c_void_p
+        L.cx_fluorescent_multislice_workspace_size.restype = nat.c_int32
+        L.cx_fluorescent_multislice_workspace_size.argtypes = [P, nat.ctypes.POINTER(nat.c_size_t)]
+        L.cx_fluorescent_multislice.restype = nat.c_int32
+        L.cx_fluorescent_multislice.argtypes = [P, V, V, V, V, V, V, nat.c_size_t, V]
+        L._cx_fluor_sig = True
+    return L
+
+
+def _seed_of(key) -> int:
+    """64-bit generator seed from an int or a (2,) uint32 key (jax's PRNGKey data)."""
+    k = np.asarray(key)
+    if k.ndim == 0:
+        return int(k) & 0xFFFFFFFFFFFFFFFF
+    seed = 0
+    for v in k.astype(np.uint64).reshape(-1):
+        seed = ((seed << 32) ^ int(v)) & 0xFFFFFFFFFFFFFFFF
+    return seed
+
+
+def fluorescent_multislice_thick_sample(field: Field, fluorescence_stack, dn_stack, n, thickness_per_slice,
+                                        pad_width: int, key, num_samples: int = 1, propagator_forward=None,
+                                        propagator_backward=None, kykx=(0.0, 0.0), remove_evanescent: bool = False,
+                                        bandlimit: bool = False, *, random_phases=None):
+    """Thick, transparent, fluorescent sample (functional/samples.py:285-441):
+    Monte-Carlo samples of random fluorophore phases; per sample the padded
+    field goes through the slices (phase exp(i 2 pi dn dz / lambda), plus the
+    fluorescence with its random phase, then an ASM step of ``dz``), and the
+    stack of intensities comes from propagating the result back slice by slice.
+    Returns the (D, h, w) float32 intensity stack averaged over the samples.
+
+    One native call (``cx_fluorescent_multislice``).  Phases: ``random_phases``
+    ((num_samples, D, h, w) radians) if given, else the library's counter-based
+    generator seeded by ``key`` (an int or a (2,) uint32 key); the reference's
+    jax.random stream is not reproduced.  As in the reference, each sample
+    starts from the field the previous one ended with."""
+    from .sources import materialize
+
+    torch = nat.torch_mod()
+    field = materialize(field)
+    if field.chromatic or getattr(field, "vectorial", False):
+        raise NotImplementedError("fluorescent multislice takes a monochromatic scalar field")
+    if propagator_forward is not None or propagator_backward is not None:
+        raise NotImplementedError("custom propagators are not supported by the fused slice kernels")
+    dev = field.device
+    fl = fluorescence_stack if isinstance(fluorescence_stack, torch.Tensor) else torch.as_tensor(
+        np.asarray(fluorescence_stack, np.float32))
+    dn = dn_stack if isinstance(dn_stack, torch.Tensor) else torch.as_tensor(np.asarray(dn_stack, np.float32))
+    fl = fl.to(device=dev, dtype=torch.float32).contiguous()
+    dn = dn.to(device=dev, dtype=torch.float32).contiguous()
+    if tuple(fl.shape) != tuple(dn.shape):
+        raise AssertionError("fluorescence_stack and dn_stack must have equal shapes")
+    D, ny, nx = dn.shape
+    if (ny, nx) != tuple(field.spatial_shape) or field.u.ndim != 2:
+        raise AssertionError("one (h, w) field with stack slices of its shape is expected")
+    S = int(num_samples)
+    ph = None
+    if random_phases is not None:
+        ph = random_phases if isinstance(random_phases, torch.Tensor) else torch.as_tensor(
+            np.asarray(random_phases, np.float32))
+        ph = ph.to(device=dev, dtype=torch.float32).contiguous()
+        if tuple(ph.shape) != (S, D, ny, nx):
+            raise AssertionError(f"random_phases must have shape {(S, D, ny, nx)}, got {tuple(ph.shape)}")
+    d = cx_fluor_desc()
+    d.ny, d.nx, d.pad, d.n_slices, d.num_samples = ny, nx, int(pad_width), D, S
+    d.remove_evanescent, d.bandlimit = int(bool(remove_evanescent)), int(bool(bandlimit))
+    d.seed = _seed_of(key)
+    d.n_medium = float(n)
+    d.wavelength = float(field.spectrum.wavelength[0])
+    d.dy, d.dx = (float(v) for v in field.dx_wv[0])
+    d.dz = float(thickness_per_slice)
+    d.ky0, d.kx0 = (float(v) for v in np.asarray(kykx, np.float64).reshape(2))
+    L = _fluor_lib()
+    wsb = nat.c_size_t(0)
+    nat.check(L.cx_fluorescent_multislice_workspace_size(d, wsb))
+    ws = nat.workspace(wsb.value, dev)
+    u = field.u.contiguous()
+    out = torch.empty((D, ny, nx), dtype=torch.float32, device=dev)
+    nat.check(L.cx_fluorescent_multislice(d, nat.ptr(u), nat.ptr(fl), nat.ptr(dn),
+                                          nat.ptr(ph) if ph is not None else None, nat.ptr(out), nat.ptr(ws),
+                                          wsb.value, nat.stream_handle(dev)))
+    return out

@@ -339,6 +339,38 @@ cx_status cx_czt_propagate(const cx_czt_prop_desc* d, const void* u_in, void* u_
                            size_t workspace_bytes, cx_stream_t stream);
 
 /* ---------------------------------------------------------------------------
+ * Fluorescent thick sample: fluorescent_multislice_thick_sample
+ * (functional/samples.py:285-441).  Per Monte-Carlo sample: the padded field
+ * goes through D slices, u <- IFFT2(FFT2(u exp(i 2 pi dz dn_i / lambda)
+ * + fl_i exp(i ph_i)) H(dz)) (ASM, band limit / evanescent options as
+ * compute_asm_propagator), then out[D - 1 - i] += |crop(IFFT2(U H(-dz)^(i+1)))|^2
+ * with U = FFT2(u_D); the next sample starts from U H(-dz)^D, as the
+ * reference's loop carries it; out is divided by num_samples.
+ * u_in: (ny, nx) complex64; fluorescence, dn: (D, ny, nx) float32;
+ * phases: (num_samples, D, ny, nx) float32 in radians, or NULL: phase =
+ * float32(2 pi) * (top 24 bits of splitmix64(seed + (c + 1) * 0x9E3779B97F4A7C15)) / 2^24,
+ * c = sample * D ny nx + (i ny + y) nx + x (the reference draws them from
+ * jax.random, which this library does not reproduce); out: (D, ny, nx) float32.
+ * ------------------------------------------------------------------------- */
+typedef struct {
+  int32_t ny, nx;            /* field shape (unpadded) */
+  int32_t pad;               /* pad_width on each side */
+  int32_t n_slices;          /* D */
+  int32_t num_samples;       /* Monte-Carlo samples */
+  int32_t remove_evanescent, bandlimit;
+  int32_t reserved;
+  uint64_t seed;             /* phase generator seed (phases == NULL) */
+  double n_medium, wavelength, dy, dx;
+  double dz;                 /* thickness_per_slice */
+  double ky0, kx0;           /* kykx */
+} cx_fluor_desc;
+
+cx_status cx_fluorescent_multislice_workspace_size(const cx_fluor_desc* d, size_t* bytes);
+cx_status cx_fluorescent_multislice(const cx_fluor_desc* d, const void* u_in, const float* fluorescence,
+                                    const float* dn, const float* phases, float* out, void* workspace,
+                                    size_t workspace_bytes, cx_stream_t stream);
+
+/* ---------------------------------------------------------------------------
  * High-NA lens: high_na_ff_lens (functional/lenses.py:98-156) of n_fields
  * monochromatic fields (ny, nx) complex64, scalar, or vectorial (ny, nx, 3)
  * with components (z, y, x) converted to the spherical basis first

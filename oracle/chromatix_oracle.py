@@ -817,6 +817,60 @@ def multislice_thick_sample(field: OField, absorption_stack, dn_stack, n, thickn
     return crop(field, pad_width)
 
 
+def fluor_phases(seed: int, sample: int, shape):
+    """The counter-based phases of cx_fluorescent_multislice (no counterpart in
+    the reference, which draws them with jax.random): splitmix64 of
+    seed + (c + 1) * 0x9E3779B97F4A7C15 (mod 2^64), c = sample * size + index,
+    top 24 bits as u in [0, 1), phase = float32(2 pi) * u in float32."""
+    n = int(np.prod(shape))
+    with np.errstate(over="ignore"):
+        c = np.uint64(sample) * np.uint64(n) + np.arange(n, dtype=np.uint64)
+        z = np.uint64(seed) + (c + np.uint64(1)) * np.uint64(0x9E3779B97F4A7C15)
+        z = (z ^ (z >> np.uint64(30))) * np.uint64(0xBF58476D1CE4E5B9)
+        z = (z ^ (z >> np.uint64(27))) * np.uint64(0x94D049BB133111EB)
+        z = z ^ (z >> np.uint64(31))
+    u = (z >> np.uint64(40)).astype(np.float32) * np.float32(1.0 / 16777216.0)
+    return (np.float32(2 * np.pi) * u).astype(np.float32).reshape(shape)
+
+
+def fluorescent_multislice_thick_sample(field: OField, fluorescence_stack, dn_stack, n, thickness_per_slice,
+                                        pad_width, phases, kykx=(0.0, 0.0), remove_evanescent=False,
+                                        bandlimit=False):
+    """Fluorescent thick sample (functional/samples.py:285-441) with the
+    Monte-Carlo phases given, ``phases`` (num_samples, D, h, w): per sample the
+    forward slices u <- ifft2(fft2(fl_i e^(i ph_i) + u e^(i 2 pi dn_i dz / lam)) Hf),
+    then U = fft2(u) and I[D-1-i] += |crop(ifft2(U Hb^(i+1)))|^2; the field
+    (U Hb^D after a sample) carries into the next sample as in the reference's
+    fori_loop; I / num_samples."""
+    fluorescence_stack = np.asarray(fluorescence_stack)
+    dn_stack = np.asarray(dn_stack)
+    assert fluorescence_stack.shape == dn_stack.shape
+    phases = np.asarray(phases)
+    S, D = phases.shape[0], dn_stack.shape[0]
+    original_shape = field.spatial_shape
+    axes = field.spatial_dims
+    field = pad(field, pad_width)
+    dn = center_pad(dn_stack, (0, pad_width, pad_width))
+    Hf = compute_asm_propagator(field, thickness_per_slice, n, kykx, remove_evanescent=remove_evanescent,
+                                bandlimit=bandlimit)
+    Hb = compute_asm_propagator(field, -thickness_per_slice, n, kykx, remove_evanescent=remove_evanescent,
+                                bandlimit=bandlimit)
+    lam = field.broadcasted_wavelength
+    intensity = np.zeros((D,) + tuple(original_shape))
+    u = field.u
+    for s in range(S):
+        fl = center_pad(fluorescence_stack * np.exp(1j * phases[s]), (0, pad_width, pad_width))
+        for i in range(D):
+            u = u * np.exp(1j * 2 * np.pi * dn[i] * thickness_per_slice / lam)
+            u = np.fft.ifftn(np.fft.fftn(fl[i] + u, axes=axes) * Hf, axes=axes)
+        u = np.fft.fftn(u, axes=axes)
+        for i in range(D):
+            u = u * Hb
+            fi = field.replace(u=np.fft.ifftn(u, axes=axes))
+            intensity[D - 1 - i] += crop(fi, pad_width).intensity
+    return intensity / S
+
+
 def multislice_loss_and_grad(u0, dn_stack, absorption_stack, target, n, dz, wavelength, dx, NA=None,
                              reverse_propagate_distance=None):
     """FP64 reference for the differentiable multislice benchmark.
