@@ -16,6 +16,12 @@ from .propagation import (
     transform_propagate,
     transform_propagate_sas,
 )
+from .rays import (
+    compute_free_space_abcd,
+    compute_plano_convex_spherical_lens_abcd,
+    compute_thin_spherical_lens_abcd,
+    ray_transfer,
+)
 from .pupils import circular_pupil, square_pupil, super_gaussian_pupil, tukey_pupil
 from .samples import fluorescent_multislice_thick_sample, multislice_thick_sample, thin_sample
 from .sources import objective_point_source, plane_wave

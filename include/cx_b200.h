@@ -371,6 +371,31 @@ cx_status cx_fluorescent_multislice(const cx_fluor_desc* d, const void* u_in, co
                                     size_t workspace_bytes, cx_stream_t stream);
 
 /* ---------------------------------------------------------------------------
+ * Ray transfer: ray_transfer (functional/rays.py:102-154), Collins' integral
+ * of an ABCD system with magnification M:
+ *   u_out = exp(i k (D - 1/M) |g|^2 / (2B M^4)) IFFT2(H FFT2(exp(i k (A - M) |g|^2 / (2B)) u_in)),
+ * H = exp(-i pi (lambda / n) (B / M) |f|^2) (the transfer kernel of z = B/M),
+ * g = (i - N/2) d + origin, k = 2 pi n / lambda; the output spacing is d / M
+ * (the caller's metadata).  u_in, u_out: (batch, ny, nx, n_wv) complex64
+ * (n_wv = 1: (batch, ny, nx)); planes_dev: n_planes = batch * n_wv cx_plane
+ * entries (wavelength, dy, dx of each plane; z is set to B / M inside).
+ * ------------------------------------------------------------------------- */
+typedef struct {
+  int32_t ny, nx, n_wv;
+  int32_t n_planes;        /* batch * n_wv */
+  int32_t precision;       /* cx_precision of the transfer kernel */
+  int32_t reserved;
+  double A, B, D;          /* ABCD[0][0], ABCD[0][1], ABCD[1][1] */
+  double magnification;
+  double n_medium;
+  double origin_y, origin_x;
+} cx_ray_desc;
+
+cx_status cx_ray_transfer_workspace_size(const cx_ray_desc* d, size_t* bytes);
+cx_status cx_ray_transfer(const cx_ray_desc* d, const cx_plane* planes_dev, const void* u_in, void* u_out,
+                          void* workspace, size_t workspace_bytes, cx_stream_t stream);
+
+/* ---------------------------------------------------------------------------
  * High-NA lens: high_na_ff_lens (functional/lenses.py:98-156) of n_fields
  * monochromatic fields (ny, nx) complex64, scalar, or vectorial (ny, nx, 3)
  * with components (z, y, x) converted to the spherical basis first

@@ -817,6 +817,28 @@ def multislice_thick_sample(field: OField, absorption_stack, dn_stack, n, thickn
     return crop(field, pad_width)
 
 
+def _fft_centred(x, axes, inverse=False):
+    """``fft`` / ``ifft`` with shift=True (utils/fft.py:8-48)."""
+    f = np.fft.ifftn if inverse else np.fft.fftn
+    return np.fft.fftshift(f(np.fft.ifftshift(x, axes=axes), axes=axes), axes=axes)
+
+
+def ray_transfer(field: OField, ABCD, n, magnification=1.0) -> OField:
+    """Collins' integral through an ABCD system (functional/rays.py:102-154)."""
+    A, B, D = ABCD[0][0], ABCD[0][1], ABCD[1][1]
+    M = magnification
+    lam = field.broadcasted_wavelength
+    k = 2 * np.pi * n / lam
+    input_phase = k / (2 * B) * (A - M) * l2_sq_norm(field.grid)
+    transfer_phase = (np.pi * (lam / n) * B / M) * l2_sq_norm(field.f_grid)
+    output_phase = k / (2 * B) * (D - 1 / M) * l2_sq_norm(field.grid / (M**2))
+    axes = field.spatial_dims
+    fft_input = field.u * np.exp(1j * input_phase)
+    u = np.exp(1j * output_phase) * _fft_centred(_fft_centred(fft_input, axes) * np.exp(-1j * transfer_phase),
+                                                 axes, inverse=True)
+    return field.replace(u=u, dx=field.dx / M)
+
+
 def fluor_phases(seed: int, sample: int, shape):
     """The counter-based phases of cx_fluorescent_multislice (no counterpart in
     the reference, which draws them with jax.random): splitmix64 of
