@@ -39,18 +39,6 @@ namespace cx {
   X(80) X(96) X(112) X(128) X(160) X(192) X(224) X(256) X(320) X(384) X(448) X(512) X(640) X(768) X(896)    \
   X(1024) X(1280) X(1536) X(1792) X(2048)
 
-// First-stage zero mask for an input that is nonzero only on [0, N / 2):
-// with an even first radix R_0 the inputs r >= R_0 / 2 of every first-stage
-// butterfly (indices j + r N / R_0 >= N / 2) are zero.  Odd first radices
-// (odd N) get no mask.
-template <int N>
-__host__ __device__ constexpr unsigned lower_half_mask() {
-  constexpr int R0 = Plan<N>::P.r[0];
-  unsigned m = 0u;
-  if (R0 % 2 == 0)
-    for (int r = R0 / 2; r < R0; ++r) m |= 1u << r;
-  return m;
-}
 
 struct ConvArgs {
   int h, w;               // image (sample) plane shape = output shape

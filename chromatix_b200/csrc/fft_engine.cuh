@@ -528,6 +528,19 @@ __host__ __device__ constexpr unsigned edge_zero_mask() {
   return m;
 }
 
+// First-stage zero mask for an input that is nonzero only on [0, N / 2)
+// (zero padding to twice the length): with an even first radix R_0 the
+// inputs r >= R_0 / 2 of every first-stage butterfly (indices
+// j + r N / R_0 >= N / 2) are zero.  Odd first radices (odd N) get no mask.
+template <int N>
+__host__ __device__ constexpr unsigned lower_half_mask() {
+  constexpr int R0 = Plan<N>::P.r[0];
+  unsigned m = 0u;
+  if (R0 % 2 == 0)
+    for (int r = R0 / 2; r < R0; ++r) m |= 1u << r;
+  return m;
+}
+
 // Same transform with the load and/or store functor applied in a compact,
 // coalesced loop through the team's shared buffer (lane-strided indices)
 // instead of once per butterfly value inside the unrolled first / last

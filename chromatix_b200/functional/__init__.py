@@ -23,5 +23,10 @@ from .rays import (
     ray_transfer,
 )
 from .pupils import circular_pupil, square_pupil, super_gaussian_pupil, tukey_pupil
-from .samples import fluorescent_multislice_thick_sample, multislice_thick_sample, thin_sample
+from .samples import (
+    fluorescent_multislice_thick_sample,
+    multislice_thick_sample,
+    polarized_multislice_thick_sample,
+    thin_sample,
+)
 from .sources import objective_point_source, plane_wave

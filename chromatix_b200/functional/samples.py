@@ -7,7 +7,8 @@ import numpy as np
 from .. import _native as nat
 from ..core.field import Field
 
-__all__ = ["thin_sample", "multislice_thick_sample", "fluorescent_multislice_thick_sample"]
+__all__ = ["thin_sample", "multislice_thick_sample", "fluorescent_multislice_thick_sample",
+           "polarized_multislice_thick_sample"]
 
 
 def thin_sample(field: Field, absorption, dn, thickness) -> Field:
@@ -316,3 +317,61 @@ def fluorescent_multislice_thick_sample(field: Field, fluorescence_stack, dn_sta
                                           nat.ptr(ph) if ph is not None else None, nat.ptr(out), nat.ptr(ws),
                                           wsb.value, nat.stream_handle(dev)))
     return out
+
+
+class cx_polar_desc(nat.ctypes.Structure):
+    _fields_ = ([(k, nat.c_int32) for k in ("ny", "nx", "n_slices", "reserved")] +
+                [(k, nat.c_double) for k in ("n_medium", "wavelength", "dy", "dx", "dz", "NA")])
+
+
+def _polar_lib():
+    L = nat.lib()
+    if not hasattr(L, "_cx_polar_sig"):
+        P = nat.ctypes.POINTER(cx_polar_desc)
+        V = nat.c_void_p
+        L.cx_polarized_multislice_workspace_size.restype = nat.c_int32
+        L.cx_polarized_multislice_workspace_size.argtypes = [P, nat.ctypes.POINTER(nat.c_size_t)]
+        L.cx_polarized_multislice.restype = nat.c_int32
+        L.cx_polarized_multislice.argtypes = [P, V, V, V, V, nat.c_size_t, V]
+        L._cx_polar_sig = True
+    return L
+
+
+def polarized_multislice_thick_sample(field: Field, potential_stack, n, thickness_per_slice, NA=1.0) -> Field:
+    """Birefringent thick sample (functional/samples.py:444-546): a
+    monochromatic ``VectorField`` through the (D, h, w, 3, 3) scattering
+    potential, per slice u <- P_op(u) + H_op(V_i Q_op(u)) with the vectorial
+    free-space and scattering operators on the grid zero-padded to twice the
+    size, band-limited to ``NA``.  One native call
+    (``cx_polarized_multislice``): per slice two row passes and two column
+    passes whose CTAs hold the three components, so the 3x3 k-space projector
+    and the potential apply between the transforms."""
+    from .sources import materialize
+
+    torch = nat.torch_mod()
+    field = materialize(field)
+    if not getattr(field, "vectorial", False):
+        raise AssertionError("Must be a vectorial Field")
+    nat.require_cuda(field.u, "Field.u")
+    if field.u.ndim != 3:
+        raise NotImplementedError("one (h, w, 3) vector field")
+    ny, nx = field.spatial_shape
+    V = potential_stack if isinstance(potential_stack, torch.Tensor) else torch.as_tensor(
+        np.asarray(potential_stack, np.float32))
+    if torch.is_complex(V):
+        raise NotImplementedError("real scattering potentials (the reference's Float array)")
+    V = V.to(device=field.device, dtype=torch.float32).contiguous()
+    if V.ndim != 5 or tuple(V.shape[1:]) != (ny, nx, 3, 3):
+        raise AssertionError(f"potential_stack must have shape (D, {ny}, {nx}, 3, 3), got {tuple(V.shape)}")
+    d = cx_polar_desc(ny=ny, nx=nx, n_slices=V.shape[0], n_medium=float(n),
+                      wavelength=float(field.spectrum.wavelength[0]), dz=float(thickness_per_slice), NA=float(NA))
+    d.dy, d.dx = (float(v) for v in field.dx_wv[0])
+    L = _polar_lib()
+    wsb = nat.c_size_t(0)
+    nat.check(L.cx_polarized_multislice_workspace_size(d, wsb))
+    u = field.u.contiguous()
+    out = torch.empty_like(u)
+    ws = nat.workspace(wsb.value, field.device)
+    nat.check(L.cx_polarized_multislice(d, nat.ptr(u), nat.ptr(V), nat.ptr(out), nat.ptr(ws), wsb.value,
+                                        nat.stream_handle(field.device)))
+    return field.replace(u=out)

@@ -396,6 +396,31 @@ cx_status cx_ray_transfer(const cx_ray_desc* d, const cx_plane* planes_dev, cons
                           void* workspace, size_t workspace_bytes, cx_stream_t stream);
 
 /* ---------------------------------------------------------------------------
+ * Polarized thick sample: polarized_multislice_thick_sample
+ * (functional/samples.py:444-546) of a monochromatic vector field u_in
+ * (ny, nx, 3) complex64, components (z, y, x), through D slices of a real
+ * scattering potential (D, ny, nx, 3, 3) float32 (rows and columns in
+ * (z, y, x) order), on the grid zero-padded to (2 ny, 2 nx):
+ *   u <- crop IFFT2(Q (e FFT2(pad u) + h FFT2(pad(V_i crop IFFT2(Q FFT2(pad u))))))
+ * Q = I - k k^T / km^2 (k = (kz, ky, kx), km = 2 pi n / lambda, zero where
+ * |k_perp| > NA km), e = exp(i kz dz), h = -i/2 exp(i kz dz) dz / kz (0 where
+ * kz = 0).  Even ny, nx (the reference takes its frequencies from the field
+ * padded by N // 2 per side, which is 2N only for even N), 2N <= 4096.
+ * ------------------------------------------------------------------------- */
+typedef struct {
+  int32_t ny, nx;
+  int32_t n_slices;
+  int32_t reserved;
+  double n_medium, wavelength, dy, dx;
+  double dz;               /* thickness_per_slice */
+  double NA;
+} cx_polar_desc;
+
+cx_status cx_polarized_multislice_workspace_size(const cx_polar_desc* d, size_t* bytes);
+cx_status cx_polarized_multislice(const cx_polar_desc* d, const void* u_in, const float* potential, void* u_out,
+                                  void* workspace, size_t workspace_bytes, cx_stream_t stream);
+
+/* ---------------------------------------------------------------------------
  * High-NA lens: high_na_ff_lens (functional/lenses.py:98-156) of n_fields
  * monochromatic fields (ny, nx) complex64, scalar, or vectorial (ny, nx, 3)
  * with components (z, y, x) converted to the spherical basis first

@@ -817,6 +817,53 @@ def multislice_thick_sample(field: OField, absorption_stack, dn_stack, n, thickn
     return crop(field, pad_width)
 
 
+def polarized_multislice_thick_sample(u, dx, wavelength, potential_stack, n, thickness_per_slice, NA=1.0):
+    """Birefringent multislice (functional/samples.py:444-546) of a
+    monochromatic vector field ``u`` (y x 3, components z, y, x) through a
+    (d y x 3 3) scattering potential, FP64: per slice
+    u <- P_op(u) + H_op(V_i Q_op(u)) on the grid zero-padded to twice the size
+    (padding after the data, crop of the first rows / columns)."""
+    u = np.asarray(u, dtype=np.complex128)
+    ny, nx = u.shape[:2]
+    P, Q = 2 * ny, 2 * nx
+    dy, dxx = (float(dx), float(dx)) if np.ndim(dx) == 0 else (float(dx[0]), float(dx[1]))
+    # k grid of the field padded by N // 2 per side, ifftshifted (FFT order)
+    ky = 2 * np.pi * np.fft.fftfreq(P, d=dy)
+    kx = 2 * np.pi * np.fft.fftfreq(Q, d=dxx)
+    KY, KX = np.meshgrid(ky, kx, indexing="ij")
+    km = 2 * np.pi * n / wavelength
+    kz = np.sqrt(np.maximum(0.0, km**2 - KY**2 - KX**2))
+    k = np.stack([kz, KY, KX], axis=-1) / km
+    Qm = np.eye(3) - k[..., :, None] * k[..., None, :]
+    Qm = np.where(((KY**2 + KX**2) <= NA**2 * km**2)[..., None, None], Qm, 0.0)
+    dz = thickness_per_slice
+    with np.errstate(divide="ignore", invalid="ignore"):
+        e = np.where(kz > 0, np.exp(1j * kz * dz), 0)
+        h = np.where(kz > 0, -1j / 2 * np.exp(1j * kz * dz) / kz * dz, 0)
+
+    def pad_op(v):
+        return np.pad(v, [(0, ny), (0, nx), (0, 0)])
+
+    def crop_op(v):
+        return v[:ny, :nx]
+
+    def fft(v):
+        return np.fft.fft2(v, axes=(0, 1))
+
+    def ifft(v):
+        return np.fft.ifft2(v, axes=(0, 1))
+
+    def matvec(M, v):
+        return np.einsum("...ij,...j->...i", M, v)
+
+    for V in np.asarray(potential_stack, dtype=np.float64):
+        Qu = crop_op(ifft(matvec(Qm, fft(pad_op(u)))))
+        s = matvec(V, Qu)
+        u = crop_op(ifft(matvec(Qm, e[..., None] * fft(pad_op(u))))) + crop_op(
+            ifft(matvec(Qm, h[..., None] * fft(pad_op(s)))))
+    return u
+
+
 def _fft_centred(x, axes, inverse=False):
     """``fft`` / ``ifft`` with shift=True (utils/fft.py:8-48)."""
     f = np.fft.ifftn if inverse else np.fft.fftn
