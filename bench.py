@@ -448,6 +448,61 @@ def microscope_published_arm(args):
     print(json.dumps(line), flush=True)
 
 
+def next_rows_arm(args):
+    """Timings of the widened rows, one JSON line each: high_na_ff_lens
+    (512^2 vector field -> 512^2), fluorescent multislice (256^2, 64 slices,
+    pad 64, one sample), polarized multislice (256^2 vector field, 32 slices),
+    ray_transfer (16 fields of 1024^2).  Seeded synthetic inputs; algorithmic
+    bytes = the inputs read and outputs written once, against measured HBM."""
+    import numpy as np
+    import torch
+
+    import chromatix_b200 as cx
+    import chromatix_b200.functional as cf
+
+    dev = torch.device("cuda", 0)
+    g = torch.Generator(device=dev).manual_seed(0)
+    timer = _device_timer(torch, dev, args.steps, args.warmup)
+    peak, src = _peak_hbm()
+
+    def crand(shape):
+        return torch.complex(torch.randn(shape, generator=g, device=dev), torch.randn(shape, generator=g, device=dev))
+
+    def emit(name, ms, nbytes, cfg):
+        achieved = nbytes / (ms * 1e-3) / 1e9
+        line = _base_line(f"ms, {name}", round(ms, 4), "ms", args.steps, args.warmup, ms, "c64/f32",
+                          dict(cfg, l2="flushed between timed steps"), higher_is_better=False,
+                          roofline={"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
+                                    "frac": round(achieved / peak, 4), "traffic": None, "peak_source": src})
+        print(json.dumps(line), flush=True)
+
+    u = crand((512, 512, 3))
+    f = cx.Field.build(u, 0.3, 0.532)
+    ms = timer(lambda: cf.high_na_ff_lens(f, 100.0, 1.33, 0.8, output_shape=(512, 512), output_dx=0.1))
+    emit("high_na_ff_lens 512^2 vector field", ms, 2 * u.numel() * 8, {"workload": "high_na_ff_lens"})
+
+    D, N = 64, 256
+    fl = torch.rand((D, N, N), generator=g, device=dev)
+    dn = 0.02 * torch.rand((D, N, N), generator=g, device=dev)
+    fs = cx.Field.build(crand((N, N)), 0.3, 0.532)
+    ms = timer(lambda: cf.fluorescent_multislice_thick_sample(fs, fl, dn, 1.33, 0.5, 64, 7))
+    emit("fluorescent multislice 256^2, 64 slices, pad 64", ms, 3 * D * N * N * 4 + N * N * 8,
+         {"workload": "fluorescent_multislice"})
+
+    D2 = 32
+    pot = 0.02 * torch.rand((D2, N, N, 3, 3), generator=g, device=dev)
+    fv = cx.Field.build(crand((N, N, 3)), 0.2, 0.55)
+    ms = timer(lambda: cf.polarized_multislice_thick_sample(fv, pot, 1.33, 0.5, 1.0))
+    emit("polarized multislice 256^2 vector field, 32 slices", ms, pot.numel() * 4 + 2 * N * N * 24,
+         {"workload": "polarized_multislice"})
+
+    ur = crand((16, 1024, 1024))
+    fr = cx.ScalarField(ur, 0.5, 0.0, cx.MonoSpectrum(0.532))
+    abcd = cf.compute_free_space_abcd(30.0) @ cf.compute_thin_spherical_lens_abcd(50.0)
+    ms = timer(lambda: cf.ray_transfer(fr, abcd, 1.0, 1.5))
+    emit("ray_transfer 16 x 1024^2", ms, 2 * ur.numel() * 8, {"workload": "ray_transfer"})
+
+
 def rescaled_published_arm(args):
     """The reference's published rescaled-propagation timings
     (docs/examples/rescaled_propagation.ipynb, cells 4, 8, 19): 1024^2 plane
@@ -822,7 +877,7 @@ def main():
     ap.add_argument("--accuracy", action="store_true", help="also report the error vs the FP64 oracle")
     ap.add_argument("--workload", default="psf",
                     choices=["psf", "serve", "psf_published", "rescaled_published", "microscope_published", "asm",
-                             "multislice", "mbs"],
+                             "multislice", "mbs", "next_rows"],
                     help="psf: the batched 4f PSF stack (headline); the others print one line each for the "
                          "other configurations")
     ap.add_argument("--micro-planes", type=int, default=128, help="microscope_published: planes (published: 128)")
@@ -847,6 +902,8 @@ def main():
         rescaled_published_arm(args)
     elif args.workload == "microscope_published":
         microscope_published_arm(args)
+    elif args.workload == "next_rows":
+        next_rows_arm(args)
     elif args.workload == "multislice":
         multislice_arm(args)
     elif args.workload == "mbs":
