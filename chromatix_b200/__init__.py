@@ -7,9 +7,9 @@ ABI of ``include/cx_b200.h`` (``chromatix_b200/_lib/libcx_b200.so``).
 
 from . import config
 from .config import get_precision, precision, set_precision
-from .core import ChromaticScalarField, Field, MonoSpectrum, ScalarField, Spectrum, VectorField, crop, pad, shift_grid
+from .core import ChromaticScalarField, ChromaticVectorField, Field, MonoSpectrum, ScalarField, Spectrum, VectorField, crop, pad, shift_grid
 
-__all__ = ["Field", "ScalarField", "ChromaticScalarField", "VectorField", "Spectrum", "MonoSpectrum", "pad", "crop", "shift_grid",
+__all__ = ["Field", "ScalarField", "ChromaticScalarField", "VectorField", "ChromaticVectorField", "Spectrum", "MonoSpectrum", "pad", "crop", "shift_grid",
            "config", "set_precision", "get_precision", "precision", "functional"]
 
 

@@ -81,6 +81,8 @@ class Field:
     # ---------------------------------------------------------------- layout
     @property
     def spatial_dims(self):
+        if self.chromatic and self.vectorial:
+            return (-4, -3)
         return (-3, -2) if (self.chromatic or self.vectorial) else (-2, -1)
 
     @property
@@ -264,8 +266,10 @@ class Field:
             if ndim != 2:
                 raise NotImplementedError(f"a monochromatic field has 2 (scalar) or 3 (vector) dimensions, got {ndim}")
             return ScalarField(u, dx, 0.0, spec)
+        if ndim == 4:
+            return ChromaticVectorField(u, dx, 0.0, spec)
         if ndim != 3:
-            raise NotImplementedError("vectorial fields are not part of this build")
+            raise NotImplementedError(f"a chromatic field has 3 (scalar) or 4 (vector) dimensions, got {ndim}")
         return ChromaticScalarField(u, dx, 0.0, spec)
 
     @classmethod
@@ -412,6 +416,38 @@ class VectorField(Field):
         return (float(np.prod(self.dx_wv[0])) * pd[..., None, None, None]).to(torch.float32)
 
 
+class ChromaticVectorField(Field):
+    """Chromatic vector field, ``u`` of shape (y x wv 3), components (z, y, x)
+    innermost (core/field.py:813-894)."""
+
+    chromatic = True
+    vectorial = True
+
+    def __init__(self, u, dx, origin, spectrum: Spectrum):
+        super().__init__(u, _broadcast_dx(dx, spectrum.size),
+                         np.broadcast_to(np.asarray(origin, dtype=np.float64), (spectrum.size, 2)).copy(), spectrum)
+        if self.u.ndim != 4:
+            raise AssertionError(f"Expected 4-dimensional field, got shape {tuple(self.u.shape)}.")
+        if self.u.shape[-2] != spectrum.size:
+            raise AssertionError("Expected last dimension of u to be same as wavelengths.")
+        if self.u.shape[-1] != 3:
+            raise AssertionError(f"Expected last dimension of u to be 3, got {self.u.shape[-1]}")
+
+    @property
+    def intensity(self):
+        """sum over wavelengths (spectral density) and components of |u|^2
+        (core/field.py:889-894), by the native readout kernel."""
+        torch = _torch()
+        nat.require_cuda(self.u, "Field.u")
+        u = self.u.contiguous()
+        W = self.spectrum.size
+        out = torch.empty(u.shape[:-2], dtype=torch.float32, device=u.device)
+        dens = nat.upload(np.repeat(np.asarray(self.spectrum.density, np.float64), 3), u.device)
+        nat.check(nat.lib().cx_intensity(nat.ptr(u), out.numel(), 3 * W, nat.ptr(dens), nat.ptr(out),
+                                         nat.stream_handle(u.device)))
+        return out
+
+
 def pad(field: Field, pad_width, cval: float = 0.0) -> Field:
     """``pad`` (core/field.py:534-549): zero (or ``cval``) padding of y and x."""
     torch = _torch()
@@ -420,11 +456,16 @@ def pad(field: Field, pad_width, cval: float = 0.0) -> Field:
     py, px = int(pad_width[0]), int(pad_width[1])
     u = field.u
     inner = field.chromatic or field.vectorial  # wavelength / component axis innermost
+    shape = tuple(u.shape)
+    if field.chromatic and field.vectorial:
+        u = u.reshape(shape[:-2] + (shape[-2] * shape[-1],))  # (wv, 3) as one inner axis
     if inner:
         u = u.movedim(-1, -3)
     u = torch.nn.functional.pad(u, (px, px, py, py), value=complex(cval) if cval else 0.0)
     if inner:
         u = u.movedim(-3, -1).contiguous()
+    if field.chromatic and field.vectorial:
+        u = u.reshape(u.shape[:-1] + shape[-2:])
     return field.replace(u=u)
 
 

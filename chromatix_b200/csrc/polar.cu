@@ -19,10 +19,11 @@ enum PolMode { POL_LOAD = 0, POL_SCATTER = 1, POL_NEXT = 2 };
 struct PolArgs {
   int N, M, P, Q;             // field (N, M), padded (P, Q) = (2N, 2M)
   int mode, last, slice;
+  int n_wv, wv;               // wavelengths interleaved in u_in / u_out, the one processed
   double km, NA2km2, dy, dx;  // km = 2 pi n / lambda
   float scale;                // 1 / (P Q)
-  const float2* u_in;         // (N, M, 3)
-  float2* u_out;              // (N, M, 3)
+  const float2* u_in;         // (N, M, W, 3)
+  float2* u_out;              // (N, M, W, 3)
   const float* V;             // (D, N, M, 3, 3) potential
   const float2* Tin;          // (N, Q, 3) x-spectra
   float2* Tout;               // (N, Q, 3)
@@ -66,8 +67,9 @@ __global__ void __launch_bounds__(PolRowCfg<Q>::THREADS, PolRowCfg<Q>::MINB) k_p
     const bool valid = y < a.N;
     if constexpr (MODE == POL_LOAD) {
       if (valid) {
-        const float2* src = a.u_in + (size_t)y * a.M * 3 + c;
-        auto load = [&](int n) -> float2 { return n < a.M ? src[(size_t)n * 3] : make_float2(0.f, 0.f); };
+        const size_t es = (size_t)a.n_wv * 3;  // element stride
+        const float2* src = a.u_in + (size_t)y * a.M * es + (size_t)a.wv * 3 + c;
+        auto load = [&](int n) -> float2 { return n < a.M ? src[(size_t)n * es] : make_float2(0.f, 0.f); };
         float2* dst = a.Tout + (size_t)y * Q * 3 + c;
         auto store = [&](int k, float2 v, int) { dst[(size_t)k * 3] = v; };
         team_fft<Q, false, LPV, false, lower_half_mask<Q>()>(s, tw, lane, team, load, store);
@@ -87,7 +89,9 @@ __global__ void __launch_bounds__(PolRowCfg<Q>::THREADS, PolRowCfg<Q>::MINB) k_p
       float2* s1 = s0 + C::LEN;
       float2* s2 = s1 + C::LEN;
       const float* Vr = MODE == POL_SCATTER ? a.V + ((size_t)a.slice * a.N + (valid ? y : 0)) * a.M * 9 : nullptr;
-      float2* orow = (MODE == POL_NEXT && a.last) ? a.u_out + (size_t)(valid ? y : 0) * a.M * 3 : nullptr;
+      const size_t es = (size_t)a.n_wv * 3;
+      float2* orow = (MODE == POL_NEXT && a.last) ? a.u_out + (size_t)(valid ? y : 0) * a.M * es + (size_t)a.wv * 3
+                                                    : nullptr;
       for (int x = t3; x < Q && valid; x += 3 * LPV) {
         const int px = pad_idx(x);
         if (x >= a.M) {
@@ -105,9 +109,9 @@ __global__ void __launch_bounds__(PolRowCfg<Q>::THREADS, PolRowCfg<Q>::MINB) k_p
           v2 = w2;
         }
         if (orow) {
-          orow[(size_t)x * 3 + 0] = v0;
-          orow[(size_t)x * 3 + 1] = v1;
-          orow[(size_t)x * 3 + 2] = v2;
+          orow[(size_t)x * es + 0] = v0;
+          orow[(size_t)x * es + 1] = v1;
+          orow[(size_t)x * es + 2] = v2;
         }
         s0[px] = v0;
         s1[px] = v1;
@@ -328,8 +332,8 @@ struct PolPlan {
 };
 
 static cx_status pol_plan(const cx_polar_desc* d, PolPlan* p) {
-  if (!d || d->ny < 2 || d->nx < 2 || d->n_slices < 1 || !(d->wavelength > 0) || !(d->n_medium > 0) ||
-      !(d->dy > 0) || !(d->dx > 0)) {
+  if (!d || d->ny < 2 || d->nx < 2 || d->n_slices < 1 || d->n_wv < 1 || d->wv < 0 || d->wv >= d->n_wv ||
+      !(d->wavelength > 0) || !(d->n_medium > 0) || !(d->dy > 0) || !(d->dx > 0)) {
     set_error("invalid polarized multislice descriptor");
     return CX_ERR_INVALID;
   }
@@ -394,6 +398,8 @@ extern "C" cx_status cx_polarized_multislice(const cx_polar_desc* d, const void*
   a.dy = d->dy;
   a.dx = d->dx;
   a.scale = (float)(1.0 / ((double)a.P * (double)a.Q));
+  a.n_wv = d->n_wv;
+  a.wv = d->wv;
   a.u_in = static_cast<const float2*>(u_in);
   a.u_out = static_cast<float2*>(u_out);
   a.V = potential;

@@ -320,7 +320,7 @@ def fluorescent_multislice_thick_sample(field: Field, fluorescence_stack, dn_sta
 
 
 class cx_polar_desc(nat.ctypes.Structure):
-    _fields_ = ([(k, nat.c_int32) for k in ("ny", "nx", "n_slices", "reserved")] +
+    _fields_ = ([(k, nat.c_int32) for k in ("ny", "nx", "n_slices", "n_wv", "wv", "reserved")] +
                 [(k, nat.c_double) for k in ("n_medium", "wavelength", "dy", "dx", "dz", "NA")])
 
 
@@ -339,7 +339,8 @@ def _polar_lib():
 
 def polarized_multislice_thick_sample(field: Field, potential_stack, n, thickness_per_slice, NA=1.0) -> Field:
     """Birefringent thick sample (functional/samples.py:444-546): a
-    monochromatic ``VectorField`` through the (D, h, w, 3, 3) scattering
+    ``VectorField`` (or, wavelength by wavelength with the potential shared as
+    in the reference, a ``ChromaticVectorField``) through the (D, h, w, 3, 3) scattering
     potential, per slice u <- P_op(u) + H_op(V_i Q_op(u)) with the vectorial
     free-space and scattering operators on the grid zero-padded to twice the
     size, band-limited to ``NA``.  One native call
@@ -353,8 +354,9 @@ def polarized_multislice_thick_sample(field: Field, potential_stack, n, thicknes
     if not getattr(field, "vectorial", False):
         raise AssertionError("Must be a vectorial Field")
     nat.require_cuda(field.u, "Field.u")
-    if field.u.ndim != 3:
-        raise NotImplementedError("one (h, w, 3) vector field")
+    W = field.spectrum.size if field.chromatic else 1
+    if field.u.ndim != (4 if field.chromatic else 3):
+        raise NotImplementedError("one (h, w, 3) or (h, w, wv, 3) vector field")
     ny, nx = field.spatial_shape
     V = potential_stack if isinstance(potential_stack, torch.Tensor) else torch.as_tensor(
         np.asarray(potential_stack, np.float32))
@@ -363,15 +365,16 @@ def polarized_multislice_thick_sample(field: Field, potential_stack, n, thicknes
     V = V.to(device=field.device, dtype=torch.float32).contiguous()
     if V.ndim != 5 or tuple(V.shape[1:]) != (ny, nx, 3, 3):
         raise AssertionError(f"potential_stack must have shape (D, {ny}, {nx}, 3, 3), got {tuple(V.shape)}")
-    d = cx_polar_desc(ny=ny, nx=nx, n_slices=V.shape[0], n_medium=float(n),
-                      wavelength=float(field.spectrum.wavelength[0]), dz=float(thickness_per_slice), NA=float(NA))
-    d.dy, d.dx = (float(v) for v in field.dx_wv[0])
     L = _polar_lib()
-    wsb = nat.c_size_t(0)
-    nat.check(L.cx_polarized_multislice_workspace_size(d, wsb))
     u = field.u.contiguous()
     out = torch.empty_like(u)
-    ws = nat.workspace(wsb.value, field.device)
-    nat.check(L.cx_polarized_multislice(d, nat.ptr(u), nat.ptr(V), nat.ptr(out), nat.ptr(ws), wsb.value,
-                                        nat.stream_handle(field.device)))
+    for w in range(W):  # independent wavelengths, one workspace in stream order
+        d = cx_polar_desc(ny=ny, nx=nx, n_slices=V.shape[0], n_wv=W, wv=w, n_medium=float(n),
+                          wavelength=float(field.spectrum.wavelength[w]), dz=float(thickness_per_slice), NA=float(NA))
+        d.dy, d.dx = (float(v) for v in field.dx_wv[w])
+        wsb = nat.c_size_t(0)
+        nat.check(L.cx_polarized_multislice_workspace_size(d, wsb))
+        ws = nat.workspace(wsb.value, field.device)
+        nat.check(L.cx_polarized_multislice(d, nat.ptr(u), nat.ptr(V), nat.ptr(out), nat.ptr(ws), wsb.value,
+                                            nat.stream_handle(field.device)))
     return field.replace(u=out)

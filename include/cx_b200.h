@@ -397,8 +397,9 @@ cx_status cx_ray_transfer(const cx_ray_desc* d, const cx_plane* planes_dev, cons
 
 /* ---------------------------------------------------------------------------
  * Polarized thick sample: polarized_multislice_thick_sample
- * (functional/samples.py:444-546) of a monochromatic vector field u_in
- * (ny, nx, 3) complex64, components (z, y, x), through D slices of a real
+ * (functional/samples.py:444-546) of a vector field u_in (ny, nx, 3)
+ * complex64, components (z, y, x) -- or of one wavelength of a chromatic
+ * vector field (ny, nx, n_wv, 3) -- through D slices of a real
  * scattering potential (D, ny, nx, 3, 3) float32 (rows and columns in
  * (z, y, x) order), on the grid zero-padded to (2 ny, 2 nx):
  *   u <- crop IFFT2(Q (e FFT2(pad u) + h FFT2(pad(V_i crop IFFT2(Q FFT2(pad u))))))
@@ -410,8 +411,10 @@ cx_status cx_ray_transfer(const cx_ray_desc* d, const cx_plane* planes_dev, cons
 typedef struct {
   int32_t ny, nx;
   int32_t n_slices;
+  int32_t n_wv, wv;        /* u is (ny, nx, n_wv, 3); this call processes wavelength wv (the reference
+                              broadcasts the potential over the wavelengths of a chromatic field) */
   int32_t reserved;
-  double n_medium, wavelength, dy, dx;
+  double n_medium, wavelength, dy, dx;  /* of wavelength wv */
   double dz;               /* thickness_per_slice */
   double NA;
 } cx_polar_desc;

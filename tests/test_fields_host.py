@@ -38,3 +38,13 @@ def test_seed_of_key_forms():
     assert _seed_of(5) == 5
     assert _seed_of(np.array([1, 2], np.uint32)) == (1 << 32) | 2
     assert _seed_of(-1) == 0xFFFFFFFFFFFFFFFF
+
+
+def test_chromatic_vector_field_layout_and_padding():
+    wl = (np.array([0.5, 0.6]), np.ones(2))
+    u = torch.arange(6 * 5 * 2 * 3, dtype=torch.float32).reshape(6, 5, 2, 3).to(torch.complex64)
+    f = cx.Field.build(u, 0.4, wl)
+    assert type(f) is cx.ChromaticVectorField and f.spatial_dims == (-4, -3) and f.spatial_shape == (6, 5)
+    p = pad(f, (1, 2))
+    assert tuple(p.u.shape) == (8, 9, 2, 3) and torch.equal(p.u[1:7, 2:7], u)
+    assert torch.equal(crop(p, (1, 2)).u, u)

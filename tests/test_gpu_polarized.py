@@ -57,3 +57,25 @@ def test_polarized_multislice_rejects_unsupported_forms():
     scalar = cx.Field.build(torch.zeros((16, 16), dtype=torch.complex64, device="cuda"), 0.2, 0.5)
     with pytest.raises(AssertionError):
         cf.polarized_multislice_thick_sample(scalar, np.zeros((1, 16, 16, 3, 3), np.float32), 1.0, 0.5)
+
+
+def test_polarized_multislice_chromatic_vector_field():
+    """A ChromaticVectorField: every wavelength through the same potential
+    (the reference broadcasts it over the wavelength axis), with its own
+    spacing and wavenumber."""
+    import torch
+
+    import chromatix_b200 as cx
+    import chromatix_b200.functional as cf
+
+    wl = np.array([0.47, 0.55, 0.61])
+    rng = np.random.default_rng(9)
+    u = (rng.standard_normal((24, 32, 3, 3)) + 1j * rng.standard_normal((24, 32, 3, 3))).astype(np.complex64)
+    V = rng.uniform(-0.05, 0.05, (3, 24, 32, 3, 3)).astype(np.float32)
+    f = cx.Field.build(torch.as_tensor(u, device="cuda"), 0.2, (wl, np.ones(3)))
+    assert isinstance(f, cx.ChromaticVectorField)
+    out = to_np(cf.polarized_multislice_thick_sample(f, torch.as_tensor(V, device="cuda"), 1.33, 0.5, 1.0).u)
+    for w in range(3):
+        ref = O.polarized_multislice_thick_sample(u[:, :, w].astype(np.complex128), 0.2, wl[w],
+                                                  V.astype(np.float64), 1.33, 0.5, 1.0)
+        assert rel(out[:, :, w], ref) < 1e-5
