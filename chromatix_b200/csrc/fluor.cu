@@ -10,12 +10,13 @@
 // Backward: H_b^(i+1) = H(-(i+1) dz) with the band limit of dz (|z| and a
 // conjugate phase for z < 0, as compute_asm_propagator; the limit and the
 // evanescent mask are powers of themselves), so plane i of the stack is the
-// prop2d column pass of the forward state with z = -(i+1) dz followed by its
-// inverse row pass; the planes are cropped in those passes and summed as
-// px^2 |.|^2 / S into out[D - 1 - i].
+// column FFT of the forward state (once per sample), times H(-(i+1) dz), the
+// column inverse and the prop2d inverse row pass; the planes are cropped in
+// those passes and summed as px^2 |.|^2 / S into out[D - 1 - i].
 // The reference carries the field from one sample into the next: sample s + 1
-// starts from U_s H_b^D (a spectrum, used as a field); that carry is a
-// column pass without the inverse (k_fluor_carry), times px.
+// starts from U_s H_b^D (a spectrum, used as a field): px U H(-D dz), an
+// elementwise product with the spectrum U = FFT_y(state) that the backward
+// planes share (k_fluor_cols computes it once per sample).
 #include <cmath>
 #include <cstdint>
 #include <vector>
@@ -56,11 +57,48 @@ __global__ void k_fluor_fill_h(float2* __restrict__ H, Prop2DArgs a, const cx_pl
     H[i] = prop_kernel(i / a.px, i % a.px, a, p);
 }
 
-// The carry: T2 = scale * H * FFT_y(T) per column (the prop2d column pass
-// without its inverse), V-column tiles as k_prop_cols.  Once per sample.
-template <int NY>
-__global__ void __launch_bounds__(ColCfg<NY>::THREADS, ColCfg<NY>::MINB)
-    k_fluor_carry(const float2* __restrict__ T, float2* __restrict__ T2, Prop2DArgs a, float scale) {
+// Column passes of the backward stack, V-column tiles as k_prop_cols:
+//   FLUOR_SPEC: U = FFT_y(S) of the forward state, all rows (once per sample)
+//   FLUOR_BACK: plane q of a chunk: IFFT_y(U H(z_q)) / (py px), rows
+//               [pad, pad + ny) into T2 (q, ny, px) -- the column pass of
+//               k_prop_cols without its forward transform, which is the same
+//               for every plane
+enum FluorCol { FLUOR_SPEC = 0, FLUOR_BACK = 1 };
+
+// no blocks-per-SM bound: the FP64 propagator in the staged load needs
+// about 90 registers, more than the column configuration's bound leaves
+// Base ASM propagator of |z| = dz per frequency (FFT order), FP64: {v, kind}
+// with kind 1 propagating (phase v = K sqrt(kern)), 2 evanescent (decay
+// v = K sqrt(-kern)), 0 outside the band limit -- the FP64 branch of
+// prop_kernel_accurate with shift 0.  Plane z = -m dz then has phase -m v
+// (the conjugate) or decay exp(-m v), m = |z| / dz: the multiplier is
+// linear in |z|, so the square root and the divisions run once per call.
+__global__ void k_fluor_ptable(double2* __restrict__ tab, Prop2DArgs a, const cx_plane* plp) {
+  const cx_plane pl = *plp;
+  const double K = 6.283185307179586476925286766559 * fabs(pl.z) * a.n_med / pl.wavelength;
+  const double q = pl.wavelength / a.n_med;
+  const long total = (long)a.py * a.px;
+  for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < total; i += (long)gridDim.x * blockDim.x) {
+    const int ky = (int)(i / a.px), kx = (int)(i % a.px);
+    const double fy = (double)freq_index(ky, a.py) / ((double)a.py * pl.dy);
+    const double fx = (double)freq_index(kx, a.px) / ((double)a.px * pl.dx);
+    double2 e = make_double2(0.0, 0.0);
+    if (!(a.bandlimit && (fabs(fy - pl.bl_y0) > pl.bl_hy || fabs(fx - pl.bl_x0) > pl.bl_hx))) {
+      const double gy = fy - a.ky0, gx = fx - a.kx0;
+      const double kern = 1.0 - q * q * (gy * gy + gx * gx);
+      if (kern >= 0.0 || a.remove_evanescent)
+        e = make_double2(K * sqrt(kern > 0.0 ? kern : 0.0), 1.0);
+      else
+        e = make_double2(K * sqrt(-kern), 2.0);
+    }
+    tab[i] = e;
+  }
+}
+
+template <int NY, int MODE>
+__global__ void __launch_bounds__(ColCfg<NY>::THREADS, 1)
+    k_fluor_cols(const float2* __restrict__ T, float2* __restrict__ T2, Prop2DArgs a, int nb,
+                 const double2* __restrict__ tab, double inv_dz) {
   using C = ColCfg<NY>;
   constexpr int V = C::V, LEN = C::LEN;
   extern __shared__ float2 sm[];
@@ -70,44 +108,68 @@ __global__ void __launch_bounds__(ColCfg<NY>::THREADS, ColCfg<NY>::MINB)
   const int team = threadIdx.x / C::LPV, lane = threadIdx.x % C::LPV;
   float2* s = tile + team * LEN;
   const int tiles_x = (a.px + V - 1) / V;
-  const cx_plane pl = a.planes[0];
-  for (int t = blockIdx.x; t < tiles_x; t += gridDim.x) {
-    const int x0 = t * V;
+  const long total = (long)tiles_x * (MODE == FLUOR_BACK ? nb : 1);
+  const float scale = 1.0f / ((float)a.py * (float)a.px);
+  for (long t = blockIdx.x; t < total; t += gridDim.x) {
+    const int q = (int)(t / tiles_x);
+    const int x0 = (int)(t % tiles_x) * V;
     __syncthreads();
     load_col_tile<V, LEN>(tile, T, a.px, x0, a.px, 0, a.py, [](int r) { return r; });
     __syncthreads();
     const int kx = x0 + team;
     const bool valid = kx < a.px;
     auto load1 = [&](int n) -> float2 { return s[pad_idx(n)]; };
-    auto store1 = [&](int k, float2 v, int) {
-      s[pad_idx(k)] = valid ? cscale(cmul(v, prop_kernel(k, kx, a, pl)), scale) : v;
-    };
-    team_fft_ex<NY, false, false, true, C::LPV, C::CTA>(s, tw, lane, team, load1, store1);
+    if constexpr (MODE == FLUOR_SPEC) {
+      auto store1 = [&](int k, float2 v, int) { s[pad_idx(k)] = v; };
+      team_fft<NY, false, C::LPV, C::CTA>(s, tw, lane, team, load1, store1);
+    } else {
+      const cx_plane pl = a.planes[q];
+      const double m = rint(fabs(pl.z) * inv_dz);  // the plane's multiple of dz
+      const bool neg = pl.z < 0.0;
+      auto loadh = [&](int n) -> float2 {
+        const float2 v = s[pad_idx(n)];
+        if (!valid) return v;
+        const double2 e = tab[(size_t)n * a.px + kx];
+        float2 h = make_float2(0.f, 0.f);
+        if (e.y == 1.0) {
+          h = expi_reduced(neg ? -m * e.x : m * e.x);
+        } else if (e.y == 2.0) {
+          h = make_float2(expf((float)(-m * e.x)), 0.f);
+        }
+        return cscale(cmul(v, h), scale);
+      };
+      auto store1 = [&](int k, float2 v, int) { s[pad_idx(k)] = v; };
+      team_fft_ex<NY, true, true, false, C::LPV, C::CTA>(s, tw, lane, team, loadh, store1);
+    }
     __syncthreads();
-    for (int idx = threadIdx.x; idx < a.py * V; idx += blockDim.x) {
+    const int r0 = MODE == FLUOR_SPEC ? 0 : a.out_y0;
+    const int nr = MODE == FLUOR_SPEC ? a.py : a.out_ny;
+    for (int idx = threadIdx.x; idx < nr * V; idx += blockDim.x) {
       const int r = idx / V, c = idx % V, x = x0 + c;
-      if (x < a.px) T2[(size_t)r * a.px + x] = tile[c * LEN + pad_idx(r)];
+      if (x < a.px) T2[((size_t)q * nr + r) * a.px + x] = tile[c * LEN + pad_idx(r0 + r)];
     }
   }
 }
 
-template <int NY>
-static cx_status launch_carry(const float2* T, float2* T2, const Prop2DArgs& a, float scale, cudaStream_t st) {
+template <int NY, int MODE>
+static cx_status launch_fluor_cols(const float2* T, float2* T2, const Prop2DArgs& a, int nb, const double2* tab,
+                                   double inv_dz, cudaStream_t st) {
   using C = ColCfg<NY>;
-  auto k = k_fluor_carry<NY>;
+  auto k = k_fluor_cols<NY, MODE>;
   CX_CUDA_TRY(set_smem(k, C::SMEM));
-  const long tiles = (a.px + C::V - 1) / C::V;
-  k<<<persistent_grid(k, C::THREADS, C::SMEM, tiles), C::THREADS, C::SMEM, st>>>(T, T2, a, scale);
+  const long units = (long)((a.px + C::V - 1) / C::V) * (MODE == FLUOR_BACK ? nb : 1);
+  k<<<persistent_grid(k, C::THREADS, C::SMEM, units), C::THREADS, C::SMEM, st>>>(T, T2, a, nb, tab, inv_dz);
   CX_LAUNCH_CHECK();
   return CX_OK;
 }
 
-static cx_status dispatch_carry(int n, const float2* T, float2* T2, const Prop2DArgs& a, float scale,
-                                cudaStream_t st) {
+static cx_status dispatch_fluor_cols(int n, int mode, const float2* T, float2* T2, const Prop2DArgs& a, int nb,
+                                     const double2* tab, double inv_dz, cudaStream_t st) {
   switch (n) {
-#define CX_CASE_(N) \
-  case N:           \
-    return launch_carry<N>(T, T2, a, scale, st);
+#define CX_CASE_(N)                                                                              \
+  case N:                                                                                        \
+    return mode == FLUOR_SPEC ? launch_fluor_cols<N, FLUOR_SPEC>(T, T2, a, nb, tab, inv_dz, st)  \
+                              : launch_fluor_cols<N, FLUOR_BACK>(T, T2, a, nb, tab, inv_dz, st);
     CX_FOR_EACH_SIZE(CX_CASE_)
 #undef CX_CASE_
   }
@@ -115,12 +177,20 @@ static cx_status dispatch_carry(int n, const float2* T, float2* T2, const Prop2D
   return CX_ERR_UNSUPPORTED;
 }
 
+// the carry, in place: V = scale U H(z) (an elementwise product with the spectrum)
+__global__ void k_fluor_carry(float2* __restrict__ U, Prop2DArgs a, const cx_plane* pl, float scale) {
+  const long total = (long)a.py * a.px;
+  const cx_plane p = *pl;
+  for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < total; i += (long)gridDim.x * blockDim.x)
+    U[i] = cscale(cmul(U[i], prop_kernel((int)(i / a.px), (int)(i % a.px), a, p)), scale);
+}
+
 static constexpr int kFluorChunk = 32;  // backward planes per column / row pass
 
 struct FluorPlan {
   int py, px, D, S, CH;
   Prop2DArgs col;
-  size_t off_h, off_f, off_v, off_ph, off_t2, off_o, total;
+  size_t off_h, off_f, off_v, off_ph, off_t2, off_o, off_tab, total;
 };
 
 static size_t fal(size_t b) { return (b + 255) & ~(size_t)255; }
@@ -173,7 +243,8 @@ static cx_status fluor_plan(const cx_fluor_desc* d, FluorPlan* p) {
   p->off_ph = p->off_v + fal(field);
   p->off_t2 = p->off_ph + fal(sizeof(float) * (size_t)p->D * d->ny * d->nx);
   p->off_o = p->off_t2 + fal(sizeof(float2) * (size_t)p->CH * d->ny * p->px);
-  p->total = p->off_o + fal(sizeof(float2) * (size_t)p->CH * d->ny * d->nx);
+  p->off_tab = p->off_o + fal(sizeof(float2) * (size_t)p->CH * d->ny * d->nx);
+  p->total = p->off_tab + fal(sizeof(double2) * (size_t)p->py * p->px);
   return ensure_twiddles(&a.twg);
 }
 
@@ -251,6 +322,7 @@ extern "C" cx_status cx_fluorescent_multislice(const cx_fluor_desc* d, const voi
   float* ph_buf = reinterpret_cast<float*>(w + p.off_ph);
   float2* T2 = reinterpret_cast<float2*>(w + p.off_t2);
   float2* O = reinterpret_cast<float2*>(w + p.off_o);
+  double2* tab = reinterpret_cast<double2*>(w + p.off_tab);
   std::vector<cx_plane> host(p.D + 2);
   if ((s = fluor_upload_planes(d, p, planes, host.data(), st)) != CX_OK) return s;
   // the slice propagator table H(dz), FP64 sin / cos
@@ -259,7 +331,11 @@ extern "C" cx_status cx_fluorescent_multislice(const cx_fluor_desc* d, const voi
     a.precise = 1;
     k_fluor_fill_h<<<grid_for((long)p.py * p.px), 256, 0, st>>>(Hf, a, planes);
     CX_LAUNCH_CHECK();
+    k_fluor_ptable<<<grid_for((long)p.py * p.px), 256, 0, st>>>(tab, p.col, planes);
+    CX_LAUNCH_CHECK();
   }
+  // plane multiples of |dz| (dz = 0: every plane's propagator is 1, m = 0)
+  const double inv_dz = d->dz != 0.0 ? 1.0 / std::fabs(d->dz) : 0.0;
   const long plane = (long)d->ny * d->nx;
   const long stack = plane * p.D;
   CX_CUDA_TRY(cudaMemsetAsync(out, 0, sizeof(float) * (size_t)stack, st));
@@ -316,7 +392,8 @@ extern "C" cx_status cx_fluorescent_multislice(const cx_fluor_desc* d, const voi
       a.H = Hf;
       if ((s = dispatch_cols(p.py, F, F, a, st)) != CX_OK) return s;
     }
-    // backward planes, cropped, in chunks of CH
+    // U = FFT_y(state) once, into V; then the backward planes, cropped, in chunks of CH
+    if ((s = dispatch_fluor_cols(p.py, FLUOR_SPEC, F, V, p.col, 1, tab, inv_dz, st)) != CX_OK) return s;
     for (int c0 = 0; c0 < p.D; c0 += p.CH) {
       const int nb = p.D - c0 < p.CH ? p.D - c0 : p.CH;
       Prop2DArgs b = p.col;
@@ -326,16 +403,15 @@ extern "C" cx_status cx_fluorescent_multislice(const cx_fluor_desc* d, const voi
       b.out_ny = d->ny;
       b.out_x0 = d->pad;
       b.out_nx = d->nx;
-      if ((s = dispatch_cols(p.py, F, T2, b, st)) != CX_OK) return s;
+      if ((s = dispatch_fluor_cols(p.py, FLUOR_BACK, V, T2, b, nb, tab, inv_dz, st)) != CX_OK) return s;
       if ((s = dispatch_rows_inv(p.px, T2, O, b, st)) != CX_OK) return s;
       k_fluor_accumulate<<<grid_for((long)nb * plane), 256, 0, st>>>(O, out, c0, nb, p.D, plane, w_sample);
       CX_LAUNCH_CHECK();
     }
     if (smp + 1 < p.S) {
-      // carry: U H_b^D = px FFT_y(state) H(-D dz), a spectrum in field layout
-      Prop2DArgs c = p.col;
-      c.planes = planes + p.D + 1;
-      if ((s = dispatch_carry(p.py, F, V, c, (float)p.px, st)) != CX_OK) return s;
+      // carry: U H_b^D = px FFT_y(state) H(-D dz), a spectrum in field layout (in place in V)
+      k_fluor_carry<<<grid_for((long)p.py * p.px), 256, 0, st>>>(V, p.col, planes + p.D + 1, (float)p.px);
+      CX_LAUNCH_CHECK();
     }
   }
   return CX_OK;
