@@ -19,6 +19,7 @@
 // planes share (k_fluor_cols computes it once per sample).
 #include <cmath>
 #include <cstdint>
+#include <type_traits>
 #include <vector>
 
 #include "multislice.cuh"
@@ -63,7 +64,34 @@ __global__ void k_fluor_fill_h(float2* __restrict__ H, Prop2DArgs a, const cx_pl
 //               [pad, pad + ny) into T2 (q, ny, px) -- the column pass of
 //               k_prop_cols without its forward transform, which is the same
 //               for every plane
-enum FluorCol { FLUOR_SPEC = 0, FLUOR_BACK = 1 };
+//   FLUOR_FWD:  the forward slice step, FFT_y x H(dz) (table) IFFT_y / (py px), in place
+enum FluorCol { FLUOR_SPEC = 0, FLUOR_BACK = 1, FLUOR_FWD = 2 };
+
+// Narrow column tiles for the single-plane forward pass: at least 4 columns
+// (32-byte row segments), whole warps for exact-size teams, at most the
+// column configuration's width.  At 384^2 the column configuration's
+// 16-column tiles give 24 CTAs; 4-column tiles give 96.
+template <int N>
+struct NarrowColCfg {
+  using C0 = ColCfg<N>;
+  static constexpr bool CTA = C0::CTA;
+  static constexpr int LPV = C0::LPV;
+  static constexpr int pick() {
+    int v = 4;
+    while (CTA && (v * LPV) % 32 != 0) v *= 2;
+    return v < C0::V ? v : C0::V;
+  }
+  static constexpr int V = pick();
+  static_assert(!CTA || (V * LPV) % 32 == 0, "exact-size teams must fill whole warps");
+  static constexpr int LEN = col_len(N, V);
+  static constexpr int THREADS = V * LPV;
+  static constexpr int TW = tw_len(N);
+  static constexpr int MINB = minb_for(THREADS);
+  static constexpr size_t SMEM = sizeof(float2) * ((size_t)TW + (size_t)V * LEN);
+};
+
+template <int NY, int MODE>
+using FluorColCfg = typename std::conditional<MODE == FLUOR_FWD, NarrowColCfg<NY>, ColCfg<NY>>::type;
 
 // no blocks-per-SM bound: the FP64 propagator in the staged load needs
 // about 90 registers, more than the column configuration's bound leaves
@@ -96,10 +124,10 @@ __global__ void k_fluor_ptable(double2* __restrict__ tab, Prop2DArgs a, const cx
 }
 
 template <int NY, int MODE>
-__global__ void __launch_bounds__(ColCfg<NY>::THREADS, 1)
-    k_fluor_cols(const float2* __restrict__ T, float2* __restrict__ T2, Prop2DArgs a, int nb,
-                 const double2* __restrict__ tab, double inv_dz) {
-  using C = ColCfg<NY>;
+__global__ void __launch_bounds__(FluorColCfg<NY, MODE>::THREADS, 1)
+    k_fluor_cols(const float2* T, float2* T2, Prop2DArgs a, int nb, const double2* __restrict__ tab,
+                 double inv_dz) {
+  using C = FluorColCfg<NY, MODE>;
   constexpr int V = C::V, LEN = C::LEN;
   extern __shared__ float2 sm[];
   float2* tw = sm;
@@ -122,6 +150,14 @@ __global__ void __launch_bounds__(ColCfg<NY>::THREADS, 1)
     if constexpr (MODE == FLUOR_SPEC) {
       auto store1 = [&](int k, float2 v, int) { s[pad_idx(k)] = v; };
       team_fft<NY, false, C::LPV, C::CTA>(s, tw, lane, team, load1, store1);
+    } else if constexpr (MODE == FLUOR_FWD) {
+      // H(dz) from the explicit table (a.H, FFT order)
+      auto store1 = [&](int k, float2 v, int) { s[pad_idx(k)] = valid ? cmul(v, a.H[(size_t)k * a.px + kx]) : v; };
+      team_fft<NY, false, C::LPV, C::CTA>(s, tw, lane, team, load1, store1);
+      team_barrier<C::LPV, C::CTA>(team);
+      auto load2 = [&](int n) -> float2 { return s[pad_idx(n)]; };
+      auto store2 = [&](int k, float2 v, int) { s[pad_idx(k)] = cscale(v, scale); };
+      team_fft<NY, true, C::LPV, C::CTA>(s, tw, lane, team, load2, store2);
     } else {
       const cx_plane pl = a.planes[q];
       const double m = rint(fabs(pl.z) * inv_dz);  // the plane's multiple of dz
@@ -142,8 +178,8 @@ __global__ void __launch_bounds__(ColCfg<NY>::THREADS, 1)
       team_fft_ex<NY, true, true, false, C::LPV, C::CTA>(s, tw, lane, team, loadh, store1);
     }
     __syncthreads();
-    const int r0 = MODE == FLUOR_SPEC ? 0 : a.out_y0;
-    const int nr = MODE == FLUOR_SPEC ? a.py : a.out_ny;
+    const int r0 = MODE == FLUOR_BACK ? a.out_y0 : 0;
+    const int nr = MODE == FLUOR_BACK ? a.out_ny : a.py;
     for (int idx = threadIdx.x; idx < nr * V; idx += blockDim.x) {
       const int r = idx / V, c = idx % V, x = x0 + c;
       if (x < a.px) T2[((size_t)q * nr + r) * a.px + x] = tile[c * LEN + pad_idx(r0 + r)];
@@ -154,7 +190,7 @@ __global__ void __launch_bounds__(ColCfg<NY>::THREADS, 1)
 template <int NY, int MODE>
 static cx_status launch_fluor_cols(const float2* T, float2* T2, const Prop2DArgs& a, int nb, const double2* tab,
                                    double inv_dz, cudaStream_t st) {
-  using C = ColCfg<NY>;
+  using C = FluorColCfg<NY, MODE>;
   auto k = k_fluor_cols<NY, MODE>;
   CX_CUDA_TRY(set_smem(k, C::SMEM));
   const long units = (long)((a.px + C::V - 1) / C::V) * (MODE == FLUOR_BACK ? nb : 1);
@@ -168,8 +204,9 @@ static cx_status dispatch_fluor_cols(int n, int mode, const float2* T, float2* T
   switch (n) {
 #define CX_CASE_(N)                                                                              \
   case N:                                                                                        \
-    return mode == FLUOR_SPEC ? launch_fluor_cols<N, FLUOR_SPEC>(T, T2, a, nb, tab, inv_dz, st)  \
-                              : launch_fluor_cols<N, FLUOR_BACK>(T, T2, a, nb, tab, inv_dz, st);
+    return mode == FLUOR_SPEC  ? launch_fluor_cols<N, FLUOR_SPEC>(T, T2, a, nb, tab, inv_dz, st) \
+           : mode == FLUOR_FWD ? launch_fluor_cols<N, FLUOR_FWD>(T, T2, a, nb, tab, inv_dz, st)  \
+                               : launch_fluor_cols<N, FLUOR_BACK>(T, T2, a, nb, tab, inv_dz, st);
     CX_FOR_EACH_SIZE(CX_CASE_)
 #undef CX_CASE_
   }
@@ -390,7 +427,7 @@ extern "C" cx_status cx_fluorescent_multislice(const cx_fluor_desc* d, const voi
       a.planes = planes;
       a.kernel = CX_KERNEL_EXPLICIT;
       a.H = Hf;
-      if ((s = dispatch_cols(p.py, F, F, a, st)) != CX_OK) return s;
+      if ((s = dispatch_fluor_cols(p.py, FLUOR_FWD, F, F, a, 1, tab, inv_dz, st)) != CX_OK) return s;
     }
     // U = FFT_y(state) once, into V; then the backward planes, cropped, in chunks of CH
     if ((s = dispatch_fluor_cols(p.py, FLUOR_SPEC, F, V, p.col, 1, tab, inv_dz, st)) != CX_OK) return s;
