@@ -35,10 +35,12 @@ struct PolArgs {
 // ---------------------------------------------------------------------------
 // rows: a CTA holds R rows x 3 components (one team each)
 // ---------------------------------------------------------------------------
+// about 96 threads (3 teams of 32 lanes at Q = 512): a 256-row field then runs
+// 256 CTAs instead of 64
 template <int Q>
 struct PolRowCfg {
   static constexpr int LPV = Plan<Q>::LPV;
-  static constexpr int R0 = 128 / LPV > 0 ? 128 / LPV : 1;
+  static constexpr int R0 = 32 / LPV > 0 ? 32 / LPV : 1;
   static constexpr int R = LPV >= 32 && R0 > 5 ? 5 : R0;  // named barriers 1..15
   static constexpr int TEAMS = 3 * R;
   static constexpr int THREADS = TEAMS * LPV;
