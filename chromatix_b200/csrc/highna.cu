@@ -30,10 +30,10 @@ __global__ void k_high_na_pupil(HighNaArgs a, const float2* __restrict__ u, floa
     const double sz = sqrt(fmax(1.0 - a.c_s * (fy * fy + fx * fx), 0.0));
     double dr = 0.0, di = 0.0;
     if (sz != 0.0) {
-      double s, c;
-      sincos(a.kf * sz, &s, &c);
-      dr = c / sz;
-      di = s / sz;
+      // FP64 phase k f sz reduced mod 2 pi in FP64, FP32 sin / cos
+      const float2 e = expi_reduced(a.kf * sz);
+      dr = (double)e.x / sz;
+      di = (double)e.y / sz;
     }
     if (a.P == 1) {
       const float2 v = u[i];

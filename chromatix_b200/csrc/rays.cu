@@ -24,11 +24,9 @@ __global__ void k_ray_chirp(const float2* in, float2* out, const cx_plane* __res
     const long b = pix / ((long)nx * ny);
     const cx_plane pl = planes[b * W + w];
     const double gy = ((double)y - 0.5 * ny) * pl.dy + oy, gx = ((double)x - 0.5 * nx) * pl.dx + ox;
+    // FP64 phase (it reaches 1e3..1e5 rad), reduced mod 2 pi in FP64, FP32 sin / cos
     const double ph = coef_n * 6.283185307179586476925286766559 / pl.wavelength * (gy * gy + gx * gx);
-    double s, c;
-    sincos(ph, &s, &c);
-    const float2 v = in[i];
-    out[i] = make_float2((float)(v.x * c - v.y * s), (float)(v.x * s + v.y * c));
+    out[i] = cmul(in[i], expi_reduced(ph));
   }
 }
 
