@@ -1,8 +1,9 @@
 """The oracle's ray transfer (functional/rays.py:102-154) pinned by known
 answers (the reference has no test of it): free space with unit
-magnification is the Fresnel transfer-function propagation; every ABCD
-system conserves the field's summed intensity; the ABCD products follow the
-reference's matrices (no GPU)."""
+magnification is the Fresnel transfer-function propagation; a Gaussian beam
+through a lens and a focal length of free space focuses to the paraxial
+waist lambda f / (pi w0); every ABCD system conserves the field's summed
+intensity; the ABCD products follow the reference's matrices (no GPU)."""
 
 import numpy as np
 
@@ -40,3 +41,18 @@ def test_abcd_matrices():
     # a thick plano-convex lens of zero thickness acts as a thin lens of power (n_l - n_m) / (R n_m)
     M = R.compute_plano_convex_spherical_lens_abcd(100.0, 50.0, 0.0, 1.5, 1.0)
     np.testing.assert_allclose(M, [[1, 0], [-0.5 / 50.0, 1]], atol=1e-15)
+
+
+def test_gaussian_beam_focuses_to_its_paraxial_waist():
+    # lambda B / M = 50 um <= N dx^2 = 64 um: the transfer function is sampled without aliasing
+    N, dx, lam, f, w0 = 256, 0.5, 0.5, 100.0, 10.0
+    g = (np.arange(N) - N / 2) * dx
+    Y, X = np.meshgrid(g, g, indexing="ij")
+    field = O.field_build(np.exp(-(X**2 + Y**2) / w0**2), dx, lam)
+    lens = np.array([[1.0, 0.0], [-1 / f, 1.0]])
+    free = np.array([[1.0, f], [0.0, 1.0]])
+    out = O.ray_transfer(field, free @ lens, 1.0)
+    I = np.abs(out.u) ** 2
+    w = 2 * np.sqrt((I * X**2).sum() / I.sum())  # I ~ exp(-2 r^2 / w^2): <x^2> = w^2 / 4
+    assert abs(w - lam * f / (np.pi * w0)) < 1e-3 * w
+    np.testing.assert_allclose(I.sum(), (np.abs(field.u) ** 2).sum(), rtol=1e-12)
