@@ -257,8 +257,18 @@ def gpu_arm(args):
         }
         if not args.no_cpu_baseline and world == 1:
             line["cpu_baseline"] = cpu_baseline(args.cpu_sample_z)
-        if args.accuracy:
-            line["rel_err_vs_fp64"] = accuracy_check(dev)
+        if not args.no_accuracy:
+            # outside the timed region: 2 of the 64 planes against the FP64 oracle
+            line["accuracy"] = accuracy_check(dev)
+            line["rel_err_vs_fp64"] = line["accuracy"]["rel_err_vs_fp64"]
+    if not args.no_serve:
+        # a short Poisson stream of the serving configuration (latency beside throughput)
+        serve = run_serve_stream(dev, rank, world, dist, args.rate, args.headline_serve_seconds)
+        if rank == 0:
+            line["latency_ms"] = serve["latency_ms"]
+            line["serve"] = {k: serve[k] for k in ("value", "unit", "requests", "achieved_req_s", "seconds",
+                                                   "rate_req_s", "offered_device_load")}
+    if rank == 0:
         print(json.dumps(line), flush=True)
     if dist:
         dist.destroy_process_group()
@@ -319,7 +329,9 @@ def dominant_kernel_time(dev, z, phase_d, dx):
 
 
 def accuracy_check(dev):
-    """Relative L2 error of the CUDA PSF vs the FP64 oracle on 2 defocus planes."""
+    """Relative L2 error of the CUDA PSF vs the FP64 oracle on 2 defocus planes
+    (the first and the last), and the reference-order float32 restatement's
+    own error on the same planes."""
     import torch
 
     import chromatix_b200.functional as cf
@@ -333,8 +345,12 @@ def accuracy_check(dev):
     I = f.intensity.cpu().numpy()
     O.set_fft_workers(os.cpu_count())
     o = O.ff_lens(O.phase_change(O.objective_point_source((N, N), dx, spec, zz, F_OBJ, N_MED, NA), phase),
-                  F_TUBE, N_MED)
-    return float(O.rel_l2(I, o.intensity))
+                  F_TUBE, N_MED).intensity
+    r = O.ff_lens(O.phase_change(O.objective_point_source((N, N), dx, spec, zz, F_OBJ, N_MED, NA, prec=O.REF32),
+                                 phase), F_TUBE, N_MED).intensity
+    return {"rel_err_vs_fp64": float(O.rel_l2(I, o)), "rel_err_vs_ref32": float(O.rel_l2(I, r)),
+            "ref32_rel_err_vs_fp64": float(O.rel_l2(r, o)), "planes": "z[0], z[63] (2 of 64), 3 wavelengths",
+            "tolerance": 1e-5}
 
 
 # ---------------------------------------------------------------------------
@@ -695,28 +711,18 @@ SERVE_SIDES = (256, 512, 1024, 2048)
 SERVE_OPS = ("asm", "transfer", "czt_zoom")
 
 
-def serve_arm(args):
-    """Poisson arrivals (mean ``--rate`` req/s) of requests with side N in
+def run_serve_stream(dev, rank, world, dist, rate, seconds, accuracy=False):
+    """Poisson arrivals (mean ``rate`` req/s) of requests with side N in
     {256, 512, 1024, 2048}, op in {ASM, Fresnel transfer, CZT zoom to 512^2},
     z ~ U[1, 500] um, lambda ~ U[0.4, 0.7] um, n = 1.33, dx = 0.3 um,
     random-phase fields resident in HBM, mode "same" with pad N/2, 60 GB
-    admission budget; p50 / p99 latency from arrival to completion."""
+    admission budget; p50 / p99 latency from arrival to completion.  Every
+    rank serves its own stream (replicas); the statistics are the max (time,
+    latency) or sum (pixels) over ranks."""
     import torch
 
     from chromatix_b200.serving import PropagationServer, Request, percentile
 
-    rank = int(os.environ.get("RANK", "0"))
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
-    torch.cuda.set_device(local)
-    dev = torch.device("cuda", local)
-    dist = None
-    if world > 1:
-        import datetime
-
-        import torch.distributed as dist
-
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300), device_id=dev)
     rng = np.random.default_rng(1000 + rank)
     fields = {}
     for N in SERVE_SIDES:
@@ -748,15 +754,16 @@ def serve_arm(args):
                 srv.submit(Request(op=op, u=fields[N][1], dx=0.3, z=250.0, wavelength=0.55, zoom=1.7))
                 srv.drain()
             service[f"{op}/{N}"] = round(srv.gpu_ms[op] / 3, 4)
-    offered_load = args.rate * float(np.mean(list(service.values()))) / 1e3
+    offered_load = rate * float(np.mean(list(service.values()))) / 1e3
     for c in (srv.host_s, srv.gpu_ms, srv.batches):
         c.clear()
     if dist:
         dist.barrier()
-    n_req = max(1, int(args.rate * args.serve_seconds))
-    arrivals = np.cumsum(rng.exponential(1.0 / args.rate, n_req))
+    n_req = max(1, int(rate * seconds))
+    arrivals = np.cumsum(rng.exponential(1.0 / rate, n_req))
     reqs = []
-    with ClockSampler(local) as clk:
+    keep = []
+    with ClockSampler(int(dev.index or 0)) as clk:
         t0 = time.perf_counter()
         i = 0
         while i < n_req or srv.busy:
@@ -765,7 +772,10 @@ def serve_arm(args):
                 reqs.append(srv.submit(make(t0 + arrivals[i])))
                 i += 1
             for r in srv.step():
-                r.out = None  # the client consumes the result: its buffer returns to the pool
+                if accuracy and len(keep) < 6 and r.side <= 1024:
+                    keep.append(r)  # checked against the FP64 oracle after the stream
+                else:
+                    r.out = None  # the client consumes the result: its buffer returns to the pool
         torch.cuda.synchronize(dev)
         t_end = time.perf_counter()
     elapsed = t_end - t0
@@ -779,26 +789,74 @@ def serve_arm(args):
         dist.all_reduce(sm, op=dist.ReduceOp.SUM)
         stats = [float(mx[0]), float(sm[1]), float(mx[2]), float(mx[3])]
     elapsed, px, p50, p99 = stats
+    by_op = {op: round(percentile([r.latency * 1e3 for r in reqs if r.op == op], 99), 3) for op in SERVE_OPS}
+    by_side = {str(N): round(percentile([r.latency * 1e3 for r in reqs if r.side == N], 99), 3) for N in SERVE_SIDES}
+    out = {"value": round(px / elapsed / 1e6, 1), "unit": "Mpx/s", "requests": n_req * world,
+           "achieved_req_s": round(n_req * world / elapsed, 1), "seconds": seconds, "rate_req_s": rate,
+           "elapsed_s": elapsed, "n_req": n_req,
+           "latency_ms": {"p50": round(p50, 3), "p99": round(p99, 3), "mean": round(float(lat.mean()), 3),
+                          "p99_by_op": by_op, "p99_by_side": by_side},
+           "service_ms_alone": service, "offered_device_load": round(offered_load, 3),
+           "launch_host_ms_by_op": {k: round(v * 1e3, 1) for k, v in srv.host_s.items()},
+           "device_ms_by_op": {k: round(v, 1) for k, v in srv.gpu_ms.items()},
+           "batches_by_op": dict(srv.batches), "clocks": clk.summary()}
+    if accuracy and rank == 0:
+        out["rel_err_vs_fp64"] = serve_accuracy(keep)
+    return out
+
+
+def serve_accuracy(reqs):
+    """Relative L2 error of served results against the FP64 oracle (worst of
+    the requests kept from the stream)."""
+    from oracle import chromatix_oracle as O
+
+    O.set_fft_workers(os.cpu_count())
+    worst = {}
+    for r in reqs:
+        u = r.u.cpu().numpy()
+        f = O.field_build(u, r.dx, r.wavelength)
+        N = r.side
+        if r.op == "asm":
+            ref = O.asm_propagate(f, r.z, r.n, N // 2, mode="same").u
+        elif r.op == "transfer":
+            ref = O.transfer_propagate(f, r.z, r.n, N // 2, mode="same").u
+        else:
+            ref = O.asm_propagate(f, r.z, r.n, N // 2, output_dx=np.array([r.dx / r.zoom] * 2),
+                                  output_shape=r.out_shape).u
+        e = float(O.rel_l2(r.out.cpu().numpy(), ref))
+        worst[r.op] = max(worst.get(r.op, 0.0), e)
+    return {k: float(f"{v:.3g}") for k, v in worst.items()}
+
+
+def serve_arm(args):
+    """The serving configuration as its own line (see run_serve_stream)."""
+    import torch
+
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300), device_id=dev)
+    r = run_serve_stream(dev, rank, world, dist, args.rate, args.serve_seconds, accuracy=not args.no_accuracy)
     if rank == 0:
-        by_op = {op: round(percentile([r.latency * 1e3 for r in reqs if r.op == op], 99), 3) for op in SERVE_OPS}
         line = {
-            "metric": "served Mpx/s (p50/p99 request latency)", "value": round(px / elapsed / 1e6, 1),
-            "unit": "Mpx/s", "n_gpus": world, "steps": n_req, "warmup": len(SERVE_OPS) * len(SERVE_SIDES),
-            "ms_per_step": round(elapsed * 1e3 / n_req, 4), "higher_is_better": True, "scaling": "weak",
+            "metric": "served Mpx/s (p50/p99 request latency)", "value": r["value"],
+            "unit": "Mpx/s", "n_gpus": world, "steps": r["n_req"], "warmup": len(SERVE_OPS) * len(SERVE_SIDES),
+            "ms_per_step": round(r["elapsed_s"] * 1e3 / r["n_req"], 4), "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "c64", "data": "synthetic (seeded Poisson stream)",
             "config": {"workload": "serving stream: Poisson arrivals of ASM / Fresnel transfer / CZT-zoom requests, "
                                    "N in {256,512,1024,2048}, pad N/2, mode same, 60 GB admission budget",
                        "rate_req_s": args.rate, "seconds": args.serve_seconds, "streams": 4, "max_batch": 32,
                        "parallelism": f"replicas x{world}" if world > 1 else "single GPU"},
-            "latency_ms": {"p50": round(p50, 3), "p99": round(p99, 3), "mean": round(float(lat.mean()), 3),
-                           "p99_by_op": by_op},
-            "requests": n_req * world, "achieved_req_s": round(n_req * world / elapsed, 1),
-            "service_ms_alone": service, "offered_device_load": round(offered_load, 3),
-            "launch_host_ms_by_op": {k: round(v * 1e3, 1) for k, v in srv.host_s.items()},
-            "device_ms_by_op": {k: round(v, 1) for k, v in srv.gpu_ms.items()},
-            "batches_by_op": dict(srv.batches),
-            "clocks": clk.summary(),
         }
+        line.update({k: v for k, v in r.items() if k not in ("value", "unit", "elapsed_s", "n_req")})
         print(json.dumps(line), flush=True)
     if dist:
         dist.destroy_process_group()
@@ -866,6 +924,20 @@ def reference_arm(args):
     print(json.dumps(line), flush=True)
 
 
+def launch_ranks(n: int) -> int:
+    """``--gpus N`` without a launcher: start N ranks of this script with
+    torch.distributed.run on this node (one process per GPU) and return its
+    exit status."""
+    import socket
+
+    with socket.socket() as sk:
+        sk.bind(("127.0.0.1", 0))
+        port = sk.getsockname()[1]
+    cmd = [sys.executable, "-m", "torch.distributed.run", "--nnodes=1", f"--nproc-per-node={n}",
+           "--master-addr", "127.0.0.1", "--master-port", str(port), os.path.abspath(__file__)] + sys.argv[1:]
+    return subprocess.call(cmd)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -874,7 +946,11 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--cpu-sample-z", type=int, default=2)
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--accuracy", action="store_true", help="also report the error vs the FP64 oracle")
+    ap.add_argument("--no-accuracy", action="store_true",
+                    help="skip the error against the FP64 oracle (computed outside the timed region)")
+    ap.add_argument("--no-serve", action="store_true", help="psf: skip the short serving stream (latency_ms)")
+    ap.add_argument("--headline-serve-seconds", type=float, default=1.0,
+                    help="psf: length of the serving stream whose latency the headline line reports")
     ap.add_argument("--workload", default="psf",
                     choices=["psf", "serve", "psf_published", "rescaled_published", "microscope_published", "asm",
                              "multislice", "mbs", "next_rows"],
@@ -890,6 +966,8 @@ def main():
     args = ap.parse_args()
     if args.warmup < 3 and args.impl == "ours":
         args.warmup = 3
+    if args.gpus > 1 and "WORLD_SIZE" not in os.environ:
+        sys.exit(launch_ranks(args.gpus))
     if args.impl == "reference":
         reference_arm(args)
     elif args.workload == "serve":

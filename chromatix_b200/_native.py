@@ -100,6 +100,20 @@ class cx_prop2d_desc(ctypes.Structure):
         ("n_medium", c_double),
         ("ky0", c_double),
         ("kx0", c_double),
+        ("conj_kernel", c_int32),
+        ("crop_y", c_int32),
+        ("crop_x", c_int32),
+        ("reserved", c_int32),
+    ]
+
+
+class cx_ew_desc(ctypes.Structure):
+    _fields_ = [
+        ("n_batch", ctypes.c_int64),
+        ("ny", c_int32),
+        ("nx", c_int32),
+        ("n_wv", c_int32),
+        ("map_batched", c_int32),
     ]
 
 
@@ -147,6 +161,32 @@ _SIGS = {
         [ctypes.POINTER(cx_prop2d_desc), c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_size_t, c_void_p],
     ),
     "cx_fill_propagator": (c_int32, [ctypes.POINTER(cx_prop2d_desc), c_void_p, c_void_p, c_void_p]),
+    "cx_phase_change": (c_int32, [ctypes.POINTER(cx_ew_desc), c_void_p, c_void_p, c_void_p, c_void_p, c_void_p]),
+    "cx_phase_change_adjoint": (
+        c_int32,
+        [ctypes.POINTER(cx_ew_desc), c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p],
+    ),
+    "cx_thin_sample": (
+        c_int32, [ctypes.POINTER(cx_ew_desc), c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p]
+    ),
+    "cx_thin_sample_adjoint": (
+        c_int32,
+        [ctypes.POINTER(cx_ew_desc), c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p,
+         c_void_p, c_void_p],
+    ),
+    "cx_intensity_adjoint": (c_int32, [c_void_p, ctypes.c_int64, c_int32, c_void_p, c_void_p, c_void_p, c_void_p]),
+    "cx_pad": (
+        c_int32,
+        [ctypes.POINTER(cx_ew_desc), c_int32, c_int32, ctypes.c_float, ctypes.c_float, c_void_p, c_void_p, c_void_p],
+    ),
+    "cx_plane_wave": (
+        c_int32,
+        [ctypes.POINTER(cx_ew_desc), c_void_p, c_double, c_double, c_double, c_double, c_void_p, c_void_p],
+    ),
+    "cx_pupil": (
+        c_int32,
+        [ctypes.POINTER(cx_ew_desc), c_int32, c_void_p, c_double, c_double, c_void_p, c_void_p, c_void_p],
+    ),
     "cx_psf_workspace_size": (c_int32, [ctypes.POINTER(cx_psf_desc), ctypes.POINTER(c_size_t)]),
     "cx_psf_4f": (
         c_int32,
@@ -256,3 +296,18 @@ def copy_stream(device):
 def require_cuda(t, what="tensor"):
     if not t.is_cuda:
         raise ValueError(f"{what} must live on a CUDA device (the library has no CPU path)")
+
+
+def wants_grad(*tensors) -> bool:
+    """True when autograd is recording and one of ``tensors`` requires a gradient."""
+    torch = torch_mod()
+    return torch.is_grad_enabled() and any(isinstance(t, torch.Tensor) and t.requires_grad for t in tensors)
+
+
+def refuse_grad(op: str, *tensors) -> None:
+    """Raise instead of silently cutting the autograd graph: ``op`` writes its
+    result through the native library and has no adjoint here."""
+    if wants_grad(*tensors):
+        raise NotImplementedError(
+            f"{op}: no gradient is implemented for this operation (its result would be cut from the autograd "
+            "graph); call it on detached inputs or under torch.no_grad()")

@@ -61,6 +61,55 @@ def _broadcast_dx(dx, n_wv: int) -> np.ndarray:
     return out
 
 
+_INTENSITY_FN = None
+
+
+def _intensity_launch(u, C: int, dens, out_shape):
+    torch = _torch()
+    out = torch.empty(out_shape, dtype=torch.float32, device=u.device)
+    nat.check(nat.lib().cx_intensity(nat.ptr(u), out.numel(), C, nat.ptr(dens), nat.ptr(out),
+                                     nat.stream_handle(u.device)))
+    return out
+
+
+def _intensity_fn():
+    """autograd Function of the native intensity readout; the backward is
+    ``cx_intensity_adjoint`` (g_u = 2 density g_I u)."""
+    global _INTENSITY_FN
+    if _INTENSITY_FN is None:
+        torch = _torch()
+
+        class _Intensity(torch.autograd.Function):
+            @staticmethod
+            def forward(ctx, u, C, dens, out_shape):
+                ctx.C = C
+                ctx.save_for_backward(u, dens)
+                return _intensity_launch(u, C, dens, out_shape)
+
+            @staticmethod
+            def backward(ctx, g):
+                u, dens = ctx.saved_tensors
+                g = g.to(torch.float32).contiguous()
+                gu = torch.empty_like(u)
+                nat.check(nat.lib().cx_intensity_adjoint(nat.ptr(u), g.numel(), ctx.C, nat.ptr(dens), nat.ptr(g),
+                                                         nat.ptr(gu), nat.stream_handle(u.device)))
+                return gu, None, None, None
+
+        _INTENSITY_FN = _Intensity
+    return _INTENSITY_FN
+
+
+def _intensity(u, C: int, density, out_shape):
+    """sum_c density[c] |u[..., c]|^2 over C interleaved channels (native)."""
+    torch = _torch()
+    nat.require_cuda(u, "Field.u")
+    u = u.to(torch.complex64).contiguous()
+    dens = nat.upload(np.asarray(density, np.float64).reshape(-1), u.device)
+    if nat.wants_grad(u):
+        return _intensity_fn().apply(u, C, dens, tuple(out_shape))
+    return _intensity_launch(u, C, dens, tuple(out_shape))
+
+
 class Field:
     """Base of the scalar field containers (core/field.py:49-531)."""
 
@@ -198,18 +247,13 @@ class Field:
     @property
     def intensity(self):
         """|u|^2 (mono) or sum_wv density |u|^2 (core/field.py:656-665, 735-740),
-        computed by the native readout kernel."""
-        torch = _torch()
-        nat.require_cuda(self.u, "Field.u")
-        u = self.u.contiguous()
+        computed by the native readout kernel (differentiable: its adjoint is
+        ``cx_intensity_adjoint``)."""
+        u = self.u
         W = self.n_wv if self.chromatic else 1
         out_shape = u.shape[:-1] if self.chromatic else u.shape
-        out = torch.empty(out_shape, dtype=torch.float32, device=u.device)
-        dens = nat.upload(np.asarray(self.spectrum.density, np.float64) if self.chromatic else np.ones(1), u.device)
-        n_pix = out.numel()
-        nat.check(nat.lib().cx_intensity(nat.ptr(u), n_pix, W, nat.ptr(dens), nat.ptr(out),
-                                         nat.stream_handle(u.device)))
-        return out
+        dens = np.asarray(self.spectrum.density, np.float64) if self.chromatic else np.ones(1)
+        return _intensity(u, W, dens, out_shape)
 
     def intensity_to(self, out):
         """Write the intensity into ``out`` (a float32 tensor of the intensity's
@@ -399,14 +443,7 @@ class VectorField(Field):
     def intensity(self):
         """sum over the components of |u|^2 (core/field.py:808-811), by the
         native readout kernel."""
-        torch = _torch()
-        nat.require_cuda(self.u, "Field.u")
-        u = self.u.contiguous()
-        out = torch.empty(u.shape[:-1], dtype=torch.float32, device=u.device)
-        dens = nat.upload(np.ones(3), u.device)
-        nat.check(nat.lib().cx_intensity(nat.ptr(u), out.numel(), 3, nat.ptr(dens), nat.ptr(out),
-                                         nat.stream_handle(u.device)))
-        return out
+        return _intensity(self.u, 3, np.ones(3), self.u.shape[:-1])
 
     @property
     def power(self):
@@ -437,36 +474,70 @@ class ChromaticVectorField(Field):
     def intensity(self):
         """sum over wavelengths (spectral density) and components of |u|^2
         (core/field.py:889-894), by the native readout kernel."""
+        return _intensity(self.u, 3 * self.spectrum.size,
+                          np.repeat(np.asarray(self.spectrum.density, np.float64), 3), self.u.shape[:-2])
+
+
+def _channels(field: "Field") -> int:
+    """Interleaved innermost values per pixel (wavelengths x vector components)."""
+    return int(np.prod(field.u.shape[field.ndim + field.spatial_dims[1] + 1:]))
+
+
+def _pad_native(u, batch: int, ny: int, nx: int, C: int, py: int, px: int, cval: complex):
+    torch = _torch()
+    d = nat.cx_ew_desc(n_batch=batch, ny=ny, nx=nx, n_wv=C, map_batched=0)
+    out = torch.empty((batch, ny + 2 * py, nx + 2 * px, C), dtype=torch.complex64, device=u.device)
+    nat.check(nat.lib().cx_pad(d, py, px, float(cval.real), float(cval.imag), nat.ptr(u.contiguous()), nat.ptr(out),
+                               nat.stream_handle(u.device)))
+    return out
+
+
+_PAD_FN = None
+
+
+def _pad_fn():
+    """autograd Function of the native pad: the gradient is the crop."""
+    global _PAD_FN
+    if _PAD_FN is None:
         torch = _torch()
-        nat.require_cuda(self.u, "Field.u")
-        u = self.u.contiguous()
-        W = self.spectrum.size
-        out = torch.empty(u.shape[:-2], dtype=torch.float32, device=u.device)
-        dens = nat.upload(np.repeat(np.asarray(self.spectrum.density, np.float64), 3), u.device)
-        nat.check(nat.lib().cx_intensity(nat.ptr(u), out.numel(), 3 * W, nat.ptr(dens), nat.ptr(out),
-                                         nat.stream_handle(u.device)))
-        return out
+
+        class _Pad(torch.autograd.Function):
+            @staticmethod
+            def forward(ctx, u, dims, cval):
+                batch, ny, nx, C, py, px = dims
+                ctx.dims = dims
+                return _pad_native(u, batch, ny, nx, C, py, px, cval)
+
+            @staticmethod
+            def backward(ctx, g):
+                batch, ny, nx, C, py, px = ctx.dims
+                return g[:, py:py + ny, px:px + nx, :].contiguous(), None, None
+
+        _PAD_FN = _Pad
+    return _PAD_FN
 
 
 def pad(field: Field, pad_width, cval: float = 0.0) -> Field:
-    """``pad`` (core/field.py:534-549): zero (or ``cval``) padding of y and x."""
-    torch = _torch()
+    """``pad`` (core/field.py:534-549): constant (``cval``) padding of y and x,
+    one pass of the native pad kernel (``cx_pad``)."""
     if isinstance(pad_width, (int, np.integer)):
         pad_width = (int(pad_width), int(pad_width))
     py, px = int(pad_width[0]), int(pad_width[1])
     u = field.u
-    inner = field.chromatic or field.vectorial  # wavelength / component axis innermost
+    nat.require_cuda(u, "Field.u")
+    ny, nx = field.spatial_shape
+    C = _channels(field)
     shape = tuple(u.shape)
-    if field.chromatic and field.vectorial:
-        u = u.reshape(shape[:-2] + (shape[-2] * shape[-1],))  # (wv, 3) as one inner axis
-    if inner:
-        u = u.movedim(-1, -3)
-    u = torch.nn.functional.pad(u, (px, px, py, py), value=complex(cval) if cval else 0.0)
-    if inner:
-        u = u.movedim(-3, -1).contiguous()
-    if field.chromatic and field.vectorial:
-        u = u.reshape(u.shape[:-1] + shape[-2:])
-    return field.replace(u=u)
+    lead = shape[: field.ndim + field.spatial_dims[0]]
+    batch = int(np.prod(lead)) if lead else 1
+    cv = complex(cval)
+    dims = (batch, ny, nx, C, py, px)
+    if nat.wants_grad(u):
+        out = _pad_fn().apply(u.to(_torch().complex64), dims, cv)
+    else:
+        out = _pad_native(u.to(_torch().complex64), batch, ny, nx, C, py, px, cv)
+    inner = shape[field.ndim + field.spatial_dims[1] + 1:]
+    return field.replace(u=out.reshape(lead + (ny + 2 * py, nx + 2 * px) + inner))
 
 
 def crop(field: Field, crop_width) -> Field:

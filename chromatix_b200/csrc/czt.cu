@@ -62,6 +62,25 @@ static cx_status czt_args(const cx_czt_desc* d, CztArgs* a) {
   a->lw = std::log(std::hypot(d->w_re, d->w_im));
   a->modN = d->mod_n;
   a->scale = d->scale;
+  if (d->adjoint) {
+    // x'[j] = sum_k conj(scale M_k a^-j w^jk) y'[k], M_k = w^(-N k) a^N (or 1):
+    // a Bluestein transform of m inputs onto n outputs with w' = conj(w),
+    // input factor conj(M_k) conj(w)^(k^2/2) (a' = conj(w)^N), output factor
+    // conj(w)^(j^2/2) conj(a)^(-j) [conj(a)^N] scale
+    const double ta = a->ta, la = a->la, tw = a->tw, lw = a->lw;
+    const double N = d->mod_n >= 0 ? (double)d->mod_n : 0.0;
+    a->n = d->m;
+    a->m = d->n;
+    a->tw = -tw;
+    a->lw = lw;
+    a->ta = -N * tw;
+    a->la = N * lw;
+    a->modN = -1;
+    a->gb_l = -la;
+    a->gb_t = ta;
+    a->c_l = N * la;
+    a->c_t = -N * ta;
+  }
   return CX_OK;
 }
 

@@ -37,6 +37,9 @@ struct CztArgs {
   //          * sum_j x[j] mag_in exp(i pi c_in (j - j0_in)^2) f[k + s - j],
   // with the finite chirp filter f in chat (see the filter kernel)
   int kind = 0;
+  // kind 0: an extra output factor exp(k (gb_l + i gb_t) + c_l + i c_t) -- the
+  // a-dependent part of the adjoint transform (zero for the forward one)
+  double gb_l = 0.0, gb_t = 0.0, c_l = 0.0, c_t = 0.0;
   double c_in = 0.0, j0_in = 0.0, mag_in = 1.0;
   double c_out = 0.0, dx_out = 0.0, k0_out = 0.0, org_out = 0.0, mag_out = 1.0;
 };
@@ -64,8 +67,8 @@ __device__ __forceinline__ float2 czt_out_chirp(const CztArgs& a, int k) {
     return make_float2((float)a.mag_out * e.x, (float)a.mag_out * e.y);
   }
   const double kk = (double)k;
-  double lm = a.lw * 0.5 * kk * kk;
-  double ph = a.tw * 0.5 * kk * kk;
+  double lm = a.lw * 0.5 * kk * kk + a.gb_l * kk + a.c_l;
+  double ph = a.tw * 0.5 * kk * kk + a.gb_t * kk + a.c_t;
   if (a.modN >= 0) {
     const double N = (double)a.modN;
     lm += -a.lw * N * kk + a.la * N;

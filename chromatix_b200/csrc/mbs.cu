@@ -94,3 +94,25 @@ extern "C" cx_status cx_mbs_iterate(const cx_mbs_desc* d, const void* eps, const
   if ((s = mbs_middle(a, st)) != CX_OK) return s;
   return mbs_dispatch_z(a.Z, MBS_ZI_STEP, a, st);
 }
+
+extern "C" cx_status cx_mbs_forward(const cx_mbs_desc* d, const void* eps, const void* x, void* out, void* workspace,
+                                    size_t workspace_bytes, cx_stream_t stream) {
+  MbsArgs a;
+  cx_status s = mbs_args(d, &a);
+  if (s != CX_OK) return s;
+  if (!eps || !x || !out || !workspace || workspace_bytes < sizeof(float2) * 3 * (size_t)a.vox || x == out) {
+    set_error("invalid MBS forward arguments (x and out must differ)");
+    return CX_ERR_INVALID;
+  }
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  a.eps = static_cast<const float2*>(eps);
+  a.x = static_cast<const float2*>(x);
+  a.prec_y = static_cast<const float2*>(x);  // unused when forward_only
+  a.buf = static_cast<float2*>(workspace);
+  a.x_new = static_cast<float2*>(out);
+  a.acc = nullptr;
+  a.forward_only = 1;
+  if ((s = mbs_dispatch_z(a.Z, MBS_Z_DISC, a, st)) != CX_OK) return s;
+  if ((s = mbs_middle(a, st)) != CX_OK) return s;
+  return mbs_dispatch_z(a.Z, MBS_ZI_STEP, a, st);
+}

@@ -37,6 +37,7 @@ struct MbsArgs {
   float2* x_new;      // output (3 planes)
   double* acc;        // [0] sum |x_new - x|^2, [1] sum |x_new|^2
   const float2* twg;
+  int forward_only = 0;  // MBS_ZI_STEP: write prec_forward(x) = -V(G + x) instead of the update (no sums)
 };
 
 __device__ __forceinline__ float2 mbs_disc(const MbsArgs& a, float2 v, float2 e) {
@@ -96,6 +97,10 @@ __global__ void __launch_bounds__(RowCfg<NZ>::THREADS, RowCfg<NZ>::MINB) k_mbs_z
             const float2 xo = xrow[k];
             const float2 gk = cscale(g, inv_n);
             const float2 vx = mbs_disc(a, cadd(gk, xo), se[k]);
+            if (a.forward_only) {
+              orow[k] = make_float2(-vx.x, -vx.y);
+              return;
+            }
             const float2 xn = cadd(cadd(prow[k], vx), xo);
             orow[k] = xn;
             const float2 dd = csub(xn, xo);
@@ -127,7 +132,7 @@ __global__ void __launch_bounds__(RowCfg<NZ>::THREADS, RowCfg<NZ>::MINB) k_mbs_z
       red[1][wid] = nsum;
     }
     __syncthreads();
-    if (threadIdx.x == 0) {
+    if (threadIdx.x == 0 && a.acc) {
       double d0 = 0.0, n0 = 0.0;
       for (int w = 0; w < nw; ++w) {
         d0 += red[0][w];

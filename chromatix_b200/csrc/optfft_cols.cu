@@ -39,9 +39,11 @@ __global__ void __launch_bounds__(ColCfg<NY>::THREADS, ColCfg<NY>::MINB) k_opt_c
       if (hcol && kx < a.px) v = cmul(v, hcol[(size_t)k * a.px]);
       if (pl.conj) v = cconj(v);
       v = cmul(post, v);
-      if (pl.chirp_out != 0.0) {
+      if (pl.chirp_out != 0.0 || pl.pupil_out_r2 > 0.0) {
         const double ry = pl.dy_out * ((double)row - 0.5 * a.py) + pl.oy;
-        v = cmul(v, chirp(pl.chirp_out, ry, rx));
+        if (pl.chirp_out != 0.0) v = cmul(v, chirp(pl.chirp_out, ry, rx));
+        // output-grid pupil (the adjoint of the input pupil of ff_lens)
+        if (pl.pupil_out_r2 > 0.0 && ry * ry + rx * rx > pl.pupil_out_r2) v = make_float2(0.f, 0.f);
       }
       s[pad_idx(k)] = v;
     };

@@ -41,16 +41,22 @@ static cx_status make_args(const cx_prop2d_desc* d, Prop2DArgs* a) {
   a->W = d->n_wv;
   a->n_in_planes = d->n_in_planes;
   a->n_out_planes = d->n_out_planes;
+  if (d->crop_y < 0 || d->crop_x < 0 || 2 * d->crop_y >= a->py || 2 * d->crop_x >= a->px ||
+      (d->mode_same && (d->crop_y || d->crop_x))) {
+    set_error("invalid crop (%d, %d) of the padded grid %dx%d (crop applies to mode_same = 0 only)", d->crop_y,
+              d->crop_x, a->py, a->px);
+    return CX_ERR_INVALID;
+  }
   if (d->mode_same) {
     a->out_y0 = d->pad_y;
     a->out_ny = d->ny;
     a->out_x0 = d->pad_x;
     a->out_nx = d->nx;
   } else {
-    a->out_y0 = 0;
-    a->out_ny = a->py;
-    a->out_x0 = 0;
-    a->out_nx = a->px;
+    a->out_y0 = d->crop_y;
+    a->out_ny = a->py - 2 * d->crop_y;
+    a->out_x0 = d->crop_x;
+    a->out_nx = a->px - 2 * d->crop_x;
   }
   a->kernel = d->kernel;
   a->precision = d->precision;
@@ -61,7 +67,7 @@ static cx_status make_args(const cx_prop2d_desc* d, Prop2DArgs* a) {
   a->kx0 = d->kx0;
   a->na_f2 = -1.0;
   a->precise = 0;
-  a->conj_h = 0;
+  a->conj_h = d->conj_kernel ? 1 : 0;
   a->twg = nullptr;
   a->planes = nullptr;
   a->H = nullptr;

@@ -23,7 +23,7 @@ struct Prop2DArgs {
   double n_med, ky0, kx0;
   double na_f2;  // >= 0: k-space NA mask |f|^2 <= na_f2 (samples.py:276-280); < 0: none
   int precise;   // 1: FP64 sin/cos (tables reused many times); 0: FP64 reduction + hardware sin/cos
-  int conj_h;    // 1: use conj(H) (explicit propagator tables, adjoint passes)
+  int conj_h;    // 1: use conj(H) (adjoint passes; any kernel kind)
   const cx_plane* planes;
   const float2* H;
   const float2* twg;  // device twiddle tables (ensure_twiddles)
@@ -175,11 +175,12 @@ __device__ __forceinline__ bool outside_na(int ky, int kx, const Prop2DArgs& a, 
 
 __device__ __forceinline__ float2 prop_kernel(int ky, int kx, const Prop2DArgs& a, const cx_plane& pl) {
   if (outside_na(ky, kx, a, pl)) return make_float2(0.f, 0.f);
-  if (a.kernel == CX_KERNEL_EXPLICIT) {
-    const float2 h = a.H[((size_t)pl.h_plane * a.py + ky) * a.px + kx];
-    return a.conj_h ? cconj(h) : h;
-  }
-  return a.precision == CX_PREC_REF32 ? prop_kernel_ref32(ky, kx, a, pl) : prop_kernel_accurate(ky, kx, a, pl);
+  float2 h;
+  if (a.kernel == CX_KERNEL_EXPLICIT)
+    h = a.H[((size_t)pl.h_plane * a.py + ky) * a.px + kx];
+  else
+    h = a.precision == CX_PREC_REF32 ? prop_kernel_ref32(ky, kx, a, pl) : prop_kernel_accurate(ky, kx, a, pl);
+  return a.conj_h ? cconj(h) : h;
 }
 
 // --------------------------------------------------------------------------

@@ -7,6 +7,8 @@ meanings.  The fixed-point iteration runs in fused CUDA passes
 HBM, the 3D FFTs are split into z / y / x passes with the preconditioner's
 scattering potential and Green's-function division fused in, and the
 convergence test reads FP64 residual sums accumulated on the device.
+``use_bicgstab=True`` runs BiCGStab on the same operator (``cx_mbs_forward``)
+with native FP64-accumulated inner products and fused vector updates.
 """
 
 from __future__ import annotations
@@ -42,6 +44,12 @@ def _lib():
         L.cx_mbs_precondition.argtypes = [P, V, V, V, V, nat.c_size_t, V]
         L.cx_mbs_iterate.restype = nat.c_int32
         L.cx_mbs_iterate.argtypes = [P, V, V, V, V, V, V, nat.c_size_t, V]
+        L.cx_mbs_forward.restype = nat.c_int32
+        L.cx_mbs_forward.argtypes = [P, V, V, V, V, nat.c_size_t, V]
+        L.cx_cvec_dot.restype = nat.c_int32
+        L.cx_cvec_dot.argtypes = [V, V, nat.ctypes.c_int64, V, V]
+        L.cx_cvec_lincomb.restype = nat.c_int32
+        L.cx_cvec_lincomb.argtypes = [nat.ctypes.c_int64, nat.ctypes.POINTER(nat.c_double), V, V, V, V, V, V]
         _SIG = True
     return L
 
@@ -199,15 +207,17 @@ def solve(sample: Sample, source: Source, initial_E=None, maxiter: int = 1000, t
           shift=None, scale=None, return_info: bool = False):
     """Electric field of the scattering problem (solver.py:101-146).
 
-    Fixed-point iteration ``x <- prec_y - prec_forward(x) + x``.  Stops when
+    ``use_bicgstab=True``: BiCGStab on ``prec_forward(x) = prec_y``
+    (solver.py:143-144), stopping at ||r|| <= tol ||prec_y|| (``rtol`` in
+    place of tol when given) -- see ``_bicgstab``.  Otherwise the
+    fixed-point iteration ``x <- prec_y - prec_forward(x) + x``.  Stops when
     ``||x_{k+1} - x_k||_2 <= tol`` (the absolute rule of jaxopt's
     FixedPointIteration, which the reference uses) or, if ``rtol`` is given,
     when ``||x_{k+1} - x_k|| / ||x_{k+1}|| < rtol``; both norms are FP64 sums
     accumulated on the device.  Returns E of shape (X, Y, Z, 3).
     """
     torch = nat.torch_mod()
-    if use_bicgstab:
-        raise NotImplementedError("BiCGStab is not part of this build; the fixed-point iteration is")
+    nat.refuse_grad("modified Born series solve", sample.permittivity, source.field)
     eps = sample.permittivity.to(torch.complex64).contiguous()
     nat.require_cuda(eps, "permittivity")
     X, Y, Z = eps.shape
@@ -231,6 +241,13 @@ def solve(sample: Sample, source: Source, initial_E=None, maxiter: int = 1000, t
     num_scale = float(prec_y.abs().max().item())
     prec_y /= num_scale
     x = prec_y.clone() if initial_E is None else _planes(initial_E.to(torch.complex64)) / num_scale
+    if use_bicgstab:
+        x, info = _bicgstab(L, d, eps, prec_y, x, ws, ws_b.value, st, maxiter, tol, rtol)
+        E = (x * num_scale).movedim(0, -1).contiguous()
+        if return_info:
+            info.update({"shift": shift, "scale": scale, "num_scale": num_scale})
+            return E, info
+        return E
     x_new = torch.empty_like(x)
     acc = torch.zeros(2, dtype=torch.float64, device=dev)
     acc_h = torch.zeros(2, dtype=torch.float64).pin_memory()
@@ -257,3 +274,103 @@ def solve(sample: Sample, source: Source, initial_E=None, maxiter: int = 1000, t
         return E, {"iterations": it, "residual_abs": res_abs, "residual_rel": res_rel, "shift": shift,
                    "scale": scale, "num_scale": num_scale, "loop_ms": ev0.elapsed_time(ev1)}
     return E
+
+
+class _Krylov:
+    """Native complex vector algebra on the device (FP64 inner products read
+    back through page-locked memory)."""
+
+    def __init__(self, L, n, dev, st):
+        torch = nat.torch_mod()
+        self.L, self.n, self.st = L, int(n), st
+        self.acc = torch.zeros(4, dtype=torch.float64, device=dev)
+        self.nrm = torch.zeros(1, dtype=torch.float64, device=dev)
+        self.host = torch.zeros(4, dtype=torch.float64).pin_memory()
+        self.ev = torch.cuda.Event()
+
+    def _read(self, t, k):
+        self.host[:k].copy_(t[:k], non_blocking=True)
+        self.ev.record()
+        self.ev.synchronize()
+        return self.host[:k].numpy().copy()
+
+    def dot(self, x, y):
+        """(sum conj(x) y, sum |x|^2, sum |y|^2) in FP64."""
+        nat.check(self.L.cx_cvec_dot(nat.ptr(x), nat.ptr(y), self.n, nat.ptr(self.acc), self.st))
+        a = self._read(self.acc, 4)
+        return complex(a[0], a[1]), float(a[2]), float(a[3])
+
+    def comb(self, out, c0, x, c1, y, c2=0.0, z=None, norm=False):
+        """out = c0 x + c1 y [+ c2 z]; returns sum |out|^2 when ``norm``."""
+        c = (nat.c_double * 6)(complex(c0).real, complex(c0).imag, complex(c1).real, complex(c1).imag,
+                               complex(c2).real, complex(c2).imag)
+        nat.check(self.L.cx_cvec_lincomb(self.n, c, nat.ptr(x), nat.ptr(y), nat.ptr(z), nat.ptr(out),
+                                         nat.ptr(self.nrm) if norm else None, self.st))
+        return float(self._read(self.nrm, 1)[0]) if norm else None
+
+
+def _bicgstab(L, d, eps, b, x, ws, ws_bytes, st, maxiter, tol, rtol):
+    """BiCGStab on prec_forward(x) = prec_y (solver.py:143-144).
+
+    The reference calls jax.scipy.sparse.linalg.bicgstab (unpreconditioned:
+    the series' preconditioning is already in prec_forward); this is the same
+    published algorithm (van der Vorst, SIAM J. Sci. Stat. Comput. 13, 1992),
+    with its stopping rule ||r|| <= max(tol ||b||, 0) (``rtol`` overrides
+    tol when given) and its breakdown exits (rho = 0, alpha = 0 or
+    omega = 0 end the loop).  Matrix-vector products are ``cx_mbs_forward``;
+    inner products accumulate in FP64 on the device."""
+    torch = nat.torch_mod()
+    n = x.numel()
+    K = _Krylov(L, n, x.device, st)
+
+    def A(v, out):
+        nat.check(L.cx_mbs_forward(d, nat.ptr(eps), nat.ptr(v), nat.ptr(out), nat.ptr(ws), ws_bytes, st))
+
+    q = torch.empty_like(x)
+    A(x, q)
+    r = torch.empty_like(x)
+    rs = K.comb(r, 1.0, b, -1.0, q, norm=True)
+    _, bs, _ = K.dot(b, b)
+    thr2 = (rtol if rtol is not None else tol) ** 2 * bs
+    rhat = r.clone()
+    p, q = r.clone(), r.clone()
+    s_, t = torch.empty_like(x), torch.empty_like(x)
+    rho = alpha = omega = 1.0 + 0j
+    it, status = 0, "maxiter"
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ev0.record()
+    while rs > thr2 and it < maxiter:
+        rho_new, _, _ = K.dot(rhat, r)
+        if rho_new == 0:
+            status = "breakdown (rho = 0)"
+            break
+        beta = rho_new / rho * alpha / omega
+        K.comb(p, 1.0, r, beta, p, -beta * omega, q)  # p = r + beta (p - omega q)
+        A(p, q)
+        rq, _, _ = K.dot(rhat, q)
+        alpha = rho_new / rq
+        ss = K.comb(s_, 1.0, r, -alpha, q, norm=True)  # s = r - alpha q
+        it += 1
+        if ss < thr2:  # early exit: x + alpha p already meets the tolerance
+            K.comb(x, 1.0, x, alpha, p)
+            r, s_ = s_, r
+            rs = ss
+            break
+        A(s_, t)
+        ts, tt, _ = K.dot(t, s_)
+        omega = ts / tt
+        K.comb(x, 1.0, x, alpha, p, omega, s_)  # x += alpha p + omega s
+        rs = K.comb(r, 1.0, s_, -omega, t, norm=True)  # r = s - omega t
+        rho = rho_new
+        if alpha == 0 or omega == 0:
+            status = "breakdown (alpha or omega = 0)"
+            break
+    else:
+        status = "converged" if rs <= thr2 else "maxiter"
+    if rs <= thr2:
+        status = "converged"
+    ev1.record()
+    ev1.synchronize()
+    res_rel = math.sqrt(rs / bs) if bs > 0 else float("inf")
+    return x, {"iterations": it, "residual_abs": math.sqrt(rs), "residual_rel": res_rel, "status": status,
+               "solver": "bicgstab", "loop_ms": ev0.elapsed_time(ev1)}

@@ -19,7 +19,7 @@ FFT_PLANE_DTYPE = np.dtype(
         ("pre_re", "<f8"), ("pre_im", "<f8"), ("post_re", "<f8"), ("post_im", "<f8"),
         ("chirp_in", "<f8"), ("chirp_out", "<f8"), ("dy_in", "<f8"), ("dx_in", "<f8"),
         ("dy_out", "<f8"), ("dx_out", "<f8"), ("oy", "<f8"), ("ox", "<f8"), ("pupil_r2", "<f8"),
-        ("in_plane", "<i4"), ("conj", "<i4"),
+        ("in_plane", "<i4"), ("conj", "<i4"), ("pupil_out_r2", "<f8"),
     ]
 )
 
@@ -64,12 +64,92 @@ def _optfft_norms(field: Field, z: float, n: float, shape):
     return out
 
 
+def _optfft_adjoint_planes(planes: np.ndarray) -> np.ndarray:
+    """Plane table of the adjoint optical FFT.
+
+    Per plane the forward map is out = c_out post C(F(pre C(c_in pupil u)))
+    (C = conjugation when ``conj``, F the centred DFT).  Its adjoint is the same
+    kernel with the grids' roles swapped: input chirp conj(c_out), output chirp
+    conj(c_in), the pupil moved to the output grid, ``conj`` flipped, and
+    pre' = post, post' = conj(pre) (conj = 0) or pre' = conj(post), post' = pre
+    (conj = 1)."""
+    a = planes.copy()
+    pre = planes["pre_re"] + 1j * planes["pre_im"]
+    post = planes["post_re"] + 1j * planes["post_im"]
+    c = planes["conj"].astype(bool)
+    pre2 = np.where(c, np.conj(post), post)
+    post2 = np.where(c, pre, np.conj(pre))
+    a["pre_re"], a["pre_im"] = pre2.real, pre2.imag
+    a["post_re"], a["post_im"] = post2.real, post2.imag
+    a["chirp_in"], a["chirp_out"] = -planes["chirp_out"], -planes["chirp_in"]
+    a["dy_in"], a["dx_in"] = planes["dy_out"], planes["dx_out"]
+    a["dy_out"], a["dx_out"] = planes["dy_in"], planes["dx_in"]
+    a["pupil_out_r2"] = np.where(planes["pupil_r2"] >= 0, np.maximum(planes["pupil_r2"], 1e-300), -1.0)
+    a["pupil_r2"] = np.where(planes["pupil_out_r2"] > 0, planes["pupil_out_r2"], -1.0)
+    a["conj"] = 1 - planes["conj"]
+    a["in_plane"] = np.arange(planes.size)
+    return a
+
+
+class _OptPlan:
+    """One ``cx_optical_fft`` call; ``adjoint()`` gives the plan of its gradient."""
+
+    def __init__(self, desc, planes, in_shape, out_shape):
+        self.desc, self.planes, self.in_shape, self.out_shape = desc, planes, tuple(in_shape), tuple(out_shape)
+
+    def adjoint(self) -> "_OptPlan":
+        d = cx_optfft_desc.from_buffer_copy(self.desc)
+        Py, Px = d.ny + 2 * d.pad_y, d.nx + 2 * d.pad_x
+        d.ny, d.nx = Py - 2 * d.crop_y, Px - 2 * d.crop_x
+        d.pad_y, d.pad_x, d.crop_y, d.crop_x = d.crop_y, d.crop_x, d.pad_y, d.pad_x
+        d.n_in_planes = d.n_out_planes
+        return _OptPlan(d, _optfft_adjoint_planes(self.planes), self.out_shape, self.in_shape)
+
+
+def _launch_optfft(plan: _OptPlan, u):
+    torch = nat.torch_mod()
+    L = _sigs(nat.lib())
+    dev = u.device
+    ws_b = nat.c_size_t(0)
+    nat.check(L.cx_optfft_workspace_size(plan.desc, ws_b))
+    u_out = torch.empty(plan.out_shape, dtype=torch.complex64, device=dev)
+    ws = nat.workspace(ws_b.value, dev)
+    planes_dev = nat.to_device_bytes(plan.planes, dev)
+    u_in = u.contiguous()
+    nat.check(L.cx_optical_fft(plan.desc, nat.ptr(planes_dev), nat.ptr(u_in), nat.ptr(u_out), nat.ptr(ws),
+                               ws_b.value, nat.stream_handle(dev)))
+    return u_out
+
+
+_OPT_FN = None
+
+
+def _opt_fn():
+    """torch autograd Function over ``cx_optical_fft``; the backward is the
+    adjoint optical FFT (the gradient jax.grad takes through
+    functional/convenience.py:9-59 and lenses.py:64-95)."""
+    global _OPT_FN
+    if _OPT_FN is None:
+        torch = nat.torch_mod()
+
+        class _OptFFT(torch.autograd.Function):
+            @staticmethod
+            def forward(ctx, u, plan):
+                ctx.plan = plan
+                return _launch_optfft(plan, u)
+
+            @staticmethod
+            def backward(ctx, g):
+                return _launch_optfft(ctx.plan.adjoint(), g.to(torch.complex64)), None
+
+        _OPT_FN = _OptFFT
+    return _OPT_FN
+
+
 def run_optfft(field: Field, z: float, n: float, pad_width=(0, 0), crop_width=(0, 0), post=1.0 + 0j,
                chirp_in=None, chirp_out=None, pupil_D=None, precision=None):
     """Launch the chirped optical FFT; returns (u_out, du (wv, 2))."""
-    torch = nat.torch_mod()
     nat.require_cuda(field.u, "Field.u")
-    L = _sigs(nat.lib())
     prec = precision or config.get_precision()
     py_, px_ = pad_width
     cy, cx = crop_width
@@ -101,22 +181,20 @@ def run_optfft(field: Field, z: float, n: float, pad_width=(0, 0), crop_width=(0
                 p["pupil_r2"] = r * r
             else:
                 p["pupil_r2"] = -1.0
+            p["pupil_out_r2"] = -1.0
             p["in_plane"] = q
             p["conj"] = conj
     d = cx_optfft_desc()
     d.ny, d.nx, d.pad_y, d.pad_x, d.crop_y, d.crop_x = ny, nx, py_, px_, cy, cx
     d.n_wv, d.n_in_planes, d.n_out_planes = W, nb * W, nb * W
     d.precision = config.precision_code(prec)
-    ws_b = nat.c_size_t(0)
-    nat.check(L.cx_optfft_workspace_size(d, ws_b))
     oy, ox = Py - 2 * cy, Px - 2 * cx
     out_shape = tuple(B) + (oy, ox) + ((W,) if field.chromatic else ())
-    u_out = torch.empty(out_shape, dtype=torch.complex64, device=field.device)
-    ws = nat.workspace(ws_b.value, field.device)
-    planes_dev = nat.to_device_bytes(planes, field.device)
-    u_in = field.u.contiguous()
-    nat.check(L.cx_optical_fft(d, nat.ptr(planes_dev), nat.ptr(u_in), nat.ptr(u_out), nat.ptr(ws), ws_b.value,
-                               nat.stream_handle(field.device)))
+    plan = _OptPlan(d, planes, tuple(field.u.shape), out_shape)
+    if nat.wants_grad(field.u):
+        u_out = _opt_fn().apply(field.u, plan)
+    else:
+        u_out = _launch_optfft(plan, field.u)
     du = np.stack([nm[2] for nm in norms])
     return u_out, du
 

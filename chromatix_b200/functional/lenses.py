@@ -95,6 +95,7 @@ def high_na_ff_lens(field: Field, f, n, NA, output_shape=None, output_dx=None) -
 
     torch = nat.torch_mod()
     field = materialize(field)
+    nat.refuse_grad("high_na_ff_lens", field.u)
     if field.chromatic:
         raise NotImplementedError("high_na_ff_lens takes a single-wavelength field")
     nat.require_cuda(field.u, "field.u")

@@ -105,12 +105,111 @@ def _plan_planes(field: Field, zs, zshape, py, px, shift_yx=(0.0, 0.0), bandlimi
     return planes, out_batch, nb_in, nb_out
 
 
-def _run_prop2d(field: Field, kernel: int, zs, zshape, n, pad_width, kykx=(0.0, 0.0), shift_yx=(0.0, 0.0),
-                remove_evanescent=False, bandlimit=False, mode="full", H=None, h_index=None, precision=None):
+class _PropPlan:
+    """One ``cx_prop2d`` call: descriptor, plane table, input and output shapes.
+
+    ``adjoint()`` returns the plan of the gradient: the same fused passes with
+    conj(H) (= H(-z) for the transfer and ASM kernels), reading the output
+    gradient plane by plane; zero padding becomes a crop.  Output planes that
+    share an input (z broadcast over the field batch) are summed afterwards."""
+
+    def __init__(self, desc, planes, in_shape, out_shape, chromatic: bool, H=None):
+        self.desc, self.planes, self.H = desc, planes, H
+        self.in_shape, self.out_shape, self.chromatic = tuple(in_shape), tuple(out_shape), bool(chromatic)
+
+    def adjoint(self) -> "_PropPlan":
+        d = nat.cx_prop2d_desc.from_buffer_copy(self.desc)
+        py, px = d.ny + 2 * d.pad_y, d.nx + 2 * d.pad_x
+        ny, nx = d.ny, d.nx
+        if not d.mode_same:
+            d.ny, d.nx = py - 2 * d.crop_y, px - 2 * d.crop_x
+            d.pad_y, d.pad_x, d.crop_y, d.crop_x = d.crop_y, d.crop_x, d.pad_y, d.pad_x
+        d.n_in_planes = d.n_out_planes
+        d.conj_kernel = 1 - d.conj_kernel
+        planes = self.planes.copy()
+        planes["in_plane"] = np.arange(planes.size)
+        spatial = 3 if self.chromatic else 2
+        out_batch = self.out_shape[: len(self.out_shape) - spatial]
+        adj_out = out_batch + (ny, nx) + ((d.n_wv,) if self.chromatic else ())
+        return _PropPlan(d, planes, self.out_shape, adj_out, self.chromatic, self.H)
+
+
+def _launch_prop2d(plan: _PropPlan, u_in):
     torch = nat.torch_mod()
+    L = nat.lib()
+    d = plan.desc
+    ws_bytes = nat.c_size_t(0)
+    nat.check(L.cx_prop2d_workspace_size(d, ws_bytes))
+    dev = u_in.device
+    u_in = u_in.contiguous()
+    u_out = torch.empty(plan.out_shape, dtype=torch.complex64, device=dev)
+    ws = nat.workspace(ws_bytes.value, dev)
+    planes_dev = nat.to_device_bytes(plan.planes, dev)
+    nat.check(L.cx_prop2d(d, nat.ptr(planes_dev), nat.ptr(u_in), nat.ptr(u_out), nat.ptr(plan.H), nat.ptr(ws),
+                          ws_bytes.value, nat.stream_handle(dev)))
+    return u_out
+
+
+_PROP_FN = None
+
+
+def _prop_fn():
+    """torch autograd Function over ``cx_prop2d``: forward the fused
+    propagation, backward the same kernels with the conjugate propagator (the
+    hand-written adjoint of functional/propagation.py:391-394, which the
+    reference obtains from jax.grad)."""
+    global _PROP_FN
+    if _PROP_FN is None:
+        torch = nat.torch_mod()
+
+        class _Prop2D(torch.autograd.Function):
+            @staticmethod
+            def forward(ctx, u, plan):
+                ctx.plan = plan
+                return _launch_prop2d(plan, u)
+
+            @staticmethod
+            def backward(ctx, g):
+                plan = ctx.plan
+                adj = plan.adjoint()
+                gu = _launch_prop2d(adj, g.to(torch.complex64))
+                return gu.sum_to_size(plan.in_shape), None
+
+        _PROP_FN = _Prop2D
+    return _PROP_FN
+
+
+def _apply_prop(plan: _PropPlan, u):
+    if plan.H is not None:
+        nat.refuse_grad("kernel_propagate (gradient with respect to the propagator)", plan.H)
+    if nat.wants_grad(u):
+        return _prop_fn().apply(u, plan)
+    return _launch_prop2d(plan, u)
+
+
+def _pad_const(field: Field, pad_width, cval):
+    """Field padded with the constant ``cval`` by the native pad kernel
+    (core/field.py:534-549); its gradient is the crop of the output gradient."""
+    from ..core.field import pad
+
+    return pad(field, pad_width, cval)
+
+
+def _run_prop2d(field: Field, kernel: int, zs, zshape, n, pad_width, kykx=(0.0, 0.0), shift_yx=(0.0, 0.0),
+                remove_evanescent=False, bandlimit=False, mode="full", H=None, h_index=None, precision=None,
+                cval=0.0):
     nat.require_cuda(field.u, "Field.u")
     prec = precision or config.get_precision()
     py_, px_ = _pad_tuple(pad_width)
+    crop = (0, 0)
+    if cval != 0 and (py_ or px_):
+        # explicit constant padding, then the padded field propagates without
+        # loader padding; "same" crops the padding off again
+        field = _pad_const(field, (py_, px_), cval)
+        if mode == "same":
+            crop = (py_, px_)
+            mode = "full"
+        py_, px_ = 0, 0
     ny, nx = field.spatial_shape
     py, px = ny + 2 * py_, nx + 2 * px_
     planes, out_batch, nb_in, nb_out = _plan_planes(field, zs, zshape, py, px, shift_yx, bandlimit, prec, h_index)
@@ -121,6 +220,7 @@ def _run_prop2d(field: Field, kernel: int, zs, zshape, n, pad_width, kykx=(0.0, 
     d.n_in_planes = nb_in * W
     d.n_out_planes = nb_out * W
     d.mode_same = 1 if mode == "same" else 0
+    d.crop_y, d.crop_x = crop
     d.kernel = kernel
     d.precision = config.precision_code(prec)
     d.remove_evanescent = int(bool(remove_evanescent))
@@ -128,19 +228,10 @@ def _run_prop2d(field: Field, kernel: int, zs, zshape, n, pad_width, kykx=(0.0, 
     d.n_medium = float(n)
     ky0, kx0 = np.asarray(kykx, dtype=np.float64).reshape(2)
     d.ky0, d.kx0 = float(ky0), float(kx0)
-    L = nat.lib()
-    ws_bytes = nat.c_size_t(0)
-    nat.check(L.cx_prop2d_workspace_size(d, ws_bytes))
-    dev = field.device
-    u_in = field.u.contiguous()
-    oy, ox = (ny, nx) if mode == "same" else (py, px)
+    oy, ox = (ny, nx) if mode == "same" else (py - 2 * crop[0], px - 2 * crop[1])
     out_shape = tuple(out_batch) + (oy, ox) + ((W,) if field.chromatic else ())
-    u_out = torch.empty(out_shape, dtype=torch.complex64, device=dev)
-    ws = nat.workspace(ws_bytes.value, dev)
-    planes_dev = nat.to_device_bytes(planes, dev)
-    nat.check(L.cx_prop2d(d, nat.ptr(planes_dev), nat.ptr(u_in), nat.ptr(u_out), nat.ptr(H), nat.ptr(ws),
-                          ws_bytes.value, nat.stream_handle(dev)))
-    return u_out
+    plan = _PropPlan(d, planes, tuple(field.u.shape), out_shape, field.chromatic, H)
+    return _apply_prop(plan, field.u)
 
 
 def _check_mode(mode):
@@ -170,13 +261,11 @@ def transfer_propagate(field: Field, z, n, pad_width, cval: float = 0, absorbing
         return rescaled_propagate(field, nat.CX_KERNEL_TRANSFER, z, n, pad_width, kykx=kykx, shift_yx=shift_yx,
                                   output_dx=output_dx, output_shape=output_shape, use_czt=use_czt, mode=mode,
                                   cval=cval, precision=precision)
-    if cval != 0:
-        raise NotImplementedError("non-zero cval padding is not supported by the fused loader")
     zs, _ = _z_array(z)
     # transfer_propagate broadcasts z only when it has more than one entry
     zshape = (zs.size,) if np.asarray(z).size > 1 else ()
     u = _run_prop2d(field, nat.CX_KERNEL_TRANSFER, zs, zshape, n, pad_width, kykx=kykx, mode=mode,
-                    precision=precision)
+                    precision=precision, cval=cval)
     out = shift_grid(field.replace(u=u), shift_yx)
     return out
 
@@ -196,11 +285,10 @@ def asm_propagate(field: Field, z, n, pad_width, cval: float = 0, absorbing_boun
                                   output_dx=output_dx, output_shape=output_shape, use_czt=use_czt, mode=mode,
                                   remove_evanescent=remove_evanescent, bandlimit=bandlimit, cval=cval,
                                   precision=precision)
-    if cval != 0:
-        raise NotImplementedError("non-zero cval padding is not supported by the fused loader")
     zs, zshape = _z_array(z)
     u = _run_prop2d(field, nat.CX_KERNEL_ASM, zs, zshape, n, pad_width, kykx=kykx, shift_yx=shift_yx,
-                    remove_evanescent=remove_evanescent, bandlimit=bandlimit, mode=mode, precision=precision)
+                    remove_evanescent=remove_evanescent, bandlimit=bandlimit, mode=mode, precision=precision,
+                    cval=cval)
     return shift_grid(field.replace(u=u), shift_yx)
 
 

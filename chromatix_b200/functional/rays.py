@@ -68,6 +68,7 @@ def ray_transfer(field: Field, ABCD, n, magnification=1.0, *, precision=None) ->
     from .sources import materialize
 
     torch = nat.torch_mod()
+    nat.refuse_grad("ray_transfer", getattr(field, "u", None))
     field = materialize(field)
     if getattr(field, "vectorial", False):
         raise NotImplementedError("ray_transfer takes scalar fields")

@@ -28,8 +28,7 @@ def rescaled_propagate(field: Field, kernel: int, z, n, pad_width, kykx=(0.0, 0.
     from .propagation import _pad_tuple
 
     prec = precision or config.get_precision()
-    if cval != 0:
-        raise NotImplementedError("non-zero cval padding is not supported by the fused loader")
+    nat.refuse_grad("rescaled (output_dx / output_shape) propagation", field.u)
     if field.n_wv != 1:
         # the reference indexes the padded extent per axis with T[d] (propagation.py:424-433),
         # which is only meaningful for a single wavelength
@@ -38,6 +37,12 @@ def rescaled_propagate(field: Field, kernel: int, z, n, pad_width, kykx=(0.0, 0.
         raise NotImplementedError("rescaled (CZT) propagation takes a scalar z")
     z = float(np.asarray(z).reshape(()))
     pad = _pad_tuple(pad_width)
+    if cval != 0 and (pad[0] or pad[1]):
+        # constant padding by the native pad kernel; the padded grid is the same
+        from ..core.field import pad as pad_field
+
+        field = pad_field(field, pad, cval)
+        pad = (0, 0)
     return _rescaled_one_call(field, kernel, z, n, pad, kykx, shift_yx, output_dx, output_shape, mode,
                               remove_evanescent, pad_width, prec, method=0 if use_czt else 1,
                               bandlimit=bool(bandlimit) and kernel == nat.CX_KERNEL_ASM)

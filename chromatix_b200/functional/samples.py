@@ -11,29 +11,79 @@ __all__ = ["thin_sample", "multislice_thick_sample", "fluorescent_multislice_thi
            "polarized_multislice_thick_sample"]
 
 
+_THIN_FN = None
+
+
+def _thin_fn():
+    """autograd Function of ``cx_thin_sample``; the backward is
+    ``cx_thin_sample_adjoint`` (gradients of the field, absorption and dn)."""
+    global _THIN_FN
+    if _THIN_FN is None:
+        torch = nat.torch_mod()
+
+        class _ThinSample(torch.autograd.Function):
+            @staticmethod
+            def forward(ctx, u, ab, dn, kd, d_bytes):
+                d = nat.cx_ew_desc.from_buffer_copy(d_bytes)
+                out = torch.empty_like(u)
+                nat.check(nat.lib().cx_thin_sample(d, nat.ptr(u), nat.ptr(ab), nat.ptr(dn), nat.ptr(kd),
+                                                   nat.ptr(out), nat.stream_handle(u.device)))
+                ctx.d_bytes = d_bytes
+                ctx.save_for_backward(out, ab, dn, kd)
+                return out
+
+            @staticmethod
+            def backward(ctx, g):
+                out, ab, dn, kd = ctx.saved_tensors
+                d = nat.cx_ew_desc.from_buffer_copy(ctx.d_bytes)
+                g = g.to(torch.complex64).contiguous()
+                nu, na, nd = ctx.needs_input_grad[:3]
+                gu = torch.empty_like(g) if nu else None
+                ga = torch.empty_like(ab) if na else None
+                gd = torch.empty_like(dn) if nd else None
+                nat.check(nat.lib().cx_thin_sample_adjoint(d, nat.ptr(g), nat.ptr(out), nat.ptr(ab), nat.ptr(dn),
+                                                           nat.ptr(kd), nat.ptr(gu), nat.ptr(ga), nat.ptr(gd),
+                                                           nat.stream_handle(g.device)))
+                return gu, ga, gd, None, None
+
+        _THIN_FN = _ThinSample
+    return _THIN_FN
+
+
 def thin_sample(field: Field, absorption, dn, thickness) -> Field:
     """``u * exp(1j 2 pi (dn + 1j absorption) thickness / lambda)``
-    (functional/samples.py:85-134).  Inside ``multislice_thick_sample`` this
-    product is fused into the slice kernel."""
+    (functional/samples.py:85-134), one pass of the native kernel
+    ``cx_thin_sample``.  Inside ``multislice_thick_sample`` this product is
+    fused into the slice kernel."""
+    from .phase_masks import _ew_desc, channel_scale
     from .sources import materialize
 
     torch = nat.torch_mod()
     field = materialize(field)
-    a = torch.as_tensor(np.asarray(absorption) if not isinstance(absorption, torch.Tensor) else absorption)
-    d = torch.as_tensor(np.asarray(dn) if not isinstance(dn, torch.Tensor) else dn)
-    if a.ndim != 2 or d.ndim != 2:
-        raise AssertionError(f"Absorption and dn must have shape {field.spatial_shape}")
-    a = a.to(device=field.device, dtype=torch.float64)
-    d = d.to(device=field.device, dtype=torch.float64)
-    lam = torch.as_tensor(field.spectrum.wavelength, device=field.device)
-    if field.chromatic:
-        a = a[..., None]
-        d = d[..., None]
+    nat.require_cuda(field.u, "Field.u")
+    ny, nx = field.spatial_shape
+
+    def _map(m, what):
+        t = m if isinstance(m, torch.Tensor) else torch.as_tensor(np.asarray(m, dtype=np.float32))
+        if t.ndim != 2:
+            raise AssertionError(f"{what} must have shape {field.spatial_shape}, got {tuple(t.shape)}")
+        if tuple(t.shape) != (ny, nx):
+            raise AssertionError(f"{what} must have shape {field.spatial_shape}, got {tuple(t.shape)}")
+        return t.to(device=field.device, dtype=torch.float32).contiguous()
+
+    a = _map(absorption, "Absorption")
+    d_ = _map(dn, "Refractive index")
+    kd = torch.as_tensor(channel_scale(field, 2 * np.pi * float(thickness) / field.spectrum.wavelength),
+                         device=field.device)
+    u = field.u.to(torch.complex64).contiguous()
+    d = _ew_desc(field, 0)
+    if nat.wants_grad(u, a, d_):
+        out = _thin_fn().apply(u, a, d_, kd, bytes(d))
     else:
-        lam = lam[0]
-    arg = 2 * np.pi * thickness / lam
-    t = torch.polar(torch.exp(-arg * a), arg * d).to(torch.complex64)
-    return field.replace(u=field.u * t)
+        out = torch.empty_like(u)
+        nat.check(nat.lib().cx_thin_sample(d, nat.ptr(u), nat.ptr(a), nat.ptr(d_), nat.ptr(kd), nat.ptr(out),
+                                           nat.stream_handle(u.device)))
+    return field.replace(u=out)
 
 
 class cx_ms_desc(nat.ctypes.Structure):
@@ -271,6 +321,7 @@ def fluorescent_multislice_thick_sample(field: Field, fluorescence_stack, dn_sta
     generator seeded by ``key`` (an int or a (2,) uint32 key); the reference's
     jax.random stream is not reproduced.  As in the reference, each sample
     starts from the field the previous one ended with."""
+    nat.refuse_grad("fluorescent_multislice_thick_sample", getattr(field, "u", None), fluorescence_stack, dn_stack)
     from .sources import materialize
 
     torch = nat.torch_mod()
@@ -347,6 +398,7 @@ def polarized_multislice_thick_sample(field: Field, potential_stack, n, thicknes
     (``cx_polarized_multislice``): per slice two row passes and two column
     passes whose CTAs hold the three components, so the 3x3 k-space projector
     and the potential apply between the transforms."""
+    nat.refuse_grad("polarized_multislice_thick_sample", getattr(field, "u", None), potential_stack)
     from .sources import materialize
 
     torch = nat.torch_mod()

@@ -277,19 +277,40 @@ def objective_point_source(shape, dx, spectrum, z, f, n, NA, power=1.0, amplitud
 def plane_wave(shape, dx, spectrum, power=1.0, amplitude=1.0, kykx=(0.0, 0.0), pupil=None, scalar: bool = True,
                *, device="cuda") -> Field:
     """``amp exp(i kykx . r)`` with optional pupil and power normalisation
-    (functional/sources.py:212-293)."""
+    (functional/sources.py:212-293), generated on the device by the native
+    kernel ``cx_plane_wave``.  Without a pupil |u| is uniform, so the power
+    normalisation is analytic (power / (amp^2 N area) folded into the
+    amplitude); with a pupil the field's power is measured after it."""
+    from .phase_masks import _ew_desc
+
     torch = nat.torch_mod()
     if not scalar:
-        raise NotImplementedError("vectorial fields are not part of this build")
+        raise NotImplementedError("vectorial plane waves are not part of this build")
     spec = Spectrum.build(spectrum)
-    field = Field.zeros(shape, dx, spec, device=device)
-    g = field._grid_np()
-    k = np.asarray(kykx, dtype=np.float64).reshape(2)
-    u = float(np.asarray(amplitude).reshape(())) * np.exp(1j * np.sum(k * g, axis=-1))
-    field = field.replace(u=torch.as_tensor(u.astype(np.complex64), device=field.device))
+    field = Field.empty(shape, dx, spec, device=device)
+    amp = float(np.asarray(amplitude).reshape(()))
+    ky, kx = (float(v) for v in np.asarray(kykx, dtype=np.float64).reshape(2))
+    W = field.n_wv
+    dxw = field.dx_wv
+    ny, nx = field.spatial_shape
+    if power is not None and pupil is None:
+        # Field.power (core/field.py:656-661, 728-733): area_w * sum_yx sum_w' density_w' |u|^2
+        area = np.prod(dxw, axis=-1)
+        dens = np.asarray(spec.density, np.float64) if field.chromatic else np.ones(1)
+        p_now = area * (amp * amp) * ny * nx * float(np.sum(dens))
+        scale = np.sqrt(float(power) / p_now)
+        amps = amp * scale
+    else:
+        amps = np.full(W, amp)
+    tab = nat.upload(np.stack([dxw[:, 0], dxw[:, 1], np.broadcast_to(amps, (W,))], axis=-1), field.device)
+    org = np.asarray(field.origin, dtype=np.float64).reshape(-1, 2)[0]
+    u = torch.empty(field.u.shape, dtype=torch.complex64, device=field.device)
+    nat.check(nat.lib().cx_plane_wave(_ew_desc(field, 0), nat.ptr(tab), ky, kx, float(org[0]), float(org[1]),
+                                      nat.ptr(u), nat.stream_handle(u.device)))
+    field = field.replace(u=u)
     if pupil is not None:
         field = pupil(field)
-    if power is not None:
-        pw = field.power
-        field = field.replace(u=field.u * torch.sqrt(power / pw))
+        if power is not None:
+            pw = field.power
+            field = field.replace(u=field.u * torch.sqrt(power / pw))
     return field

@@ -46,6 +46,7 @@ def fourier_convolution(image, kernel, *, axes=(-2, -1), fast_fft_shape: bool = 
     convolution theorem (ops/ops.py:9-86); ``reduce`` sums the result over
     all leading axes.  ``lengths``: "smallest" (smallest engine lengths
     >= 2 n) or "pow2" (next powers of two); the result is the same."""
+    nat.refuse_grad("fourier_convolution", image, kernel)
     torch = nat.torch_mod()
     ax = tuple(a % image.ndim for a in axes)
     if ax != (image.ndim - 2, image.ndim - 1):

@@ -58,6 +58,7 @@ class Request:
     t_launch: float = float("nan")
     t_done: float = float("nan")
     out: object = None
+    ready: object = None  # CUDA event on the client's stream at submit(): the field's writes are complete after it
 
     @property
     def side(self) -> int:
@@ -71,18 +72,32 @@ class Request:
         return (self.op, self.side, float(self.n)) if self.op != "czt_zoom" else ("czt_zoom", self.id)
 
 
+def _prop_ws_bytes(N: int, batch: int) -> int:
+    """Workspace of one batched ASM/transfer call on the padded (2N x 2N) grid:
+    row spectra of the inputs + filtered spectra (mode "same": N output rows)."""
+    px = 2 * N
+    return 8 * batch * (N * px + N * px) + 512
+
+
+def _prop_out_bytes(N: int, batch: int) -> int:
+    """Outputs (N x N complex64 each) and plane-table bytes of a batch."""
+    return 8 * batch * N * N + batch * 64 * 2
+
+
 def _prop_bytes(N: int, batch: int) -> int:
-    """Device bytes one batched ASM/transfer call holds while in flight:
-    outputs (N x N each) and the workspace of the padded (2N x 2N) grid."""
-    py = px = 2 * N
-    ws = 8 * batch * (N * px + py * px)  # row spectra of the inputs + filtered spectra
-    return ws + 8 * batch * N * N + batch * 64 * 2
+    """Device bytes one batched ASM/transfer call holds while in flight."""
+    return _prop_ws_bytes(N, batch) + _prop_out_bytes(N, batch)
+
+
+def _czt_out_bytes(out_shape) -> int:
+    my, mx = out_shape
+    return 8 * my * mx
 
 
 def _czt_bytes(N: int, out_shape) -> int:
     py = px = 2 * N
     my, mx = out_shape
-    return 8 * (2 * py * px + my * px + my * mx) + 8 * 2 * 8192
+    return 8 * (2 * py * px + my * px) + 8 * 2 * 8192 + _czt_out_bytes(out_shape)
 
 
 def request_bytes(r: Request) -> int:
@@ -211,6 +226,11 @@ class PropagationServer:
             raise ValueError("a request field is a contiguous square (N, N) complex64 CUDA tensor")
         if not r.t_arrival:
             r.t_arrival = time.perf_counter()
+        # the field may still be in flight on the client's stream (written by an
+        # asynchronous kernel or copy); the server's stream waits for this event
+        # before its first kernel reads it
+        r.ready = self.torch.cuda.Event()
+        r.ready.record(self.torch.cuda.current_stream(u.device))
         r.id = self._next_id
         self._next_id += 1
         self.sched.add(r)
@@ -228,11 +248,19 @@ class PropagationServer:
         for slot in self.slots:
             if slot.busy is not None:
                 continue
-            batch = self.sched.pick(self.sched.budget - self.inflight_bytes)
+            # workspaces stay allocated between batches: every other stream's
+            # held workspace counts against the budget; this stream's own is
+            # reused (or replaced) by the batch it launches
+            left = self.sched.budget - self.inflight_bytes - self.held_workspace_bytes(exclude=slot)
+            batch = self.sched.pick(left)
             if batch is None:
-                break
-            self._launch(slot, batch)
+                continue  # another free stream may hold the workspace this batch needs
+            self._launch(slot, batch, left)
         return done
+
+    def held_workspace_bytes(self, exclude=None) -> int:
+        """Device bytes of the streams' workspaces (kept between batches)."""
+        return sum(s.ws.numel() for s in self.slots if s is not exclude and s.ws is not None)
 
     def drain(self) -> list:
         out = []
@@ -258,20 +286,23 @@ class PropagationServer:
         self.completed += done
         return done
 
-    def _launch(self, slot: _Slot, batch: list) -> None:
+    def _launch(self, slot: _Slot, batch: list, budget_left: float = float("inf")) -> None:
         torch = self.torch
         t = time.perf_counter()
         for r in batch:
             r.t_launch = t
+        for r in batch:
+            if r.ready is not None:
+                slot.stream.wait_event(r.ready)
         with torch.cuda.stream(slot.stream):
             # recorded just before the batch's kernels are issued (device time only)
             slot.ev0 = ev0 = torch.cuda.Event(enable_timing=True)
             if batch[0].op == "czt_zoom":
-                nbytes = request_bytes(batch[0])
+                nbytes = _czt_out_bytes(batch[0].out_shape)
                 keep = self._run_czt(slot, batch[0])
             else:
-                nbytes = _prop_bytes(batch[0].side, len(batch))
-                keep = self._run_prop(slot, batch)
+                nbytes = _prop_out_bytes(batch[0].side, len(batch))
+                keep = self._run_prop(slot, batch, budget_left - nbytes)
             ev = torch.cuda.Event(enable_timing=True)
             ev.record(slot.stream)
         self.inflight_bytes += nbytes
@@ -280,7 +311,7 @@ class PropagationServer:
         self.host_s[op] += time.perf_counter() - t
         self.batches[op] += 1
 
-    def _run_prop(self, slot: _Slot, batch: list):
+    def _run_prop(self, slot: _Slot, batch: list, ws_budget: float = float("inf")):
         torch = self.torch
         N = batch[0].side
         B = len(batch)
@@ -310,7 +341,9 @@ class PropagationServer:
         d.n_medium = float(batch[0].n)
         wsb = nat.c_size_t(0)
         nat.check(self.L.cx_prop2d_workspace_size(d, wsb))
-        ws = slot.workspace(wsb.value, reserve=(wsb.value // B + 512) * self.max_batch)
+        # grow once to the largest batch of this shape, as far as the budget allows
+        reserve = min((wsb.value // B + 512) * self.max_batch, max(ws_budget, wsb.value))
+        ws = slot.workspace(wsb.value, reserve=reserve)
         base = slot.dev.data_ptr()
         slot.ev0.record(slot.stream)
         nat.check(self.L.cx_prop2d_ptrs(d, base, base + off_p, base + off_p + 8 * B, None, ws.data_ptr(),

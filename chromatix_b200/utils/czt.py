@@ -22,7 +22,7 @@ class cx_czt_desc(nat.ctypes.Structure):
                 ("out_ostride", nat.ctypes.c_int64), ("out_istride", nat.ctypes.c_int64),
                 ("out_estride", nat.ctypes.c_int64), ("a_re", nat.c_double), ("a_im", nat.c_double),
                 ("w_re", nat.c_double), ("w_im", nat.c_double), ("mod_n", nat.c_int32), ("layout", nat.c_int32),
-                ("scale", nat.c_double)]
+                ("scale", nat.c_double), ("adjoint", nat.c_int32), ("reserved", nat.c_int32)]
 
 
 _SIG = False
@@ -41,6 +41,53 @@ def _lib():
     return L
 
 
+def _launch_czt(d: cx_czt_desc, x, oshape, out=None):
+    torch = nat.torch_mod()
+    y = out if out is not None else torch.empty(oshape, dtype=torch.complex64, device=x.device)
+    L = _lib()
+    ws_b = nat.c_size_t(0)
+    nat.check(L.cx_czt_workspace_size(d, ws_b))
+    ws = nat.workspace(ws_b.value, x.device)
+    nat.check(L.cx_czt(d, nat.ptr(x), nat.ptr(y), nat.ptr(ws), ws_b.value, nat.stream_handle(x.device)))
+    return y
+
+
+def _adjoint_desc(d: cx_czt_desc) -> cx_czt_desc:
+    """The transform's conjugate transpose: m inputs onto n outputs (the
+    strides of input and output swap roles)."""
+    a = cx_czt_desc.from_buffer_copy(d)
+    a.adjoint = 1 - d.adjoint
+    a.in_ostride, a.in_istride, a.in_estride = d.out_ostride, d.out_istride, d.out_estride
+    a.out_ostride, a.out_istride, a.out_estride = d.in_ostride, d.in_istride, d.in_estride
+    return a
+
+
+_CZT_FN = None
+
+
+def _czt_fn():
+    """torch autograd Function over ``cx_czt``: the backward is the adjoint
+    chirp-Z transform (``adjoint = 1``), one fused Bluestein pass like the
+    forward (the gradient jax.grad takes through utils/czt.py:7-52)."""
+    global _CZT_FN
+    if _CZT_FN is None:
+        torch = nat.torch_mod()
+
+        class _CZT(torch.autograd.Function):
+            @staticmethod
+            def forward(ctx, x, d_bytes, oshape):
+                ctx.d_bytes, ctx.ishape = d_bytes, tuple(x.shape)
+                return _launch_czt(cx_czt_desc.from_buffer_copy(d_bytes), x, oshape)
+
+            @staticmethod
+            def backward(ctx, g):
+                d = _adjoint_desc(cx_czt_desc.from_buffer_copy(ctx.d_bytes))
+                return _launch_czt(d, g.to(torch.complex64).contiguous(), ctx.ishape), None, None
+
+        _CZT_FN = _CZT
+    return _CZT_FN
+
+
 def czt_axis(x, m: int, a: complex, w: complex, axis: int = -1, mod_n: int = -1, scale: float = 1.0, out=None):
     """Low-level fused CZT of a contiguous complex64 CUDA tensor along ``axis``."""
     torch = nat.torch_mod()
@@ -52,7 +99,6 @@ def czt_axis(x, m: int, a: complex, w: complex, axis: int = -1, mod_n: int = -1,
     inner = int(np.prod(x.shape[axis + 1:])) if axis + 1 < x.ndim else 1
     oshape = list(x.shape)
     oshape[axis] = m
-    y = out if out is not None else torch.empty(oshape, dtype=torch.complex64, device=x.device)
     d = cx_czt_desc()
     d.n, d.m, d.L, d.inner = n, int(m), 0, inner
     d.n_vec = outer * inner
@@ -64,12 +110,11 @@ def czt_axis(x, m: int, a: complex, w: complex, axis: int = -1, mod_n: int = -1,
     d.mod_n = int(mod_n)
     d.layout = 0 if inner == 1 else 1
     d.scale = float(scale)
-    L = _lib()
-    ws_b = nat.c_size_t(0)
-    nat.check(L.cx_czt_workspace_size(d, ws_b))
-    ws = nat.workspace(ws_b.value, x.device)
-    nat.check(L.cx_czt(d, nat.ptr(x), nat.ptr(y), nat.ptr(ws), ws_b.value, nat.stream_handle(x.device)))
-    return y
+    if nat.wants_grad(x):
+        if out is not None:
+            raise ValueError("czt_axis: out= is not differentiable")
+        return _czt_fn().apply(x, bytes(d), tuple(oshape))
+    return _launch_czt(d, x, tuple(oshape), out)
 
 
 def czt(x, m: int, a, w, axis: int = -1):

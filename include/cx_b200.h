@@ -80,6 +80,11 @@ typedef struct {
   int32_t bandlimit;
   double n_medium;
   double ky0, kx0;         /* kykx tilt subtracted from the frequency grid */
+  int32_t conj_kernel;     /* 1: multiply by conj(H) instead of H -- the adjoint of the propagation
+                              (conj(H) = H(-z) for the transfer and ASM kernels, all options included) */
+  int32_t crop_y, crop_x;  /* mode_same = 0 only: rows / columns dropped on each side of the padded grid
+                              (the adjoint of zero padding); output (py - 2 crop_y, px - 2 crop_x) */
+  int32_t reserved;
 } cx_prop2d_desc;
 
 /* Workspace bytes for cx_prop2d. */
@@ -88,7 +93,11 @@ cx_status cx_prop2d_workspace_size(const cx_prop2d_desc* d, size_t* bytes);
 /* transfer_propagate / asm_propagate / kernel_propagate (FFT branch)
  * (functional/propagation.py:168-252, 255-352, 355-394).
  * u_out: (n_out_planes/n_wv, oy, ox, n_wv) with (oy, ox) = (ny, nx) when
- * mode_same else (ny + 2 pad_y, nx + 2 pad_x).  H (CX_KERNEL_EXPLICIT only):
+ * mode_same else (ny + 2 pad_y - 2 crop_y, nx + 2 pad_x - 2 crop_x).
+ * The gradient of a propagation (the reference differentiates it with
+ * jax.grad) is the same call with conj_kernel = 1 applied to the output
+ * gradient: mode_same keeps its geometry; a "full" propagation's adjoint takes
+ * the padded grid as input (pad 0) and crops (pad_y, pad_x).  H (CX_KERNEL_EXPLICIT only):
  * planar (h_planes, py, px) complex64 in FFT (ifftshifted) order. */
 cx_status cx_prop2d(const cx_prop2d_desc* d, const cx_plane* planes_dev, const void* u_in, void* u_out,
                     const void* H, void* workspace, size_t workspace_bytes, cx_stream_t stream);
@@ -202,6 +211,8 @@ typedef struct {
   double pupil_r2;         /* circular input pupil radius^2 (< 0: none) */
   int32_t in_plane;        /* input plane (batch * n_wv + wv) */
   int32_t conj;            /* 1: conjugate input and output (inverse transform) */
+  double pupil_out_r2;     /* > 0: circular pupil of this radius^2 on the output grid (origin oy, ox), applied
+                              last; <= 0: none.  The adjoint of an input pupil. */
 } cx_fft_plane;
 
 typedef struct {
@@ -215,7 +226,12 @@ typedef struct {
 
 cx_status cx_optfft_workspace_size(const cx_optfft_desc* d, size_t* bytes);
 /* planes_dev: n_out_planes cx_fft_plane in device memory.  u_out:
- * (n_out_planes/n_wv, ny + 2 pad_y - 2 crop_y, nx + 2 pad_x - 2 crop_x, n_wv). */
+ * (n_out_planes/n_wv, ny + 2 pad_y - 2 crop_y, nx + 2 pad_x - 2 crop_x, n_wv).
+ * Adjoint (the gradient jax.grad takes through optical_fft / ff_lens): the
+ * same call on the output gradient with pad and crop swapped, spacings
+ * swapped, conj flipped, chirp_in' = -chirp_out, chirp_out' = -chirp_in,
+ * pre' = post (conj = 0 forward) or conj(post) (conj = 1), post' = conj(pre)
+ * or pre, and the input pupil moved to pupil_out_r2. */
 cx_status cx_optical_fft(const cx_optfft_desc* d, const cx_fft_plane* planes_dev, const void* u_in, void* u_out,
                          void* workspace, size_t workspace_bytes, cx_stream_t stream);
 /* Same, with a propagator table H (planar (n_out_planes, py, px), FFT order)
@@ -279,6 +295,10 @@ typedef struct {
   int32_t mod_n;       /* >= 0: multiply output k by w^(-mod_n k) a^mod_n */
   int32_t layout;      /* 0: one team per vector; 1: column tiles (unit inner strides) */
   double scale;
+  int32_t adjoint;     /* 1: the adjoint (conjugate transpose) of the transform above:
+                          x'[j] = sum_k conj(scale [w^(-N k) a^N] a^(-j) w^(j k)) y'[k], j < n.
+                          Input vectors then have m elements and outputs n (strides as given). */
+  int32_t reserved;
 } cx_czt_desc;
 
 cx_status cx_czt_workspace_size(const cx_czt_desc* d, size_t* bytes);
@@ -494,10 +514,77 @@ cx_status cx_mbs_precondition(const cx_mbs_desc* d, const void* eps, const void*
 cx_status cx_mbs_iterate(const cx_mbs_desc* d, const void* eps, const void* prec_y, const void* x, void* x_new,
                          double* acc, void* workspace, size_t workspace_bytes, cx_stream_t stream);
 
+/* prec_forward(x) = -V(G(V x) + x) (solver.py:91-93): the preconditioned
+ * operator whose system prec_forward(x) = prec_y BiCGStab solves
+ * (solver.py:143-144, jax.scipy.sparse.linalg.bicgstab). */
+cx_status cx_mbs_forward(const cx_mbs_desc* d, const void* eps, const void* x, void* out, void* workspace,
+                         size_t workspace_bytes, cx_stream_t stream);
+
+/* Complex vector algebra for the Krylov solve, FP64 accumulation (the
+ * reference's bicgstab takes these inner products in its working precision):
+ * out_dev[0..3] = (Re, Im) sum conj(x) y, sum |x|^2, sum |y|^2 over n complex64. */
+cx_status cx_cvec_dot(const void* x, const void* y, int64_t n, double* out_dev, cx_stream_t stream);
+/* out = c0 x + c1 y [+ c2 z] with complex coefficients coef (host, 6 doubles:
+ * re, im of c0, c1, c2; z may be NULL); norm_dev (may be NULL) = sum |out|^2. */
+cx_status cx_cvec_lincomb(int64_t n, const double* coef, const void* x, const void* y, const void* z, void* out,
+                          double* norm_dev, cx_stream_t stream);
+
 /* Field.intensity (core/field.py:656-665, 735-740): out[b, y, x] =
  * sum_wv density[wv] |u[b, y, x, wv]|^2.  density_dev: n_wv doubles. */
 cx_status cx_intensity(const void* u, int64_t n_pix, int32_t n_wv, const double* density_dev, float* out,
                        cx_stream_t stream);
+
+/* ---------------------------------------------------------------------------
+ * Elementwise field operations and the adjoints jax.grad takes through them.
+ * u, out: (n_batch, ny, nx, n_wv) complex64 (n_wv interleaved innermost:
+ * wavelengths, or wavelengths x vector components); real maps: one (ny, nx)
+ * float32 plane broadcast over batch and channels, or (n_batch, ny, nx) when
+ * map_batched = 1.  Gradients follow torch's convention for complex values
+ * (g = dL/dRe + i dL/dIm); the gradient of a broadcast map is summed over
+ * batch and channels.
+ * ------------------------------------------------------------------------- */
+typedef struct {
+  int64_t n_batch;
+  int32_t ny, nx;
+  int32_t n_wv;          /* interleaved innermost channels, 1..64 */
+  int32_t map_batched;   /* 1: the real maps have n_batch planes */
+} cx_ew_desc;
+
+/* phase_change (functional/phase_masks.py:29-68): out = u exp(i phase s[w]),
+ * s (device, n_wv floats) = lambda0 / lambda_w (spectrally_modulate) or 1. */
+cx_status cx_phase_change(const cx_ew_desc* d, const void* u, const float* phase, const float* s_dev, void* out,
+                          cx_stream_t stream);
+/* Its adjoint: g_u = g exp(-i phase s[w]); g_phase = sum_{b,w} s[w] Im(g conj(out)).
+ * g_u or g_phase may be NULL (not wanted). */
+cx_status cx_phase_change_adjoint(const cx_ew_desc* d, const void* g, const void* out, const float* phase,
+                                  const float* s_dev, void* g_u, float* g_phase, cx_stream_t stream);
+/* thin_sample (functional/samples.py:85-134): out = u exp(i kd[w] (dn + i absorption)),
+ * kd (device, n_wv floats) = 2 pi thickness / lambda_w. */
+cx_status cx_thin_sample(const cx_ew_desc* d, const void* u, const float* absorption, const float* dn,
+                         const float* kd_dev, void* out, cx_stream_t stream);
+/* Its adjoint: g_u = g conj(t); g_dn = sum kd Im(g conj(out)); g_absorption = -sum kd Re(g conj(out)). */
+cx_status cx_thin_sample_adjoint(const cx_ew_desc* d, const void* g, const void* out, const float* absorption,
+                                 const float* dn, const float* kd_dev, void* g_u, float* g_absorption, float* g_dn,
+                                 cx_stream_t stream);
+/* Adjoint of Field.intensity (core/field.py:656-665, 735-740):
+ * g_u[p, w] = 2 density[w] g_intensity[p] u[p, w]. */
+cx_status cx_intensity_adjoint(const void* u, int64_t n_pix, int32_t n_wv, const double* density_dev,
+                               const float* g_intensity, void* g_u, cx_stream_t stream);
+/* pad (core/field.py:534-549) of the spatial axes with the constant cval:
+ * out (n_batch, ny + 2 pad_y, nx + 2 pad_x, n_wv). */
+cx_status cx_pad(const cx_ew_desc* d, int32_t pad_y, int32_t pad_x, float cval_re, float cval_im, const void* u,
+                 void* out, cx_stream_t stream);
+/* plane_wave (functional/sources.py:212-293) before its pupil and power
+ * normalisation: u[b, y, x, w] = amp_w exp(i (ky gy + kx gx)), g = d_w (i - N/2)
+ * + origin; wv_params_dev: (n_wv, 3) doubles (dy, dx, amp). */
+cx_status cx_plane_wave(const cx_ew_desc* d, const double* wv_params_dev, double ky, double kx, double origin_y,
+                        double origin_x, void* u, cx_stream_t stream);
+/* Pupils (functional/pupils.py:17-67) on the field grid g = d_w (i - N/2) + origin:
+ * kind 0 circular (|g|^2 <= p0^2), 1 square (max |g| <= p0), 2 super-Gaussian
+ * exp(-(|g| / p0)^p1), 3 Tukey (alpha p1 on |g / extent|, extent (p2, p3));
+ * wv_params_dev: (n_wv, 6) doubles (dy, dx, p0, p1, p2, p3).  out = mask * u. */
+cx_status cx_pupil(const cx_ew_desc* d, int32_t kind, const double* wv_params_dev, double origin_y, double origin_x,
+                   const void* u, void* out, cx_stream_t stream);
 
 /* ---------------------------------------------------------------------------
  * misc

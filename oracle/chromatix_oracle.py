@@ -958,7 +958,7 @@ def multislice_loss_and_grad(u0, dn_stack, absorption_stack, target, n, dz, wave
     k = 2 * np.pi / wavelength
     us = [field.u]
     for i in range(D):
-        v = np.fft.ifft2(np.fft.fft2(us[-1]) * H)
+        v = _ifft2(_fft2(us[-1], (-2, -1)) * H, (-2, -1))
         t = np.exp(1j * k * dz * (dn_stack[i] + 1j * absorption_stack[i]))
         us.append(v * t)
     if reverse_propagate_distance is None:
@@ -967,11 +967,11 @@ def multislice_loss_and_grad(u0, dn_stack, absorption_stack, target, n, dz, wave
     if NA is not None:
         mask = l2_sq_norm(field.f_grid) <= (NA / wavelength) ** 2
         Hd = Hd * np.fft.ifftshift(mask)
-    u_out = np.fft.ifft2(np.fft.fft2(us[-1]) * Hd)
+    u_out = _ifft2(_fft2(us[-1], (-2, -1)) * Hd, (-2, -1))
     I = np.abs(u_out) ** 2
     L = float(np.sum((I - target) ** 2))
     g = 4 * (I - target) * u_out
-    g = np.fft.ifft2(np.fft.fft2(g) * np.conj(Hd))
+    g = _ifft2(_fft2(g, (-2, -1)) * np.conj(Hd), (-2, -1))
     gdn = np.zeros(dn_stack.shape)
     gab = np.zeros(dn_stack.shape)
     for i in range(D - 1, -1, -1):
@@ -980,7 +980,7 @@ def multislice_loss_and_grad(u0, dn_stack, absorption_stack, target, n, dz, wave
         gdn[i] = k * dz * np.imag(w)
         gab[i] = -k * dz * np.real(w)
         t = np.exp(1j * k * dz * (dn_stack[i] + 1j * absorption_stack[i]))
-        g = np.fft.ifft2(np.fft.fft2(g * np.conj(t)) * np.conj(H))
+        g = _ifft2(_fft2(g * np.conj(t), (-2, -1)) * np.conj(H), (-2, -1))
     return L, gdn, gab, u_out
 
 
@@ -1235,6 +1235,46 @@ def mbs_solve(permittivity, spacing, k0, source_field, maxiter=1000, tol=1e-5, s
         if res < tol:
             break
     return x * op.num_scale, it, res, op
+
+
+def mbs_bicgstab(op: "MBSOperator", x0, maxiter=1000, tol=1e-5):
+    """BiCGStab on ``op.forward(x) = op.prec_y`` (solver.py:143-144, which calls
+    jax.scipy.sparse.linalg.bicgstab), FP64: the published algorithm (van der
+    Vorst 1992) with the stopping rule ||r|| <= tol ||b|| and the breakdown
+    exits.  Returns (x, iterations, ||r|| / ||b||)."""
+    b = op.prec_y
+    vd = lambda a, c: np.vdot(a.reshape(-1), c.reshape(-1))
+    x = np.asarray(x0, np.complex128).copy()
+    r = b - op.forward(x)
+    rhat = r.copy()
+    p = r.copy()
+    q = r.copy()
+    rho = alpha = omega = 1.0 + 0j
+    bs = float(np.real(vd(b, b)))
+    thr2 = tol * tol * bs
+    it = 0
+    while float(np.real(vd(r, r))) > thr2 and it < maxiter:
+        rho_new = vd(rhat, r)
+        if rho_new == 0:
+            break
+        beta = rho_new / rho * alpha / omega
+        p = r + beta * (p - omega * q)
+        q = op.forward(p)
+        alpha = rho_new / vd(rhat, q)
+        s = r - alpha * q
+        it += 1
+        if float(np.real(vd(s, s))) < thr2:
+            x = x + alpha * p
+            r = s
+            break
+        t = op.forward(s)
+        omega = vd(t, s) / vd(t, t)
+        x = x + alpha * p + omega * s
+        r = s - omega * t
+        rho = rho_new
+        if alpha == 0 or omega == 0:
+            break
+    return x, it, float(np.sqrt(np.real(vd(r, r)) / bs))
 
 
 def mbs_source_field(current_density, k0):

@@ -25,8 +25,9 @@ def test_build_dispatch_and_vector_layout():
         cx.Field.build(torch.zeros((2, 8, 6, 3), dtype=torch.complex64), 0.5, 0.5)
 
 
+@pytest.mark.gpu
 def test_pad_and_crop_vector_field():
-    u = torch.arange(8 * 6 * 3, dtype=torch.float32).reshape(8, 6, 3).to(torch.complex64)
+    u = torch.arange(8 * 6 * 3, dtype=torch.float32).reshape(8, 6, 3).to(torch.complex64).cuda()
     v = cx.VectorField(u, 0.5, 0.0, cx.MonoSpectrum(0.5))
     p = pad(v, (2, 3))
     assert tuple(p.u.shape) == (12, 12, 3)
@@ -40,11 +41,20 @@ def test_seed_of_key_forms():
     assert _seed_of(-1) == 0xFFFFFFFFFFFFFFFF
 
 
+@pytest.mark.gpu
 def test_chromatic_vector_field_layout_and_padding():
     wl = (np.array([0.5, 0.6]), np.ones(2))
-    u = torch.arange(6 * 5 * 2 * 3, dtype=torch.float32).reshape(6, 5, 2, 3).to(torch.complex64)
+    u = torch.arange(6 * 5 * 2 * 3, dtype=torch.float32).reshape(6, 5, 2, 3).to(torch.complex64).cuda()
     f = cx.Field.build(u, 0.4, wl)
     assert type(f) is cx.ChromaticVectorField and f.spatial_dims == (-4, -3) and f.spatial_shape == (6, 5)
     p = pad(f, (1, 2))
     assert tuple(p.u.shape) == (8, 9, 2, 3) and torch.equal(p.u[1:7, 2:7], u)
     assert torch.equal(crop(p, (1, 2)).u, u)
+
+
+def test_pad_has_no_cpu_path():
+    # the native pad kernel is the only implementation: a host tensor is refused
+    u = torch.zeros((4, 4), dtype=torch.complex64)
+    f = cx.Field.build(u, 0.5, 0.5)
+    with pytest.raises(ValueError, match="CUDA"):
+        pad(f, 1, 0.5)

@@ -114,3 +114,23 @@ def test_mbs_rejects_unsupported_lengths():
     perm = np.ones((17, 32, 32), np.complex128)
     with pytest.raises(CxError):
         _cuda_solve(perm, np.zeros(perm.shape + (3,)), 1.0, 1.0, maxiter=1)
+
+
+def test_mbs_bicgstab_iterates_and_converged_field():
+    """use_bicgstab=True (solver.py:143-144): the first BiCGStab iterates track
+    the FP64 restatement of the algorithm, and the converged field equals the
+    fixed-point solution of the same preconditioned system."""
+    shape = (32, 32, 32)
+    perm, src, roi = _problem(shape)
+    op = O.MBSOperator(perm, SPACING, K0, src)
+    for k in (1, 3):
+        x64, it64, _ = O.mbs_bicgstab(op, op.prec_y, maxiter=k, tol=0.0)
+        Eb, info = _cuda_solve(perm, src, op.bias, op.scale, maxiter=k, tol=0.0, use_bicgstab=True)
+        assert info["iterations"] == it64 == k
+        assert rel(to_np(Eb), x64 * op.num_scale) < 1e-4, k
+    Eb, info = _cuda_solve(perm, src, op.bias, op.scale, maxiter=400, tol=1e-6, use_bicgstab=True)
+    assert info["status"] == "converged" and info["residual_rel"] <= 1e-6
+    Ef, it, res, _ = O.mbs_solve(perm, SPACING, K0, src, maxiter=3000, tol=1e-9, shift=op.bias, scale=op.scale)
+    assert rel(to_np(Eb), Ef) < 1e-4
+    # BiCGStab needs far fewer operator applications than the fixed-point series
+    assert 2 * info["iterations"] < it

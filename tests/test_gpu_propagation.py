@@ -200,3 +200,26 @@ def test_largest_grid_4096():
     ref = O.asm_propagate(oracle_field(u, 0.3, 0.532), 200.0, 1.33, 1024)
     assert out.u.shape == ref.u.shape == (4096, 4096)
     assert rel(to_np(out.u), ref.u) < 1e-5
+
+
+@pytest.mark.parametrize("boundary", ["tukey", "super_gaussian"])
+def test_absorbing_boundary_is_a_no_op_like_the_reference(boundary):
+    """kernel_propagate builds the tapered pupil on the pre-propagation field and
+    then returns field.replace(u=u) with the unmasked propagated u
+    (functional/propagation.py:460-463): the output does not change."""
+    import torch
+
+    import chromatix_b200.functional as cf
+
+    u = rand_field((128, 128), seed=11)
+    f = cuda_field(u, 0.3, 0.532)
+    for fn in (cf.asm_propagate, cf.transfer_propagate):
+        a = fn(f, 40.0, 1.33, 64).u
+        b = fn(f, 40.0, 1.33, 64, absorbing_boundary=boundary, absorbing_boundary_width=0.5).u
+        torch.cuda.synchronize()
+        assert torch.equal(a, b)
+    H = cf.compute_asm_propagator(f, 40.0, 1.33)
+    a = cf.kernel_propagate(f, H).u
+    b = cf.kernel_propagate(f, H, absorbing_boundary=boundary).u
+    torch.cuda.synchronize()
+    assert torch.equal(a, b)

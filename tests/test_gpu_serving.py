@@ -72,8 +72,32 @@ def test_budget_limits_batches():
     peak = 0
     while srv.busy:
         srv.step()
-        peak = max(peak, srv.inflight_bytes)
+        peak = max(peak, srv.inflight_bytes + srv.held_workspace_bytes())
     torch.cuda.synchronize()
     assert peak <= srv.sched.budget
     for r in reqs:
         assert torch.equal(r.out, _alone(r))
+
+
+def test_request_written_on_a_producer_stream_is_read_after_its_writes():
+    """A field still being written on the client's stream when it is submitted
+    (no synchronisation in between) is read only after those writes: the
+    server's stream waits on an event recorded at submit()."""
+    import torch
+
+    from chromatix_b200.serving import PropagationServer, Request
+
+    src = _field(512, 5)
+    u = torch.zeros_like(src)
+    producer = torch.cuda.Stream()
+    srv = PropagationServer(budget_bytes=4e9, n_streams=2, max_batch=4)
+    torch.cuda.synchronize()
+    with torch.cuda.stream(producer):
+        torch.cuda._sleep(50_000_000)  # tens of milliseconds of device time before the write lands
+        u.copy_(src)
+        r = srv.submit(Request(op="asm", u=u, dx=0.3, z=50.0, wavelength=0.5))
+    srv.drain()
+    torch.cuda.synchronize()
+    ref = _alone(Request(op="asm", u=src, dx=0.3, z=50.0, wavelength=0.5))
+    torch.cuda.synchronize()
+    assert torch.equal(r.out, ref)
