@@ -587,6 +587,20 @@ cx_status cx_pupil(const cx_ew_desc* d, int32_t kind, const double* wv_params_de
                    const void* u, void* out, cx_stream_t stream);
 
 /* ---------------------------------------------------------------------------
+ * Tensor-core (tcgen05) split-precision DFT: the building block of the
+ * CX_PREC_SPLIT16 transform stages that replace the radix butterflies of
+ * the FFTs inside kernel_propagate (functional/propagation.py:391-394) and
+ * optical_fft (functional/convenience.py:9-59).  y[b, k] = sum_n x[b, n]
+ * exp(-+2 pi i n k / R) for R in {16, 32, 40, 64}, x, y (batch, R) complex64:
+ * a real GEMM on FP16 hi + lo operands (3 products, FP32 accumulation in
+ * tensor memory), each vector scaled by a power of two.  status_dev[0] is
+ * set to 1 if the kernel gave up waiting for an MMA (the output is then
+ * incomplete).
+ * ------------------------------------------------------------------------- */
+cx_status cx_dft_split16(const void* x, void* y, int32_t R, int64_t batch, int32_t inverse, int32_t* status_dev,
+                         cx_stream_t stream);
+
+/* ---------------------------------------------------------------------------
  * misc
  * ------------------------------------------------------------------------- */
 const char* cx_last_error(void);
