@@ -155,11 +155,14 @@ def gpu_arm(args):
     phase_d = torch.as_tensor(phase, device=dev)
     spec = (WAVELENGTHS, np.ones(NWV))
 
+    mode = {"p": "accurate"}  # transform form of the timed steps (see below)
+
     def step_device():
-        f = cf.objective_point_source((N, N), dx, spec, z, F_OBJ, N_MED, NA, device=dev)
-        f = cf.phase_change(f, phase_d)
-        f = cf.ff_lens(f, F_TUBE, N_MED)
-        return f.intensity
+        with cx.precision(mode["p"]):
+            f = cf.objective_point_source((N, N), dx, spec, z, F_OBJ, N_MED, NA, device=dev)
+            f = cf.phase_change(f, phase_d)
+            f = cf.ff_lens(f, F_TUBE, N_MED)
+            return f.intensity
 
     # pinned host buffers for the end-to-end arm
     phase_h = torch.from_numpy(phase).pin_memory()
@@ -169,9 +172,10 @@ def gpu_arm(args):
     def step_e2e():
         ph = phase_h.to(dev, non_blocking=True)
         zz = z_h.to(dev, non_blocking=True)
-        f = cf.objective_point_source((N, N), dx, spec, zz, F_OBJ, N_MED, NA, device=dev)
-        f = cf.ff_lens(cf.phase_change(f, ph), F_TUBE, N_MED)
-        return f.intensity_to(out_h)  # streamed device->host copies overlap the FFTs
+        with cx.precision(mode["p"]):
+            f = cf.objective_point_source((N, N), dx, spec, zz, F_OBJ, N_MED, NA, device=dev)
+            f = cf.ff_lens(cf.phase_change(f, ph), F_TUBE, N_MED)
+            return f.intensity_to(out_h)  # streamed device->host copies overlap the FFTs
 
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)  # > 126 MB L2
 
@@ -197,15 +201,41 @@ def gpu_arm(args):
             dist.barrier()
         return total / steps  # ms per step (this rank)
 
-    with ClockSampler(local) as clk:
-        ms = timed(step_device, args.steps, args.warmup)
+    # the plain FP32 transform form and the split-precision tensor-core form
+    # ("split16": column transforms as FP16 hi + lo DFT contractions) on the
+    # same workload; the line reports the faster form that meets the 1e-5
+    # bar against the FP64 oracle (errors checked outside the timed region)
+    forms = ["accurate"] if args.no_split16 else ["accurate", "split16"]
+    ms_form, clk_form = {}, {}
+    for p in forms:
+        mode["p"] = p
+        with ClockSampler(local) as clk:
+            ms_form[p] = timed(step_device, args.steps, args.warmup)
+        clk_form[p] = clk
+    acc_form = {}
+    if rank == 0 and not args.no_accuracy:
+        for p in forms:
+            acc_form[p] = accuracy_check(dev, p)
+    ms_form = dict(zip(forms, max_over_ranks([ms_form[p] for p in forms], dist, dev)))
+    ok = [p for p in forms if acc_form.get(p, {}).get("rel_err_vs_fp64", 0.0) <= 1e-5]
+    best = min(ok or ["accurate"], key=lambda p: ms_form[p])
+    if dist:
+        # every rank times the same form (rank 0's accuracy decides)
+        import torch.distributed as _d
+
+        flag = torch.tensor([forms.index(best)], device=dev)
+        _d.broadcast(flag, 0)
+        best = forms[int(flag.item())]
+    mode["p"] = best
+    ms, clk = ms_form[best], clk_form[best]
     ms_e2e = timed(step_e2e, max(2, args.steps // 2), 2)
 
     # dominant kernel (column pass) launch time, measured live with CUDA events
     # on the launching stream: one chunk of the same workload
-    kern = dominant_kernel_time(dev, z, phase_d, dx)
+    with cx.precision(best):
+        kern = dominant_kernel_time(dev, z, phase_d, dx)
 
-    ms, ms_e2e = max_over_ranks([ms, ms_e2e], dist, dev)
+    ms_e2e, = max_over_ranks([ms_e2e], dist, dev)
     value = PX_PER_STEP * world / (ms * 1e-3) / 1e6
     e2e_value = PX_PER_STEP * world / (ms_e2e * 1e-3) / 1e6
 
@@ -240,16 +270,27 @@ def gpu_arm(args):
         line = {
             "metric": METRIC, "value": round(value, 1), "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": round(ms, 4), "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "c64/f32 (FP64 phase arguments)", "data": "synthetic (seeded)",
+            "vs_baseline": None,
+            "dtype": ("c64/f32 (FP64 phase arguments)" if best == "accurate" else
+                      "c64/f32 (FP64 phase arguments; column transforms as FP16 hi+lo tensor-core DFT contractions, "
+                      "FP32 accumulation)"),
+            "data": "synthetic (seeded)",
             "config": dict(CONFIG, l2="flushed between timed steps (256 MB write)",
                            parallelism=f"replicas x{world}" if world > 1 else "single GPU"),
             "e2e": {"value": round(e2e_value, 1), "unit": UNIT, "ms_per_step": round(ms_e2e, 4),
                     "h2d_bytes_per_step": int(phase.nbytes + z.nbytes),
                     "d2h_bytes_per_step": int(NZ * N * N * 4)},
             "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": hbm, "unit": "GB/s",
-                         "frac": round(achieved / hbm, 4), "traffic": traffic,
-                         "kernel": "k_psf_cols<1280> (column FFT + spectral intensity)",
+                         "frac": round(achieved / hbm, 4), "traffic": traffic if best == "accurate" else None,
+                         "kernel": ("k_psf_cols<1280> (column FFT + spectral intensity)" if best == "accurate" else
+                                    "k_psf_cols_tc<40,32> (tensor-core column FFT + spectral intensity)"),
                          "kernel_ms": round(kern["ms"], 5), "peak_source": peak_src},
+            "transform_form": best,
+            "forms": {p: {"ms_per_step": round(ms_form[p], 4),
+                          "value": round(PX_PER_STEP * world / (ms_form[p] * 1e-3) / 1e6, 1),
+                          "speedup_vs_fp32": round(ms_form["accurate"] / ms_form[p], 3),
+                          "rel_err_vs_fp64": acc_form.get(p, {}).get("rel_err_vs_fp64"),
+                          "clocks": clk_form[p].summary()} for p in forms},
             "compute": {"fp32_fft_gflop_per_step": round(flops / 1e9, 2),
                         "achieved_tflops": round(flops / (ms * 1e-3) / 1e12, 2)},
             "gpu_launches": gpu_launches,
@@ -257,10 +298,10 @@ def gpu_arm(args):
         }
         if not args.no_cpu_baseline and world == 1:
             line["cpu_baseline"] = cpu_baseline(args.cpu_sample_z)
-        if not args.no_accuracy:
+        if acc_form:
             # outside the timed region: 2 of the 64 planes against the FP64 oracle
-            line["accuracy"] = accuracy_check(dev)
-            line["rel_err_vs_fp64"] = line["accuracy"]["rel_err_vs_fp64"]
+            line["accuracy"] = acc_form[best]
+            line["rel_err_vs_fp64"] = acc_form[best]["rel_err_vs_fp64"]
     if not args.no_serve:
         # a short Poisson stream of the serving configuration (latency beside throughput)
         serve = run_serve_stream(dev, rank, world, dist, args.rate, args.headline_serve_seconds)
@@ -328,21 +369,24 @@ def dominant_kernel_time(dev, z, phase_d, dx):
     return {"ms": e0.elapsed_time(e1) / reps, "zc": zc, "rowsum": rowsum, "launches_per_step": 1 + 2 * nchunks}
 
 
-def accuracy_check(dev):
-    """Relative L2 error of the CUDA PSF vs the FP64 oracle on 2 defocus planes
-    (the first and the last), and the reference-order float32 restatement's
-    own error on the same planes."""
+def accuracy_check(dev, form="accurate"):
+    """Relative L2 error of the CUDA PSF (transform form ``form``) vs the FP64
+    oracle on 2 defocus planes (the first and the last), and the
+    reference-order float32 restatement's own error on the same planes."""
     import torch
 
+    import chromatix_b200 as cx
     import chromatix_b200.functional as cf
     from oracle import chromatix_oracle as O
 
     z, phase, dx = inputs(seed=0)
     zz = z[[0, NZ - 1]]
     spec = (WAVELENGTHS, np.ones(NWV))
-    f = cf.ff_lens(cf.phase_change(cf.objective_point_source((N, N), dx, spec, zz, F_OBJ, N_MED, NA, device=dev),
-                                   torch.as_tensor(phase, device=dev)), F_TUBE, N_MED)
-    I = f.intensity.cpu().numpy()
+    with cx.precision(form):
+        f = cf.ff_lens(cf.phase_change(cf.objective_point_source((N, N), dx, spec, zz, F_OBJ, N_MED, NA,
+                                                                 device=dev),
+                                       torch.as_tensor(phase, device=dev)), F_TUBE, N_MED)
+        I = f.intensity.cpu().numpy()
     O.set_fft_workers(os.cpu_count())
     o = O.ff_lens(O.phase_change(O.objective_point_source((N, N), dx, spec, zz, F_OBJ, N_MED, NA), phase),
                   F_TUBE, N_MED).intensity
@@ -949,6 +993,7 @@ def main():
     ap.add_argument("--no-accuracy", action="store_true",
                     help="skip the error against the FP64 oracle (computed outside the timed region)")
     ap.add_argument("--no-serve", action="store_true", help="psf: skip the short serving stream (latency_ms)")
+    ap.add_argument("--no-split16", action="store_true", help="psf: time the plain FP32 transform form only")
     ap.add_argument("--headline-serve-seconds", type=float, default=1.0,
                     help="psf: length of the serving stream whose latency the headline line reports")
     ap.add_argument("--workload", default="psf",

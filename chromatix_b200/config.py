@@ -7,6 +7,11 @@
 * ``"ref32"``: FP32 in the reference's operation order, reproducing the
   argument rounding of Chromatix's float32 JAX path (e.g. ~1.3e-4 relative
   L2 for angular-spectrum propagation at z = 100 um).
+* ``"split16"``: as ``"accurate"``, with the transform stages of the passes
+  that have a tensor-core form (the PSF column pass at 1024 / 1280 rows) run
+  as dense DFT contractions on FP16 hi + lo operands with FP32 accumulation
+  (~2e-7 relative error per transform); every other pass runs as
+  ``"accurate"``.
 """
 
 from __future__ import annotations
@@ -14,7 +19,7 @@ from __future__ import annotations
 import contextlib
 
 _PRECISION = "accurate"
-_VALID = ("accurate", "ref32")
+_VALID = ("accurate", "ref32", "split16")
 
 
 def get_precision() -> str:
@@ -38,8 +43,12 @@ def precision(p: str):
         set_precision(old)
 
 
-def precision_code(p: str | None = None) -> int:
+def precision_code(p: str | None = None, tensor_core: bool = False) -> int:
+    """cx_precision of ``p`` for one entry point; ``tensor_core``: the entry
+    point accepts CX_PREC_SPLIT16 (elsewhere "split16" means "accurate")."""
     p = p or _PRECISION
     if p not in _VALID:
         raise ValueError(f"precision must be one of {_VALID}, got {p!r}")
+    if p == "split16":
+        return 2 if tensor_core else 0
     return 0 if p == "accurate" else 1

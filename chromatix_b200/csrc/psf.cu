@@ -183,6 +183,15 @@ static cx_status psf_check(const cx_psf_desc* d) {
     set_error("cx_psf_4f needs a forward lens (f_lens > 0); use cx_optical_fft for inverse lenses");
     return CX_ERR_INVALID;
   }
+  if (d->precision < 0 || d->precision > 2) {
+    set_error("invalid PSF precision %d", d->precision);
+    return CX_ERR_INVALID;
+  }
+  if (d->precision == CX_PREC_SPLIT16 && !psf_tc_supported(d->ny, d->nx)) {
+    set_error("CX_PREC_SPLIT16 PSF: grid %dx%d not compiled in (ny 1024 or 1280, nx a multiple of 8)", d->ny,
+              d->nx);
+    return CX_ERR_UNSUPPORTED;
+  }
   return CX_OK;
 }
 
@@ -346,7 +355,7 @@ extern "C" cx_status cx_psf_4f(const cx_psf_desc* d, const cx_psf_spectrum* spec
     a.z0 = z0;
     a.zc = (a.nz - z0) < zc ? (a.nz - z0) : zc;
     if ((s = psf_dispatch_rows(a.nx, a, st)) != CX_OK) return s;
-    if ((s = psf_dispatch_cols(a.ny, a, st)) != CX_OK) return s;
+    if ((s = psf_cols(a, st)) != CX_OK) return s;
   }
   return CX_OK;
 }
@@ -387,7 +396,7 @@ extern "C" cx_status cx_psf_4f_stage(const cx_psf_desc* d, const cx_psf_spectrum
     return CX_ERR_INVALID;
   }
   a.zc = (a.nz - a.z0) < zc ? (a.nz - a.z0) : zc;
-  return stage == 0 ? psf_dispatch_rows(a.nx, a, st) : psf_dispatch_cols(a.ny, a, st);
+  return stage == 0 ? psf_dispatch_rows(a.nx, a, st) : psf_cols(a, st);
 }
 
 // ---------------------------------------------------------------------------

@@ -316,4 +316,10 @@ inline int psf_edge_q(const PsfArgs& a, bool rows, int n, int r0) {
 
 cx_status psf_dispatch_rows(int n, const PsfArgs& a, cudaStream_t st);
 cx_status psf_dispatch_cols(int n, const PsfArgs& a, cudaStream_t st);
+// CX_PREC_SPLIT16 column pass on the tensor cores (psf_tc.cu)
+bool psf_tc_supported(int ny, int nx);
+cx_status psf_dispatch_cols_tc(int n, const PsfArgs& a, cudaStream_t st);
+inline cx_status psf_cols(const PsfArgs& a, cudaStream_t st) {
+  return a.precision == CX_PREC_SPLIT16 ? psf_dispatch_cols_tc(a.ny, a, st) : psf_dispatch_cols(a.ny, a, st);
+}
 }  // namespace cx

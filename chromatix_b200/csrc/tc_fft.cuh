@@ -1,0 +1,277 @@
+// Column FFTs of length N = N1 * N2 on the tensor cores (four-step form,
+// split FP16 precision), eight columns per CTA of 256 threads.
+//
+//   X[k1 + N1 k2] = sum_n2 W_N2^(n2 k2) W_N^(n2 k1) sum_n1 W_N1^(n1 k1) x[N2 n1 + n2]
+//
+// Stage 1: for every (n2, v) a length-N1 DFT over n1 -- one real GEMM per
+// 128-row tile, rows m = 8 n2 + v, K = (re | im) of n1, the DFT matrix as B.
+// Twiddle W_N^(n2 k1) in FP32 on the way out of tensor memory.
+// Stage 2: for every (v, k1) a length-N2 DFT over n2 -- rows m = N1 v + k1.
+// Both A operands are MN-major (rows contiguous within 16-byte chunks), so
+// the loader writes eight columns of one input row as one chunk and a stage-1
+// thread (one row (n2, v)) writes its N1 outputs as N1/8 chunks of stage 2's
+// A: no transposes through shared memory.
+//
+// Precision: FP32 values enter as FP16 hi + lo pairs, D = Ahi Bhi + Alo Bhi +
+// Ahi Blo in FP32 (tensor memory); the tile is scaled by a power of two
+// (exact) per column so that column's largest input component is near 2^9,
+// which keeps every stage-1 output below FP16's maximum (N1 * 2^9 sqrt 2 <
+// 65504 for N1 <= 64) and puts hi and lo in FP16's normal range.  The
+// relative error per column transform is ~2e-7.
+//
+// The caller builds B1 / B2 once (tc_fft_build_b), allocates tensor memory
+// (TMEM_COLS) and an mbarrier, and calls tc_fft_tile per column tile with a
+// loader (8 input columns of FFT row n) and a store (output bin k of column
+// v).  Every mbarrier wait is bounded; tc_fft_tile returns false (uniformly
+// over the CTA) if one ran out.
+#pragma once
+#include "host.cuh"
+#include "tcgen05.cuh"
+
+namespace cx {
+
+template <int N1_, int N2_>
+struct TcFft {
+  static constexpr int N1 = N1_, N2 = N2_, N = N1 * N2;
+  static constexpr int V = 8, THREADS = 256;
+  static constexpr int M1 = V * N2, T1 = M1 / 128;          // stage-1 rows (n2, v), tiles
+  static constexpr int M2 = V * N1, T2 = (M2 + 127) / 128;  // stage-2 rows (v, k1), tiles (last one padded)
+  static constexpr int K1 = 2 * N1, K2 = 2 * N2;           // (re | im) inputs = outputs per stage
+  static constexpr uint32_t A1_TILE = 128u * K1 * 2u;       // bytes of one tile of hi (or lo)
+  static constexpr uint32_t A2_TILE = 128u * K2 * 2u;
+  static constexpr uint32_t A1_BYTES = 2u * T1 * A1_TILE;   // hi tiles, then lo tiles
+  static constexpr uint32_t A2_BYTES = 2u * T2 * A2_TILE;
+  static constexpr uint32_t A_BYTES = A1_BYTES > A2_BYTES ? A1_BYTES : A2_BYTES;  // stage 2 reuses stage 1's space
+  static constexpr uint32_t B1_BYTES = 2u * K1 * K1 * 2u;   // hi, lo
+  static constexpr uint32_t B2_BYTES = 2u * K2 * K2 * 2u;
+  static constexpr uint32_t SMEM = A_BYTES + B1_BYTES + B2_BYTES;
+  static constexpr int RPT = N / THREADS;                   // input rows per thread
+  static constexpr int TMEM_NEED = (T1 * K1 > T2 * K2) ? T1 * K1 : T2 * K2;
+  static constexpr int TMEM_COLS = TMEM_NEED <= 64 ? 64 : TMEM_NEED <= 128 ? 128 : TMEM_NEED <= 256 ? 256 : 512;
+  static constexpr int POLLS = 1 << 18;
+  static_assert(N1 % 8 == 0 && N2 % 16 == 0 && M1 % 128 == 0, "tile shapes");
+  static_assert(T1 == 2, "one stage-1 row per thread (256 threads, two 128-row tiles)");
+  static_assert(K1 <= 256 && K2 <= 256 && K1 % 16 == 0 && K2 % 16 == 0, "MMA N / K");
+  static_assert(N % THREADS == 0, "rows per thread");
+  static_assert(N1 <= 64, "stage-1 output range stays inside FP16");
+};
+
+struct TcFftSmem {
+  uint8_t* A;   // A1 / A2 (hi tiles then lo tiles)
+  uint8_t* B1;  // hi then lo
+  uint8_t* B2;
+  uint64_t* bar;
+  float* red;   // 64 floats: per-warp column maxima (kept until the tile's output is stored)
+};
+
+// real-expanded DFT matrix of length R as a K-major B operand (2R x 2R):
+// row j = output (re | im), column k = input (re | im); hi at B, lo at B + 4 R^2 bytes
+template <int R>
+__device__ void tc_fft_build_b(uint8_t* B, bool inverse, int tid, int nthreads) {
+  constexpr int K = 2 * R;
+  const double sgn = inverse ? 1.0 : -1.0;
+  for (int idx = tid; idx < K * K; idx += nthreads) {
+    const int j = idx / K, k = idx % K;
+    const int n = k % R, kk = j % R, pin = k / R, pout = j / R;
+    double sd, cd;
+    sincospi(sgn * 2.0 * (double)((n * kk) % R) / (double)R, &sd, &cd);
+    const float v = (float)(pin == pout ? cd : (pin == 0 ? sd : -sd));
+    const __half h = __float2half_rn(v);
+    const __half l = __float2half_rn(v - __half2float(h));
+    *reinterpret_cast<__half*>(B + tc::off_kmajor(K, j, k)) = h;
+    *reinterpret_cast<__half*>(B + K * K * 2 + tc::off_kmajor(K, j, k)) = l;
+  }
+}
+
+// 8 values (one 16-byte chunk of an operand) split and stored as hi / lo
+__device__ __forceinline__ void tc_store_chunk(uint8_t* hi_base, uint8_t* lo_base, uint32_t off, const float* v8) {
+  uint32_t hi[4], lo[4];
+#pragma unroll
+  for (int q = 0; q < 4; ++q) tc::split2(v8[2 * q], v8[2 * q + 1], hi[q], lo[q]);
+  *reinterpret_cast<uint4*>(hi_base + off) = make_uint4(hi[0], hi[1], hi[2], hi[3]);
+  *reinterpret_cast<uint4*>(lo_base + off) = make_uint4(lo[0], lo[1], lo[2], lo[3]);
+}
+
+// One tile of eight columns.  load8(n, float2 out[8]): the 8 columns of FFT
+// input row n; store(k, v, X): output bin k of column v.  tw: twiddles
+// exp(-2 pi i e / N), e < N (shared or global).  Returns false if an MMA wait
+// ran out (then no output was stored for this tile).
+template <class F, class Load8, class Store>
+__device__ bool tc_fft_tile(const TcFftSmem& S, uint32_t tmem, uint32_t& phase, const float2* __restrict__ tw,
+                            bool inverse, Load8 load8, Store store) {
+  constexpr int N1 = F::N1, N2 = F::N2, N = F::N, K1 = F::K1, K2 = F::K2;
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+
+  // ---- load 8 columns of RPT rows; per-column maximum and power-of-two
+  // scale (a row scale of both GEMMs: rows (n2, v) and (v, k1) carry v)
+  float2 xv[F::RPT][8];
+  float mx[8];
+#pragma unroll
+  for (int v = 0; v < 8; ++v) mx[v] = 0.f;
+#pragma unroll
+  for (int i = 0; i < F::RPT; ++i) {
+    load8(tid + i * F::THREADS, xv[i]);
+#pragma unroll
+    for (int v = 0; v < 8; ++v) mx[v] = fmaxf(mx[v], fmaxf(fabsf(xv[i][v].x), fabsf(xv[i][v].y)));
+  }
+#pragma unroll
+  for (int v = 0; v < 8; ++v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) mx[v] = fmaxf(mx[v], __shfl_xor_sync(0xffffffffu, mx[v], o));
+  }
+  if (lane == 0) {
+#pragma unroll
+    for (int v = 0; v < 8; ++v) S.red[warp * 8 + v] = mx[v];
+  }
+  __syncthreads();
+  float sc[8];
+#pragma unroll
+  for (int v = 0; v < 8; ++v) {
+    float m = S.red[v];
+#pragma unroll
+    for (int w = 1; w < 8; ++w) m = fmaxf(m, S.red[w * 8 + v]);
+    int e = 0;
+    if (m > 0.f) frexpf(m, &e);
+    sc[v] = ldexpf(1.f, 9 - e);
+  }
+
+  // ---- stage-1 A (MN-major): row m = 8 n2 + v, column k = part N1 + n1
+  uint8_t* A1hi = S.A;
+  uint8_t* A1lo = S.A + F::T1 * F::A1_TILE;
+#pragma unroll
+  for (int i = 0; i < F::RPT; ++i) {
+    const int n = tid + i * F::THREADS;
+    const int n1 = n / N2, n2 = n % N2;
+    const int t = n2 >> 4;  // 16 values of n2 per 128-row tile
+    const uint32_t tile = (uint32_t)t * F::A1_TILE;
+    float re[8], im[8];
+#pragma unroll
+    for (int v = 0; v < 8; ++v) {
+      re[v] = xv[i][v].x * sc[v];
+      im[v] = xv[i][v].y * sc[v];
+    }
+    tc_store_chunk(A1hi + tile, A1lo + tile, tc::off_mnmajor(128, (n2 & 15) * 8, n1), re);
+    tc_store_chunk(A1hi + tile, A1lo + tile, tc::off_mnmajor(128, (n2 & 15) * 8, N1 + n1), im);
+  }
+  tc::fence_smem_to_async();
+  tc::fence_before_sync();
+  __syncthreads();
+  if (tid == 0) {
+    tc::fence_after_sync();
+    constexpr uint32_t id1 = tc::idesc_f16_f32(128, K1, 1, 0);
+    constexpr uint32_t a_lbo = 16 * 128, b_lbo = (K1 / 8) * 128;
+    const uint32_t b1h = tc::smem_u32(S.B1), b1l = b1h + K1 * K1 * 2;
+#pragma unroll
+    for (int t = 0; t < F::T1; ++t) {
+      const uint32_t ah = tc::smem_u32(A1hi) + t * F::A1_TILE, al = tc::smem_u32(A1lo) + t * F::A1_TILE;
+      const uint32_t d = tmem + t * K1;
+#pragma unroll
+      for (int s = 0; s < K1 / 16; ++s) {
+        const uint64_t dah = tc::smem_desc(ah + s * 2 * a_lbo, a_lbo, 128);
+        const uint64_t dal = tc::smem_desc(al + s * 2 * a_lbo, a_lbo, 128);
+        const uint64_t dbh = tc::smem_desc(b1h + s * 2 * b_lbo, b_lbo, 128);
+        const uint64_t dbl = tc::smem_desc(b1l + s * 2 * b_lbo, b_lbo, 128);
+        tc::mma_f16(d, dah, dbh, id1, s > 0 ? 1u : 0u);
+        tc::mma_f16(d, dal, dbh, id1, 1u);
+        tc::mma_f16(d, dah, dbl, id1, 1u);
+      }
+    }
+    tc::mma_commit(S.bar);
+  }
+  bool ok = tc::mbar_wait(S.bar, phase, F::POLLS);
+  phase ^= 1u;
+  if (!__syncthreads_and(ok)) return false;
+  tc::fence_after_sync();
+
+  // ---- stage-1 result: thread = row (n2, v) of tile warp / 4; twiddle; stage-2 A
+  {
+    const int t = warp >> 2;
+    const int m = t * 128 + (warp & 3) * 32 + lane;
+    const int n2 = m >> 3, v = m & 7;
+    float d[K1];
+#pragma unroll
+    for (int c = 0; c < K1; c += 16) tc::tmem_ld16(tmem + ((uint32_t)((warp & 3) * 32) << 16) + t * K1 + c, d + c);
+    tc::tmem_wait_ld();
+    uint8_t* A2hi = S.A;
+    uint8_t* A2lo = S.A + F::T2 * F::A2_TILE;
+#pragma unroll
+    for (int c = 0; c < N1 / 8; ++c) {
+      float re[8], im[8];
+#pragma unroll
+      for (int q = 0; q < 8; ++q) {
+        const int k1 = 8 * c + q;
+        int ex = n2 * k1;
+        ex = ex - (ex / N) * N;
+        const float2 w = tw[ex];
+        const float wr = w.x, wi = inverse ? -w.y : w.y;
+        const float a = d[k1], b = d[N1 + k1];
+        re[q] = a * wr - b * wi;
+        im[q] = a * wi + b * wr;
+      }
+      const int m2 = v * N1 + 8 * c;  // 8 consecutive rows (v, k1)
+      const uint32_t tile = (uint32_t)(m2 >> 7) * F::A2_TILE;
+      tc_store_chunk(A2hi + tile, A2lo + tile, tc::off_mnmajor(128, m2 & 127, n2), re);
+      tc_store_chunk(A2hi + tile, A2lo + tile, tc::off_mnmajor(128, m2 & 127, N2 + n2), im);
+    }
+  }
+  tc::fence_smem_to_async();
+  tc::fence_before_sync();
+  __syncthreads();
+  if (tid == 0) {
+    tc::fence_after_sync();
+    constexpr uint32_t id2 = tc::idesc_f16_f32(128, K2, 1, 0);
+    constexpr uint32_t a_lbo = 16 * 128, b_lbo = (K2 / 8) * 128;
+    uint8_t* A2hi = S.A;
+    uint8_t* A2lo = S.A + F::T2 * F::A2_TILE;
+    const uint32_t b2h = tc::smem_u32(S.B2), b2l = b2h + K2 * K2 * 2;
+#pragma unroll
+    for (int j = 0; j < F::T2; ++j) {
+      const uint32_t ah = tc::smem_u32(A2hi) + j * F::A2_TILE, al = tc::smem_u32(A2lo) + j * F::A2_TILE;
+      const uint32_t d = tmem + j * K2;
+#pragma unroll
+      for (int s = 0; s < K2 / 16; ++s) {
+        const uint64_t dah = tc::smem_desc(ah + s * 2 * a_lbo, a_lbo, 128);
+        const uint64_t dal = tc::smem_desc(al + s * 2 * a_lbo, a_lbo, 128);
+        const uint64_t dbh = tc::smem_desc(b2h + s * 2 * b_lbo, b_lbo, 128);
+        const uint64_t dbl = tc::smem_desc(b2l + s * 2 * b_lbo, b_lbo, 128);
+        tc::mma_f16(d, dah, dbh, id2, s > 0 ? 1u : 0u);
+        tc::mma_f16(d, dal, dbh, id2, 1u);
+        tc::mma_f16(d, dah, dbl, id2, 1u);
+      }
+    }
+    tc::mma_commit(S.bar);
+  }
+  ok = tc::mbar_wait(S.bar, phase, F::POLLS);
+  phase ^= 1u;
+  if (!__syncthreads_and(ok)) return false;
+  tc::fence_after_sync();
+
+  // ---- stage-2 result: row (v, k1) holds X[k1 + N1 k2], k2 < N2
+#pragma unroll
+  for (int j0 = 0; j0 < F::T2; j0 += 2) {
+    const int j = j0 + (warp >> 2);
+    if (j < F::T2) {  // whole warps: tcgen05.ld is warp-collective
+      float d[K2];
+#pragma unroll
+      for (int c = 0; c < K2; c += 16) tc::tmem_ld16(tmem + ((uint32_t)((warp & 3) * 32) << 16) + j * K2 + c, d + c);
+      tc::tmem_wait_ld();
+      const int m2 = j * 128 + (warp & 3) * 32 + lane;
+      if (m2 < F::M2) {
+        const int v = m2 / N1, k1 = m2 - v * N1;
+        float mv = S.red[v];
+#pragma unroll
+        for (int w = 1; w < 8; ++w) mv = fmaxf(mv, S.red[w * 8 + v]);
+        int e = 0;
+        if (mv > 0.f) frexpf(mv, &e);
+        const float isc = ldexpf(1.f, e - 9);
+#pragma unroll
+        for (int k2 = 0; k2 < N2; ++k2) store(k1 + N1 * k2, v, make_float2(d[k2] * isc, d[N2 + k2] * isc));
+      }
+    }
+  }
+  tc::fence_before_sync();
+  __syncthreads();
+  return true;
+}
+
+}  // namespace cx

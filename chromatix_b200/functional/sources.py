@@ -111,7 +111,9 @@ class LazySourceField(Field):
         d.ny, d.nx = ny, nx
         d.n_z = int(r["nz"])
         d.n_wv = self.spectrum.size
-        d.precision = config.precision_code(r["precision"])
+        # the fused pipeline's column pass has a tensor-core form at 1024 / 1280 rows
+        tc = r.get("lens") is not None and ny in (1024, 1280) and nx % 8 == 0
+        d.precision = config.precision_code(r["precision"], tensor_core=tc)
         d.has_phase = 1 if r.get("phase") is not None else 0
         d.spectrally_modulate = 1 if r.get("spectrally_modulate", True) else 0
         d.normalize_power = 0 if r["power"] is None else 1

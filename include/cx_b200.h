@@ -44,7 +44,10 @@ typedef enum {
 
 typedef enum {
   CX_PREC_ACCURATE = 0, /* FP64 phase arguments reduced mod 2pi, FP32 FFT */
-  CX_PREC_REF32 = 1     /* FP32 in the reference's operation order */
+  CX_PREC_REF32 = 1,    /* FP32 in the reference's operation order */
+  CX_PREC_SPLIT16 = 2   /* as ACCURATE, with the transform stages of the passes that have a tensor-core
+                           form (the PSF column pass at 1024 / 1280 rows) run as dense DFT contractions on
+                           FP16 hi + lo operands, FP32 accumulation; other entry points reject it */
 } cx_precision;
 
 typedef enum {
