@@ -7,9 +7,11 @@
 * ``"ref32"``: FP32 in the reference's operation order, reproducing the
   argument rounding of Chromatix's float32 JAX path (e.g. ~1.3e-4 relative
   L2 for angular-spectrum propagation at z = 100 um).
-* ``"split16"``: as ``"accurate"``, with the transform stages of the passes
-  that have a tensor-core form (the PSF column pass at 1024 / 1280 rows) run
-  as dense DFT contractions on FP16 hi + lo operands with FP32 accumulation
+* ``"split16"``: as ``"accurate"``, with the column transforms of the passes
+  that have a tensor-core form -- the PSF column pass and the Fourier-
+  multiplier column pass of the propagators and the multislice slice loop,
+  on padded grids of 1024 or 1280 rows (columns a multiple of 8) -- run as
+  dense DFT contractions on FP16 hi + lo operands with FP32 accumulation
   (~2e-7 relative error per transform); every other pass runs as
   ``"accurate"``.
 """
@@ -41,6 +43,11 @@ def precision(p: str):
         yield
     finally:
         set_precision(old)
+
+
+def tensor_core_grid(py: int, px: int) -> bool:
+    """Padded grids whose column transforms have a tensor-core form."""
+    return py in (1024, 1280) and px % 8 == 0 and px >= 8
 
 
 def precision_code(p: str | None = None, tensor_core: bool = False) -> int:

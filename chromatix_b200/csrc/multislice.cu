@@ -23,7 +23,7 @@ __global__ void k_ms_fill_h(float2* __restrict__ H, Prop2DArgs a, cx_plane pl) {
 
 static cx_status ms_plan(const cx_ms_desc* d, MsPlan* p) {
   if (!d || d->ny <= 0 || d->nx <= 0 || d->pad < 0 || d->n_slices <= 0 || !(d->wavelength > 0.0) ||
-      !(d->dy > 0.0) || !(d->dx > 0.0) || d->precision < 0 || d->precision > 1) {
+      !(d->dy > 0.0) || !(d->dx > 0.0) || d->precision < 0 || d->precision > 2) {
     set_error("invalid multislice descriptor");
     return CX_ERR_INVALID;
   }
@@ -31,6 +31,11 @@ static cx_status ms_plan(const cx_ms_desc* d, MsPlan* p) {
   p->px = d->nx + 2 * d->pad;
   if (!size_supported(p->py) || !size_supported(p->px)) {
     set_error("padded grid %dx%d: FFT length not supported", p->py, p->px);
+    return CX_ERR_UNSUPPORTED;
+  }
+  if (d->precision == CX_PREC_SPLIT16 && !prop_tc_supported(p->py, p->px)) {
+    set_error("CX_PREC_SPLIT16 multislice: padded grid %dx%d not compiled in (1024 or 1280 rows, columns a "
+              "multiple of 8)", p->py, p->px);
     return CX_ERR_UNSUPPORTED;
   }
   p->D = d->n_slices;
@@ -145,7 +150,7 @@ static cx_status col_pass(const MsPlan& p, const cx_plane* plane, float2* buf, d
     a.bandlimit = 0;
     a.remove_evanescent = 0;
   }
-  return dispatch_cols(p.py, buf, buf, a, st);
+  return prop_cols(p.py, buf, buf, a, st);
 }
 
 static cx_status fill_h(const cx_ms_desc* d, const MsPlan& p, float2* H, cudaStream_t st) {

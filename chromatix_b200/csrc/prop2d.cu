@@ -28,9 +28,15 @@ static cx_status make_args(const cx_prop2d_desc* d, Prop2DArgs* a) {
               d->pad_x, d->n_wv, d->n_in_planes, d->n_out_planes);
     return CX_ERR_INVALID;
   }
-  if (d->kernel < 0 || d->kernel > 3 || d->precision < 0 || d->precision > 1) {
+  if (d->kernel < 0 || d->kernel > 3 || d->precision < 0 || d->precision > 2) {
     set_error("invalid kernel kind or precision");
     return CX_ERR_INVALID;
+  }
+  if (d->precision == CX_PREC_SPLIT16 &&
+      !prop_tc_supported(d->ny + 2 * d->pad_y, d->nx + 2 * d->pad_x)) {
+    set_error("CX_PREC_SPLIT16 propagation: padded grid %dx%d not compiled in (1024 or 1280 rows, columns a "
+              "multiple of 8)", d->ny + 2 * d->pad_y, d->nx + 2 * d->pad_x);
+    return CX_ERR_UNSUPPORTED;
   }
   a->ny = d->ny;
   a->nx = d->nx;
@@ -123,7 +129,7 @@ extern "C" cx_status cx_prop2d(const cx_prop2d_desc* d, const cx_plane* planes_d
   float2* T2 = reinterpret_cast<float2*>(static_cast<char*>(workspace) + align256(ws_T_bytes(a)));
   cudaStream_t st = static_cast<cudaStream_t>(stream);
   if ((s = dispatch_rows_fwd(a.px, static_cast<const float2*>(u_in), T, a, st)) != CX_OK) return s;
-  if ((s = dispatch_cols(a.py, T, T2, a, st)) != CX_OK) return s;
+  if ((s = prop_cols(a.py, T, T2, a, st)) != CX_OK) return s;
   return dispatch_rows_inv(a.px, T2, static_cast<float2*>(u_out), a, st);
 }
 
@@ -155,7 +161,7 @@ extern "C" cx_status cx_prop2d_ptrs(const cx_prop2d_desc* d, const cx_plane* pla
   float2* T2 = reinterpret_cast<float2*>(static_cast<char*>(workspace) + align256(ws_T_bytes(a)));
   cudaStream_t st = static_cast<cudaStream_t>(stream);
   if ((s = dispatch_rows_fwd(a.px, nullptr, T, a, st)) != CX_OK) return s;
-  if ((s = dispatch_cols(a.py, T, T2, a, st)) != CX_OK) return s;
+  if ((s = prop_cols(a.py, T, T2, a, st)) != CX_OK) return s;
   return dispatch_rows_inv(a.px, T2, nullptr, a, st);
 }
 

@@ -299,4 +299,10 @@ __global__ void __launch_bounds__(RowCfg<NX>::THREADS, RowCfg<NX>::MINB) k_prop_
 cx_status dispatch_rows_fwd(int n, const float2* u, float2* T, const Prop2DArgs& a, cudaStream_t st);
 cx_status dispatch_cols(int n, const float2* T, float2* T2, const Prop2DArgs& a, cudaStream_t st);
 cx_status dispatch_rows_inv(int n, const float2* T2, float2* out, const Prop2DArgs& a, cudaStream_t st);
+// CX_PREC_SPLIT16 column pass on the tensor cores (prop2d_tc.cu)
+bool prop_tc_supported(int py, int px);
+cx_status dispatch_cols_tc(int n, const float2* T, float2* T2, const Prop2DArgs& a, cudaStream_t st);
+inline cx_status prop_cols(int n, const float2* T, float2* T2, const Prop2DArgs& a, cudaStream_t st) {
+  return a.precision == CX_PREC_SPLIT16 ? dispatch_cols_tc(n, T, T2, a, st) : dispatch_cols(n, T, T2, a, st);
+}
 }  // namespace cx

@@ -1,0 +1,139 @@
+// Column pass of the Fourier-multiplier propagation with the column FFTs on
+// the tensor cores (CX_PREC_SPLIT16): per (output plane, eight-column tile)
+// the four-step split-precision transform, x H(ky, kx) evaluated on the fly
+// (the accurate-mode propagator of prop2d.cuh), and the inverse transform
+// (tc_fft_mult_tile), writing only the output rows -- k_prop_cols with the
+// radix butterflies replaced by dense DFT contractions.  In place when T == T2
+// (the multislice slice loop): a tile is read completely before it is written.
+#include "prop2d.cuh"
+#include "tc_fft.cuh"
+
+namespace cx {
+
+template <int N1, int N2>
+struct PropTcCfg {
+  using F = TcFft<N1, N2>;
+  static constexpr int N = F::N;
+  static constexpr size_t TW_BYTES = sizeof(float2) * N;
+  static constexpr size_t SMEM = F::SMEM + TW_BYTES + 64 + 256;
+};
+
+template <int N1, int N2>
+__global__ void __launch_bounds__(256, 1) k_prop_cols_tc(const float2* T, float2* T2, Prop2DArgs a,
+                                                         const float2* __restrict__ twN) {
+  using F = TcFft<N1, N2>;
+  using C = PropTcCfg<N1, N2>;
+  constexpr int N = F::N;
+  extern __shared__ __align__(128) uint8_t smem[];
+  TcFftSmem S;
+  S.A = smem;
+  S.B1 = smem + F::A_BYTES;
+  S.B2 = S.B1 + F::B1_BYTES;
+  float2* tw = reinterpret_cast<float2*>(S.B2 + F::B2_BYTES);
+  S.bar = reinterpret_cast<uint64_t*>(reinterpret_cast<uint8_t*>(tw) + C::TW_BYTES);
+  uint32_t* tslot = reinterpret_cast<uint32_t*>(S.bar + 1);
+  S.red = reinterpret_cast<float*>(S.bar + 8);
+  const int tid = threadIdx.x;
+
+  tc_fft_build_b<N1>(S.B1, false, tid, blockDim.x);
+  tc_fft_build_b<N2>(S.B2, false, tid, blockDim.x);
+  for (int i = tid; i < N; i += blockDim.x) tw[i] = twN[i];
+  if ((tid >> 5) == 0) {
+    tc::tmem_alloc(tslot, F::TMEM_COLS);
+    tc::tmem_relinquish();
+  }
+  if (tid == 0) {
+    tc::mbar_init(S.bar, 1);
+    tc::mbar_init_fence();
+  }
+  tc::fence_smem_to_async();
+  tc::fence_before_sync();
+  __syncthreads();
+  tc::fence_after_sync();
+  const uint32_t tmem = *tslot;
+  uint32_t phase = 0;
+  bool failed = false;
+
+  const int tiles_x = a.px / 8;
+  const long total = (long)tiles_x * a.n_out_planes;
+  const float scale = 1.0f / ((float)a.py * (float)a.px);
+  long t = blockIdx.x;
+  for (; t < total; t += gridDim.x) {
+    const int q = (int)(t / tiles_x);
+    const int x0 = (int)(t % tiles_x) * 8;
+    const cx_plane pl = a.planes[q];
+    const float2* src = T + (size_t)pl.in_plane * a.ny * a.px + x0;
+    float2* dst = T2 + (size_t)q * a.out_ny * a.px + x0;
+    auto load8 = [&](int n, float2* o) {
+      const int r = n - a.pad_y;  // padded-grid row n holds data row n - pad_y
+      if (r >= 0 && r < a.ny) {
+        const float4* p = reinterpret_cast<const float4*>(src + (size_t)r * a.px);
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+          const float4 f = p[k];
+          o[2 * k] = make_float2(f.x, f.y);
+          o[2 * k + 1] = make_float2(f.z, f.w);
+        }
+      } else {
+#pragma unroll
+        for (int k = 0; k < 8; ++k) o[k] = make_float2(0.f, 0.f);
+      }
+    };
+    auto mult = [&](int k, int v, float2 X) { return cmul(X, prop_kernel(k, x0 + v, a, pl)); };
+    auto store_row = [&](int n, const float2* row) {
+      const int r = n - a.out_y0;
+      if (r >= 0 && r < a.out_ny) {
+        float4* p = reinterpret_cast<float4*>(dst + (size_t)r * a.px);
+#pragma unroll
+        for (int k = 0; k < 4; ++k)
+          p[k] = make_float4(row[2 * k].x * scale, row[2 * k].y * scale, row[2 * k + 1].x * scale,
+                             row[2 * k + 1].y * scale);
+      }
+    };
+    if (!tc_fft_mult_tile<F>(S, tmem, phase, tw, load8, mult, store_row)) {
+      failed = true;
+      break;
+    }
+  }
+  if (failed) {
+    // an MMA wait ran out: mark this CTA's unfinished output tiles invalid
+    // (NaN) and let the MMAs in flight finish (bounded) before freeing tensor memory
+    tc::mbar_wait(S.bar, phase ^ 1u, F::POLLS);
+    const float nan = __int_as_float(0x7fc00000);
+    for (; t < total; t += gridDim.x) {
+      const int q = (int)(t / tiles_x), x0 = (int)(t % tiles_x) * 8;
+      float2* dst = T2 + (size_t)q * a.out_ny * a.px + x0;
+      for (int idx = tid; idx < a.out_ny * 8; idx += blockDim.x) dst[(size_t)(idx >> 3) * a.px + (idx & 7)] =
+          make_float2(nan, nan);
+    }
+  }
+  tc::fence_before_sync();
+  __syncthreads();
+  if ((tid >> 5) == 0) tc::tmem_dealloc(tmem, F::TMEM_COLS);
+}
+
+template <int N1, int N2>
+static cx_status launch_prop_cols_tc(const float2* T, float2* T2, const Prop2DArgs& a, cudaStream_t st) {
+  using C = PropTcCfg<N1, N2>;
+  auto k = k_prop_cols_tc<N1, N2>;
+  CX_CUDA_TRY(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)C::SMEM));
+  const long items = (long)(a.px / 8) * a.n_out_planes;
+  int grid = sm_count();
+  if (items < grid) grid = (int)items;
+  k<<<grid, 256, C::SMEM, st>>>(T, T2, a, a.twg + tw_offset(C::N));
+  CX_LAUNCH_CHECK();
+  return CX_OK;
+}
+
+bool prop_tc_supported(int py, int px) { return (py == 1024 || py == 1280) && px % 8 == 0 && px >= 8; }
+
+cx_status dispatch_cols_tc(int n, const float2* T, float2* T2, const Prop2DArgs& a, cudaStream_t st) {
+  if (!prop_tc_supported(n, a.px)) {
+    set_error("split-precision column pass: padded grid %dx%d not compiled in (1024 or 1280 rows, columns a "
+              "multiple of 8)", n, a.px);
+    return CX_ERR_UNSUPPORTED;
+  }
+  return n == 1280 ? launch_prop_cols_tc<40, 32>(T, T2, a, st) : launch_prop_cols_tc<32, 32>(T, T2, a, st);
+}
+
+}  // namespace cx

@@ -92,6 +92,51 @@ __device__ __forceinline__ void tc_store_chunk(uint8_t* hi_base, uint8_t* lo_bas
   *reinterpret_cast<uint4*>(lo_base + off) = make_uint4(lo[0], lo[1], lo[2], lo[3]);
 }
 
+// Issue D[t] = A[t] B for T row tiles of 128 (3 split products per K step of
+// 16) and commit them to the mbarrier; called by one thread.  A tiles of
+// `tile_bytes` (hi tiles then lo tiles from `a`), B (K x K, K-major, hi then
+// lo), D[t] at tensor-memory columns tmem + t K.
+template <int K, int T>
+__device__ __forceinline__ void tc_issue(uint64_t* bar, uint32_t tmem, const uint8_t* a, uint32_t tile_bytes,
+                                         int a_mn, const uint8_t* b) {
+  tc::fence_after_sync();
+  const uint32_t id = tc::idesc_f16_f32(128, K, a_mn, 0);
+  constexpr uint32_t a_lbo = 16 * 128, b_lbo = (K / 8) * 128;
+  const uint32_t bh = tc::smem_u32(b), bl = bh + K * K * 2;
+  const uint32_t a0 = tc::smem_u32(a), lo_off = T * tile_bytes;
+#pragma unroll
+  for (int t = 0; t < T; ++t) {
+    const uint32_t ah = a0 + t * tile_bytes, al = ah + lo_off;
+#pragma unroll
+    for (int s = 0; s < K / 16; ++s) {
+      const uint64_t dah = tc::smem_desc(ah + s * 2 * a_lbo, a_lbo, 128);
+      const uint64_t dal = tc::smem_desc(al + s * 2 * a_lbo, a_lbo, 128);
+      const uint64_t dbh = tc::smem_desc(bh + s * 2 * b_lbo, b_lbo, 128);
+      const uint64_t dbl = tc::smem_desc(bl + s * 2 * b_lbo, b_lbo, 128);
+      tc::mma_f16(tmem + t * K, dah, dbh, id, s > 0 ? 1u : 0u);
+      tc::mma_f16(tmem + t * K, dal, dbh, id, 1u);
+      tc::mma_f16(tmem + t * K, dah, dbl, id, 1u);
+    }
+  }
+  tc::mma_commit(bar);
+}
+
+// the operand writes of this CTA are complete and visible to the tensor
+// core; thread 0 then issues the GEMM and everyone waits for it (bounded)
+template <int K, int T>
+__device__ __forceinline__ bool tc_gemm(const TcFftSmem& S, uint32_t tmem, uint32_t& phase, const uint8_t* a,
+                                        uint32_t tile_bytes, int a_mn, const uint8_t* b, int polls) {
+  tc::fence_smem_to_async();
+  tc::fence_before_sync();
+  __syncthreads();
+  if (threadIdx.x == 0) tc_issue<K, T>(S.bar, tmem, a, tile_bytes, a_mn, b);
+  const bool ok = tc::mbar_wait(S.bar, phase, polls);
+  phase ^= 1u;
+  if (!__syncthreads_and(ok)) return false;
+  tc::fence_after_sync();
+  return true;
+}
+
 // One tile of eight columns.  load8(n, float2 out[8]): the 8 columns of FFT
 // input row n; store(k, v, X): output bin k of column v.  tw: twiddles
 // exp(-2 pi i e / N), e < N (shared or global).  Returns false if an MMA wait
@@ -270,6 +315,200 @@ __device__ bool tc_fft_tile(const TcFftSmem& S, uint32_t tmem, uint32_t& phase, 
     }
   }
   tc::fence_before_sync();
+  __syncthreads();
+  return true;
+}
+
+// Fourier multiplier on eight columns: X = FFT_N(x) (forward four-step as in
+// tc_fft_tile), Y = mult(k, v, X) (e.g. X H(k, kx)), then the unnormalised
+// inverse transform in the transposed order, which starts from the rows
+// (v, k1) that the forward pass leaves in tensor memory:
+//   y[n2 + N2 n1] = sum_k1 W_N1^(-n1 k1) W_N^(-n2 k1) sum_k2 W_N2^(-n2 k2) Y[k1 + N1 k2],
+// with IDFT(u) = conj(DFT(conj(u))) so both inverse stages reuse B1 and B2.
+// Y is scaled by 2^-ceil(log2 N) before the inverse stages (|Y| <= N max|x|
+// for |H| <= 1); the result handed to store_rows is exact up to rounding:
+// y = N * IFFT(Y) (unnormalised).  store_row(n, const float2 row[8]) writes
+// output row n (8 columns); the rows are staged in shared memory first.
+template <class F, class Load8, class Mult, class StoreRow>
+__device__ bool tc_fft_mult_tile(const TcFftSmem& S, uint32_t tmem, uint32_t& phase, const float2* __restrict__ tw,
+                                 Load8 load8, Mult mult, StoreRow store_row) {
+  constexpr int N1 = F::N1, N2 = F::N2, N = F::N, K1 = F::K1, K2 = F::K2;
+  constexpr int LOG2N = N <= 1024 ? 10 : (N <= 2048 ? 11 : 12);
+  constexpr int ROUNDS = (F::T2 + 1) / 2;
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const uint32_t wl = (uint32_t)((warp & 3) * 32) << 16;
+
+  // ---- forward stages (as tc_fft_tile)
+  float2 xv[F::RPT][8];
+  float mx[8];
+#pragma unroll
+  for (int v = 0; v < 8; ++v) mx[v] = 0.f;
+#pragma unroll
+  for (int i = 0; i < F::RPT; ++i) {
+    load8(tid + i * F::THREADS, xv[i]);
+#pragma unroll
+    for (int v = 0; v < 8; ++v) mx[v] = fmaxf(mx[v], fmaxf(fabsf(xv[i][v].x), fabsf(xv[i][v].y)));
+  }
+#pragma unroll
+  for (int v = 0; v < 8; ++v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) mx[v] = fmaxf(mx[v], __shfl_xor_sync(0xffffffffu, mx[v], o));
+  }
+  if (lane == 0) {
+#pragma unroll
+    for (int v = 0; v < 8; ++v) S.red[warp * 8 + v] = mx[v];
+  }
+  __syncthreads();
+  float sc[8];
+#pragma unroll
+  for (int v = 0; v < 8; ++v) {
+    float m = S.red[v];
+#pragma unroll
+    for (int w = 1; w < 8; ++w) m = fmaxf(m, S.red[w * 8 + v]);
+    int e = 0;
+    if (m > 0.f) frexpf(m, &e);
+    sc[v] = ldexpf(1.f, 9 - e);
+  }
+  uint8_t* Ahi = S.A;
+#pragma unroll
+  for (int i = 0; i < F::RPT; ++i) {
+    const int n = tid + i * F::THREADS;
+    const int n1 = n / N2, n2 = n % N2;
+    const uint32_t tile = (uint32_t)(n2 >> 4) * F::A1_TILE;
+    float re[8], im[8];
+#pragma unroll
+    for (int v = 0; v < 8; ++v) {
+      re[v] = xv[i][v].x * sc[v];
+      im[v] = xv[i][v].y * sc[v];
+    }
+    tc_store_chunk(Ahi + tile, Ahi + F::T1 * F::A1_TILE + tile, tc::off_mnmajor(128, (n2 & 15) * 8, n1), re);
+    tc_store_chunk(Ahi + tile, Ahi + F::T1 * F::A1_TILE + tile, tc::off_mnmajor(128, (n2 & 15) * 8, N1 + n1), im);
+  }
+  if (!tc_gemm<K1, F::T1>(S, tmem, phase, S.A, F::A1_TILE, 1, S.B1, F::POLLS)) return false;
+  {
+    const int t = warp >> 2;
+    const int m = t * 128 + (warp & 3) * 32 + lane;
+    const int n2 = m >> 3, v = m & 7;
+    float d[K1];
+#pragma unroll
+    for (int c = 0; c < K1; c += 16) tc::tmem_ld16(tmem + wl + t * K1 + c, d + c);
+    tc::tmem_wait_ld();
+#pragma unroll
+    for (int c = 0; c < N1 / 8; ++c) {
+      float re[8], im[8];
+#pragma unroll
+      for (int q = 0; q < 8; ++q) {
+        const int k1 = 8 * c + q;
+        const float2 w = tw[(n2 * k1) % N];
+        re[q] = d[k1] * w.x - d[N1 + k1] * w.y;
+        im[q] = d[k1] * w.y + d[N1 + k1] * w.x;
+      }
+      const int m2 = v * N1 + 8 * c;
+      const uint32_t tile = (uint32_t)(m2 >> 7) * F::A2_TILE;
+      tc_store_chunk(Ahi + tile, Ahi + F::T2 * F::A2_TILE + tile, tc::off_mnmajor(128, m2 & 127, n2), re);
+      tc_store_chunk(Ahi + tile, Ahi + F::T2 * F::A2_TILE + tile, tc::off_mnmajor(128, m2 & 127, N2 + n2), im);
+    }
+  }
+  if (!tc_gemm<K2, F::T2>(S, tmem, phase, S.A, F::A2_TILE, 1, S.B2, F::POLLS)) return false;
+
+  // ---- multiplier on the rows (v, k1) (each holds every k2); the inverse
+  // stage A operand (K-major: row (v, k1), column (re | im) of k2) is written
+  // row by row into the space of stage 2's operand, whose GEMM has completed
+  // (tensor memory is overwritten only after the next barrier)
+  const float rs = ldexpf(1.f, -LOG2N);
+#pragma unroll
+  for (int r = 0; r < ROUNDS; ++r) {
+    const int j = 2 * r + (warp >> 2);
+    if (j < F::T2) {
+      float y[K2];
+#pragma unroll
+      for (int c = 0; c < K2; c += 16) tc::tmem_ld16(tmem + wl + j * K2 + c, y + c);
+      tc::tmem_wait_ld();
+      const int rl = (warp & 3) * 32 + lane;
+      const int m2 = j * 128 + rl;
+      if (m2 < F::M2) {
+        const int v = m2 / N1, k1 = m2 - v * N1;
+#pragma unroll
+        for (int k2 = 0; k2 < N2; ++k2) {
+          const float2 Y = mult(k1 + N1 * k2, v, make_float2(y[k2], y[N2 + k2]));
+          y[k2] = Y.x * rs;
+          y[N2 + k2] = -Y.y * rs;  // conj: the inverse stage runs the forward DFT matrix
+        }
+      } else {
+#pragma unroll
+        for (int c = 0; c < K2; ++c) y[c] = 0.f;  // padding rows of the last tile
+      }
+      const uint32_t tile = (uint32_t)j * F::A2_TILE;
+#pragma unroll
+      for (int c = 0; c < K2 / 8; ++c)
+        tc_store_chunk(Ahi + tile, Ahi + F::T2 * F::A2_TILE + tile, tc::off_kmajor(128, rl, 8 * c), y + 8 * c);
+    }
+  }
+  if (!tc_gemm<K2, F::T2>(S, tmem, phase, S.A, F::A2_TILE, 0, S.B2, F::POLLS)) return false;
+
+  // ---- D_A row (v, k1) = DFT_N2(conj Y) over k2 -> n2; times W_N^(n2 k1);
+  // inverse stage B operand, MN-major: row (v, n2) = N2 v + n2, column (re | im) of k1
+#pragma unroll
+  for (int r = 0; r < ROUNDS; ++r) {
+    const int j = 2 * r + (warp >> 2);
+    if (j < F::T2) {
+      float d[K2];
+#pragma unroll
+      for (int c = 0; c < K2; c += 16) tc::tmem_ld16(tmem + wl + j * K2 + c, d + c);
+      tc::tmem_wait_ld();
+      const int m2 = j * 128 + (warp & 3) * 32 + lane;
+      if (m2 < F::M2) {
+        const int v = m2 / N1, k1 = m2 - v * N1;
+#pragma unroll
+        for (int c = 0; c < N2 / 8; ++c) {
+          float re[8], im[8];
+#pragma unroll
+          for (int q = 0; q < 8; ++q) {
+            const int n2 = 8 * c + q;
+            const float2 w = tw[(n2 * k1) % N];
+            re[q] = d[n2] * w.x - d[N2 + n2] * w.y;
+            im[q] = d[n2] * w.y + d[N2 + n2] * w.x;
+          }
+          const int mb = v * N2 + 8 * c;
+          const uint32_t tile = (uint32_t)(mb >> 7) * F::A1_TILE;
+          // stage A's operand (K-major) is no longer read: the GEMM has completed
+          tc_store_chunk(Ahi + tile, Ahi + F::T1 * F::A1_TILE + tile, tc::off_mnmajor(128, mb & 127, k1), re);
+          tc_store_chunk(Ahi + tile, Ahi + F::T1 * F::A1_TILE + tile, tc::off_mnmajor(128, mb & 127, N1 + k1), im);
+        }
+      }
+    }
+  }
+  if (!tc_gemm<K1, F::T1>(S, tmem, phase, S.A, F::A1_TILE, 1, S.B1, F::POLLS)) return false;
+
+  // ---- D_B row (v, n2) holds conj(y[n2 + N2 n1]) / (rs sc_v), n1 < N1: stage
+  // rows in shared memory (the operands are no longer read), then store them
+  float2* stage = reinterpret_cast<float2*>(S.A);
+  {
+    const int t = warp >> 2;
+    const int m = t * 128 + (warp & 3) * 32 + lane;
+    const int v = m / N2, n2 = m - v * N2;
+    float d[K1];
+#pragma unroll
+    for (int c = 0; c < K1; c += 16) tc::tmem_ld16(tmem + wl + t * K1 + c, d + c);
+    tc::tmem_wait_ld();
+    float mv = S.red[v];
+#pragma unroll
+    for (int w = 1; w < 8; ++w) mv = fmaxf(mv, S.red[w * 8 + v]);
+    int e = 0;
+    if (mv > 0.f) frexpf(mv, &e);
+    const float back = ldexpf(1.f, e - 9 + LOG2N);  // undoes sc_v and rs
+    // column-major staging (lanes hold consecutive n2 of one column): conflict-free
+#pragma unroll
+    for (int n1 = 0; n1 < N1; ++n1) stage[v * N + n2 + N2 * n1] = make_float2(d[n1] * back, -d[N1 + n1] * back);
+  }
+  tc::fence_before_sync();
+  __syncthreads();
+  for (int n = tid; n < N; n += F::THREADS) {
+    float2 row[8];
+#pragma unroll
+    for (int v = 0; v < 8; ++v) row[v] = stage[v * N + n];
+    store_row(n, row);
+  }
   __syncthreads();
   return true;
 }

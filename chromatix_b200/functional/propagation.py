@@ -222,7 +222,7 @@ def _run_prop2d(field: Field, kernel: int, zs, zshape, n, pad_width, kykx=(0.0, 
     d.mode_same = 1 if mode == "same" else 0
     d.crop_y, d.crop_x = crop
     d.kernel = kernel
-    d.precision = config.precision_code(prec)
+    d.precision = config.precision_code(prec, tensor_core=config.tensor_core_grid(py, px))
     d.remove_evanescent = int(bool(remove_evanescent))
     d.bandlimit = int(bool(bandlimit))
     d.n_medium = float(n)

@@ -253,7 +253,8 @@ def multislice_thick_sample(field: Field, absorption_stack, dn_stack, n, thickne
         reverse_propagate_distance = thickness_per_slice * D / 2
     d = cx_ms_desc()
     d.ny, d.nx, d.pad, d.n_slices = ny, nx, int(pad_width), D
-    d.precision = config.precision_code(precision)
+    pp = (ny + 2 * int(pad_width), nx + 2 * int(pad_width))
+    d.precision = config.precision_code(precision, tensor_core=config.tensor_core_grid(*pp))
     d.remove_evanescent, d.bandlimit = int(bool(remove_evanescent)), int(bool(bandlimit))
     d.checkpoint_every = int(checkpoint_every)
     d.n_medium = float(n)

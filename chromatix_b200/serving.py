@@ -401,7 +401,7 @@ class PropagationServer:
         d.n_in_planes = d.n_out_planes = B
         d.mode_same = 1
         d.kernel = nat.CX_KERNEL_ASM if op == "asm" else nat.CX_KERNEL_TRANSFER
-        d.precision = config.precision_code(self.precision)
+        d.precision = config.precision_code(self.precision, tensor_core=config.tensor_core_grid(2 * N, 2 * N))
         d.n_medium = float(n)
         wsb = nat.c_size_t(0)
         nat.check(self.L.cx_prop2d_workspace_size(d, wsb))

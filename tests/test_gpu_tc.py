@@ -96,3 +96,89 @@ def test_split16_psf_matches_fp64_oracle(N):
     e16, e32 = rel(I16, ref), rel(I32, ref)
     assert e16 < 1e-5, (e16, e32)
     assert e16 < 3 * e32 + 1e-6, (e16, e32)
+
+
+@pytest.mark.parametrize("method,mode", [("asm", "full"), ("asm", "same"), ("transfer", "full"), ("exact", "same")])
+def test_split16_propagation_512_pad_256_matches_fp64(method, mode):
+    """The single-field propagation configuration (512^2, pad 256 -> 1024^2,
+    dx 0.3, lambda 0.532, n 1.33, z 100 um) with the column pass on the tensor
+    cores, batch of 3 fields: relative L2 <= 1e-5 against the FP64 oracle."""
+    import torch
+
+    import chromatix_b200 as cx
+    import chromatix_b200.functional as cf
+    from oracle import chromatix_oracle as O
+    from tests.helpers import oracle_field, rand_field, rel
+
+    u = np.stack([rand_field((512, 512), seed=s) for s in (1, 2, 3)])
+    f = cx.Field.build(torch.as_tensor(u, device="cuda"), 0.3, 0.532)
+    kw = dict(mode=mode)
+    with cx.precision("split16"):
+        if method == "transfer":
+            out = cf.transfer_propagate(f, 100.0, 1.33, 256, **kw).u
+        else:
+            out = cf.asm_propagate(f, 100.0, 1.33, 256, remove_evanescent=(method == "exact"), **kw).u
+    out = out.cpu().numpy()
+    for b in range(3):
+        fo = oracle_field(u[b], 0.3, 0.532)
+        if method == "transfer":
+            ref = O.transfer_propagate(fo, 100.0, 1.33, 256, **kw).u
+        else:
+            ref = O.asm_propagate(fo, 100.0, 1.33, 256, remove_evanescent=(method == "exact"), **kw).u
+        e = rel(out[b], ref)
+        assert e < 1e-5, (b, e)
+
+
+def test_split16_propagation_1280_grid_and_adjoint():
+    """A 640^2 field padded to 1280^2 (the 40 x 32 four-step) forward against
+    the oracle, and the gradient (conj(H) through the same tensor-core pass)
+    by the dot-product identity <A u, w> = <u, A^H w>."""
+    import torch
+
+    import chromatix_b200 as cx
+    import chromatix_b200.functional as cf
+    from oracle import chromatix_oracle as O
+    from tests.helpers import oracle_field, rand_field, rel
+
+    u = rand_field((640, 640), seed=9)
+    ut = torch.as_tensor(u, device="cuda").requires_grad_(True)
+    with cx.precision("split16"):
+        y = cf.asm_propagate(cx.Field.build(ut, 0.25, 0.6), 60.0, 1.0, 320, mode="same").u
+    ref = O.asm_propagate(oracle_field(u, 0.25, 0.6), 60.0, 1.0, 320, mode="same").u
+    assert rel(y.detach().cpu().numpy(), ref) < 1e-5
+    w = (np.random.default_rng(10).standard_normal(y.shape) + 1j).astype(np.complex64)
+    torch.real(torch.sum(torch.conj(torch.as_tensor(w, device="cuda")) * y)).backward()
+    lhs = np.vdot(y.detach().cpu().numpy().astype(np.complex128).ravel(), w.astype(np.complex128).ravel())
+    rhs = np.vdot(u.astype(np.complex128).ravel(), ut.grad.cpu().numpy().astype(np.complex128).ravel())
+    assert abs(lhs - rhs) <= 1e-5 * abs(lhs)
+
+
+def test_split16_multislice_1024_forward_and_gradient():
+    """Multislice at 1024^2 (the differentiable configuration's grid, 8 slices)
+    with the slice loop's column passes on the tensor cores: forward <= 1e-5
+    and dL/d dn <= 1e-4 against the FP64 restatement."""
+    import torch
+
+    import chromatix_b200 as cx
+    import chromatix_b200.functional as cf
+    from oracle import chromatix_oracle as O
+    from tests.helpers import cuda_field, rand_field, rel
+
+    D, N = 8, 1024
+    rng = np.random.default_rng(11)
+    u = rand_field((N, N), seed=12, amp=(0.9, 1.0))
+    dn = (0.02 * rng.standard_normal((D, N, N))).astype(np.float32)
+    ab = rng.uniform(0, 0.05, (D, N, N)).astype(np.float32)
+    target = rng.uniform(0.5, 1.5, (N, N))
+    O.set_fft_workers(8)
+    L64, gdn64, _, uo64 = O.multislice_loss_and_grad(u, dn.astype(np.float64), ab.astype(np.float64), target,
+                                                     1.33, 0.2, 0.532, 0.1)
+    dn_t = torch.as_tensor(dn, device="cuda").requires_grad_(True)
+    with cx.precision("split16"):
+        out = cf.multislice_thick_sample(cuda_field(u, 0.1, 0.532), torch.as_tensor(ab, device="cuda"), dn_t, 1.33,
+                                         0.2, 0, checkpoint_every=4)
+        loss = ((out.u.abs() ** 2 - torch.as_tensor(target, device="cuda", dtype=torch.float32)) ** 2).sum()
+        loss.backward()
+    assert rel(out.u.detach().cpu().numpy(), uo64) < 1e-5
+    assert abs(float(loss) - L64) / L64 < 1e-4
+    assert rel(dn_t.grad.cpu().numpy(), gdn64) < 1e-4
