@@ -183,6 +183,7 @@ _SIGS = {
         c_int32,
         [ctypes.POINTER(cx_ew_desc), c_void_p, c_double, c_double, c_double, c_double, c_void_p, c_void_p],
     ),
+    "cx_cmul_planar": (c_int32, [ctypes.POINTER(cx_ew_desc), c_void_p, c_void_p, c_int32, c_void_p, c_void_p]),
     "cx_pupil": (
         c_int32,
         [ctypes.POINTER(cx_ew_desc), c_int32, c_void_p, c_double, c_double, c_void_p, c_void_p, c_void_p],

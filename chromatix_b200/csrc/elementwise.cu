@@ -422,3 +422,40 @@ extern "C" cx_status cx_cvec_lincomb(int64_t n, const double* coef, const void* 
   CX_LAUNCH_CHECK();
   return CX_OK;
 }
+
+// ---------------------------------------------------------------------------
+// field x planar propagator: out[b, y, x, w] = u[b, y, x, w] H[b W + w, y, x]
+// (conj(H) when conj_h): the Fourier multiplier of kernel_propagate
+// (functional/propagation.py:391-394) for transform lengths the fused passes
+// do not cover (the transforms are then chirp-Z passes)
+// ---------------------------------------------------------------------------
+namespace cx {
+__global__ void k_cmul_planar(const float2* __restrict__ u, const float2* __restrict__ H, float2* __restrict__ out,
+                              long n, int W, long plane, int conj_h) {
+  for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x) {
+    const int w = (int)(i % W);
+    const long pix = i / W;  // b * plane + yx
+    const long b = pix / plane, yx = pix - b * plane;
+    float2 h = H[(b * W + w) * plane + yx];
+    if (conj_h) h = cconj(h);
+    out[i] = cmul(u[i], h);
+  }
+}
+}  // namespace cx
+
+extern "C" cx_status cx_cmul_planar(const cx_ew_desc* d, const void* u, const void* H, int32_t conj_h, void* out,
+                                    cx_stream_t stream) {
+  cx_status st = ew_check(d);
+  if (st != CX_OK) return st;
+  if (!u || !H || !out) {
+    set_error("cx_cmul_planar: null pointer argument");
+    return CX_ERR_INVALID;
+  }
+  const long plane = (long)d->ny * d->nx, n = d->n_batch * plane * d->n_wv;
+  if (n == 0) return CX_OK;
+  k_cmul_planar<<<ew_grid(n), 256, 0, static_cast<cudaStream_t>(stream)>>>(
+      static_cast<const float2*>(u), static_cast<const float2*>(H), static_cast<float2*>(out), n, d->n_wv, plane,
+      conj_h);
+  CX_LAUNCH_CHECK();
+  return CX_OK;
+}

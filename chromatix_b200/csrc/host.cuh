@@ -43,6 +43,10 @@ void set_error(const char* fmt, ...);
 // 4096-point input): 2^9 3^2, 2^10 5, 2^11 3, 2^10 7, 2^13.
 #define CX_FOR_EACH_LONG_SIZE(X) X(4608) X(5120) X(6144) X(7168) X(8192)
 #define CX_FOR_EACH_1D_SIZE(X) CX_FOR_EACH_SIZE(X) CX_FOR_EACH_LONG_SIZE(X)
+// The Fourier-multiplier propagation passes also take 8192 (a 4096^2 field
+// padded by 2048 per side, the reference's high-resolution band-limited ASM
+// example); a 8192-point row or column is one team of 512 lanes per CTA.
+#define CX_FOR_EACH_PROP_SIZE(X) CX_FOR_EACH_SIZE(X) X(8192)
 
 inline bool size_supported(int n) {
   switch (n) {
@@ -54,6 +58,8 @@ inline bool size_supported(int n) {
       return false;
   }
 }
+
+inline bool size_supported_prop(int n) { return size_supported(n) || n == 8192; }
 
 inline bool size_supported_1d(int n) {
   switch (n) {

@@ -77,7 +77,7 @@ static cx_status make_args(const cx_prop2d_desc* d, Prop2DArgs* a) {
   a->twg = nullptr;
   a->planes = nullptr;
   a->H = nullptr;
-  if (!size_supported(a->py) || !size_supported(a->px)) {
+  if (!size_supported_prop(a->py) || !size_supported_prop(a->px)) {
     set_error("padded grid %dx%d: FFT length not supported", a->py, a->px);
     return CX_ERR_UNSUPPORTED;
   }

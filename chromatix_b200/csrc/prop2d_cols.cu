@@ -20,7 +20,7 @@ cx_status dispatch_cols(int n, const float2* T, float2* T2, const Prop2DArgs& a,
 #define CX_CASE_(N) \
   case N:           \
     return launch_cols<N>(T, T2, a, st);
-    CX_FOR_EACH_SIZE(CX_CASE_)
+    CX_FOR_EACH_PROP_SIZE(CX_CASE_)
 #undef CX_CASE_
   }
   set_error("FFT length %d is not supported", n);

@@ -32,7 +32,7 @@ cx_status dispatch_rows_fwd(int n, const float2* u, float2* T, const Prop2DArgs&
 #define CX_CASE_(N) \
   case N:           \
     return launch_rows_fwd<N>(u, T, a, st);
-    CX_FOR_EACH_SIZE(CX_CASE_)
+    CX_FOR_EACH_PROP_SIZE(CX_CASE_)
 #undef CX_CASE_
   }
   set_error("FFT length %d is not supported", n);
@@ -44,7 +44,7 @@ cx_status dispatch_rows_inv(int n, const float2* T2, float2* out, const Prop2DAr
 #define CX_CASE_(N) \
   case N:           \
     return launch_rows_inv<N>(T2, out, a, st);
-    CX_FOR_EACH_SIZE(CX_CASE_)
+    CX_FOR_EACH_PROP_SIZE(CX_CASE_)
 #undef CX_CASE_
   }
   set_error("FFT length %d is not supported", n);

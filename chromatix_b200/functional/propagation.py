@@ -187,6 +187,94 @@ def _apply_prop(plan: _PropPlan, u):
     return _launch_prop2d(plan, u)
 
 
+def _fused_size(n: int) -> bool:
+    """Transform lengths of the fused propagation passes (2^a {1, 3, 5, 7} up to 4096, and 8192)."""
+    return n == 8192 or bool(nat.lib().cx_fft_size_supported(int(n)))
+
+
+_CMUL_FN = None
+
+
+def _cmul_planar(u, H, chromatic: bool):
+    """u (B, py, px[, W]) x planar H (B W, py, px) by the native multiplier; its
+    gradient with respect to u is g conj(H)."""
+    global _CMUL_FN
+    torch = nat.torch_mod()
+
+    def launch(x, conj):
+        W = x.shape[-1] if chromatic else 1
+        py, px = (x.shape[-3], x.shape[-2]) if chromatic else (x.shape[-2], x.shape[-1])
+        B = x.numel() // (py * px * W)
+        d = nat.cx_ew_desc(n_batch=B, ny=py, nx=px, n_wv=W, map_batched=1)
+        out = torch.empty_like(x)
+        nat.check(nat.lib().cx_cmul_planar(d, nat.ptr(x), nat.ptr(H), int(conj), nat.ptr(out),
+                                           nat.stream_handle(x.device)))
+        return out
+
+    if _CMUL_FN is None:
+        class _CMul(torch.autograd.Function):
+            @staticmethod
+            def forward(ctx, x, fn):
+                ctx.fn = fn
+                return fn(x.contiguous(), False)
+
+            @staticmethod
+            def backward(ctx, g):
+                return ctx.fn(g.to(torch.complex64).contiguous(), True), None
+
+        _CMUL_FN = _CMul
+    if nat.wants_grad(u):
+        return _CMUL_FN.apply(u, launch)
+    return launch(u.contiguous(), False)
+
+
+def _prop2d_general(field: Field, kernel: int, zs, zshape, n, pad, kykx, shift_yx, remove_evanescent,
+                    bandlimit, mode, crop_w, prec, H=None, h_index=None):
+    """kernel_propagate's FFT branch (functional/propagation.py:391-394) on a
+    padded grid whose lengths the fused passes do not cover: the 2D DFT and its
+    inverse as chirp-Z passes along y and x (an exact length-N DFT by
+    Bluestein's algorithm: a = 1, w = exp(-+2 pi i / N)), the propagator from
+    ``cx_fill_propagator`` (or the caller's table), the product by the native
+    planar multiplier.  Every step is a native kernel with an adjoint."""
+    from ..core.field import pad as pad_field
+    from ..utils.czt import czt_axis
+
+    torch = nat.torch_mod()
+    py_, px_ = pad
+    f = pad_field(field, (py_, px_)) if (py_ or px_) else field
+    py, px = f.spatial_shape
+    W = f.n_wv
+    chrom = bool(f.chromatic)
+    B = f.batch_shape
+    out_batch = tuple(np.broadcast_shapes(B, zshape))
+    spatial = (py, px) + ((W,) if chrom else ())
+    u = f.u.to(torch.complex64)
+    if tuple(B) != out_batch:
+        u = u.expand(out_batch + spatial)
+    u = u.reshape((-1,) + spatial)
+    ay, ax = (-3, -2) if chrom else (-2, -1)
+    if H is None:
+        Hp = _fill_propagator(f, kernel, zs if zshape else zs[:1], n, kykx, shift_yx, bandlimit, remove_evanescent,
+                              precision=prec)
+        # (z batch..., [wv,] py, px) -> planar per (output batch element, wavelength)
+        Hp = Hp.movedim(-1, -3) if chrom else Hp.unsqueeze(-3)
+        Hp = Hp.expand(out_batch + (W, py, px)).reshape(-1, py, px).contiguous()
+    else:
+        Hp = H[torch.as_tensor(np.asarray(h_index), device=H.device)].contiguous()
+    U = czt_axis(czt_axis(u, py, 1.0, np.exp(-2j * np.pi / py), axis=ay), px, 1.0, np.exp(-2j * np.pi / px), axis=ax)
+    U = _cmul_planar(U, Hp, chrom)
+    out = czt_axis(czt_axis(U, py, 1.0, np.exp(2j * np.pi / py), axis=ay, scale=1.0 / py), px, 1.0,
+                   np.exp(2j * np.pi / px), axis=ax, scale=1.0 / px)
+    out = out.reshape(out_batch + spatial)
+    cy, cx = crop_w
+    if cy or cx:
+        sl = [slice(None)] * out.ndim
+        sl[out.ndim + ay] = slice(cy, py - cy)
+        sl[out.ndim + ax] = slice(cx, px - cx)
+        out = out[tuple(sl)].contiguous()
+    return out
+
+
 def _pad_const(field: Field, pad_width, cval):
     """Field padded with the constant ``cval`` by the native pad kernel
     (core/field.py:534-549); its gradient is the crop of the output gradient."""
@@ -212,6 +300,10 @@ def _run_prop2d(field: Field, kernel: int, zs, zshape, n, pad_width, kykx=(0.0, 
         py_, px_ = 0, 0
     ny, nx = field.spatial_shape
     py, px = ny + 2 * py_, nx + 2 * px_
+    if not (_fused_size(py) and _fused_size(px)):
+        crop_w = (py_, px_) if mode == "same" else crop
+        return _prop2d_general(field, kernel, zs, zshape, n, (py_, px_), kykx, shift_yx, remove_evanescent, bandlimit,
+                               mode, crop_w, prec, H=H, h_index=h_index)
     planes, out_batch, nb_in, nb_out = _plan_planes(field, zs, zshape, py, px, shift_yx, bandlimit, prec, h_index)
     W = field.n_wv
     d = nat.cx_prop2d_desc()

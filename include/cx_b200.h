@@ -582,6 +582,12 @@ cx_status cx_pad(const cx_ew_desc* d, int32_t pad_y, int32_t pad_x, float cval_r
  * + origin; wv_params_dev: (n_wv, 3) doubles (dy, dx, amp). */
 cx_status cx_plane_wave(const cx_ew_desc* d, const double* wv_params_dev, double ky, double kx, double origin_y,
                         double origin_x, void* u, cx_stream_t stream);
+/* The Fourier multiplier of kernel_propagate (functional/propagation.py:391-394)
+ * for grids the fused passes do not cover (their transforms are chirp-Z passes):
+ * out[b, y, x, w] = u[b, y, x, w] H[b n_wv + w, y, x], conj(H) when conj_h; H
+ * planar (n_batch n_wv, ny, nx) as cx_fill_propagator writes it. */
+cx_status cx_cmul_planar(const cx_ew_desc* d, const void* u, const void* H, int32_t conj_h, void* out,
+                         cx_stream_t stream);
 /* Pupils (functional/pupils.py:17-67) on the field grid g = d_w (i - N/2) + origin:
  * kind 0 circular (|g|^2 <= p0^2), 1 square (max |g| <= p0), 2 super-Gaussian
  * exp(-(|g| / p0)^p1), 3 Tukey (alpha p1 on |g / extent|, extent (p2, p3));

@@ -181,13 +181,59 @@ def test_analytic_square_aperture_through_cuda():
     del cx
 
 
-def test_unsupported_sizes_fail_loudly():
-    import chromatix_b200.functional as cf
-    from chromatix_b200 import _native as nat
+@pytest.mark.parametrize("shape,pad,mode", [((11, 13), 0, "full"), ((11, 13), 3, "same"), ((37, 50), 5, "full")])
+def test_general_lengths_through_chirp_z_transforms(shape, pad, mode):
+    """Padded grids outside the fused passes' lengths (here 11 x 13, 17 x 19,
+    47 x 60) propagate through chirp-Z DFTs (the reference's jnp.fft takes any
+    length): FP64 oracle parity, chromatic and z-batched, and the gradient
+    identity <A u, w> = <u, A^H w>."""
+    import torch
 
-    u = rand_field((11, 13), seed=10)
-    with pytest.raises(nat.CxError):
-        cf.asm_propagate(cuda_field(u, 0.1, 0.5), 1.0, 1.0, 0)
+    import chromatix_b200.functional as cf
+
+    u = rand_field(shape, seed=10)
+    out = cf.asm_propagate(cuda_field(u, 0.1, 0.5), 1.0, 1.0, pad, mode=mode)
+    ref = O.asm_propagate(oracle_field(u, 0.1, 0.5), 1.0, 1.0, pad, mode=mode)
+    assert out.u.shape == ref.u.shape
+    assert rel(to_np(out.u), ref.u) < 1e-5
+    out = cf.transfer_propagate(cuda_field(u, 0.1, 0.5), 2.0, 1.0, pad, mode=mode)
+    ref = O.transfer_propagate(oracle_field(u, 0.1, 0.5), 2.0, 1.0, pad, mode=mode)
+    assert rel(to_np(out.u), ref.u) < 1e-5
+    spec = (np.array([0.5, 0.6]), np.array([1.0, 1.0]))
+    uc = np.stack([u, np.conj(u)], -1).astype(np.complex64)
+    zs = np.array([0.5, 1.5, 3.0])
+    out = cf.asm_propagate(cuda_field(uc, 0.1, spec), zs, 1.0, pad, mode=mode)
+    ref = O.asm_propagate(oracle_field(uc, 0.1, spec), zs, 1.0, pad, mode=mode)
+    assert out.u.shape == ref.u.shape
+    assert rel(to_np(out.u), ref.u) < 1e-5
+    ut = torch.as_tensor(u, device="cuda").requires_grad_(True)
+    import chromatix_b200 as cx
+
+    y = cf.asm_propagate(cx.Field.build(ut, 0.1, 0.5), 1.0, 1.0, pad, mode=mode).u
+    w = (np.random.default_rng(3).standard_normal(tuple(y.shape)) + 1j).astype(np.complex64)
+    torch.real(torch.sum(torch.conj(torch.as_tensor(w, device="cuda")) * y)).backward()
+    lhs = np.vdot(to_np(y).astype(np.complex128).ravel(), w.astype(np.complex128).ravel())
+    rhs = np.vdot(u.astype(np.complex128).ravel(), to_np(ut.grad).astype(np.complex128).ravel())
+    assert abs(lhs - rhs) <= 1e-5 * abs(lhs)
+
+
+def test_published_hires_band_limited_asm_8192():
+    """The reference's high-resolution example (docs/examples/
+    rescaled_propagation.ipynb): a 4096^2 field padded by 2048 to an 8192^2
+    transform, band-limited ASM, mode "same", against the FP64 oracle (64M
+    points, computed on all host cores)."""
+    import chromatix_b200.functional as cf
+
+    u = rand_field((4096, 4096), seed=31)
+    out = cf.asm_propagate(cuda_field(u, 0.3, 0.532), 400.0, 1.33, 2048, bandlimit=True, mode="same")
+    assert out.u.shape == (4096, 4096)
+    import os
+
+    O.set_fft_workers(os.cpu_count())
+    ref = O.asm_propagate(oracle_field(u, 0.3, 0.532), 400.0, 1.33, 2048, bandlimit=True, mode="same").u
+    O.set_fft_workers(None)
+    got = to_np(out.u)
+    assert rel(got, ref) < 1e-5
 
 
 def test_largest_grid_4096():
