@@ -74,6 +74,42 @@ __device__ __forceinline__ void cp_async_wait_group() {
   asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
 }
 
+// Bulk (TMA) copies global -> shared completing on an mbarrier: one thread
+// arms the barrier with the byte count of the copies it then issues; the
+// barrier's phase completes when every byte has landed.  Source, destination
+// and size must be multiples of 16 bytes.
+__device__ __forceinline__ void bulk_mbar_init(uint64_t* bar) {
+  const unsigned b = (unsigned)__cvta_generic_to_shared(bar);
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;\n" ::"r"(b) : "memory");
+}
+__device__ __forceinline__ void bulk_expect(uint64_t* bar, unsigned bytes) {
+  const unsigned b = (unsigned)__cvta_generic_to_shared(bar);
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(b), "r"(bytes) : "memory");
+}
+__device__ __forceinline__ void bulk_copy_g2s(void* smem, const void* gmem, unsigned bytes, uint64_t* bar) {
+  const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+  const unsigned b = (unsigned)__cvta_generic_to_shared(bar);
+  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];\n" ::"r"(s),
+               "l"(gmem), "r"(bytes), "r"(b)
+               : "memory");
+}
+// shared-memory reads by the generic proxy are ordered before later bulk writes
+__device__ __forceinline__ void bulk_fence() { asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory"); }
+// bounded wait for the phase with parity `phase`; false after `polls` polls
+__device__ __forceinline__ bool bulk_wait(uint64_t* bar, unsigned phase, int polls) {
+  const unsigned b = (unsigned)__cvta_generic_to_shared(bar);
+  for (int i = 0; i < polls; ++i) {
+    unsigned done;
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+        : "=r"(done)
+        : "r"(b), "r"(phase)
+        : "memory");
+    if (done) return true;
+  }
+  return false;
+}
+
 // Cast helpers that block FMA contraction, for the float32 reference-order
 // evaluation mode.
 __device__ __forceinline__ float fm(float a, float b) { return __fmul_rn(a, b); }

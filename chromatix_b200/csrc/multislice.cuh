@@ -77,19 +77,23 @@ struct MsRowCfg {
   static constexpr int PF = (MODE == MS_FWD || MODE == MS_BWD || MODE == MS_FLUOR)
                                 ? 2 * NXA + (MODE == MS_BWD ? 2 * NXA : 0) + (MODE == MS_FLUOR ? NXA : 0)
                                 : 0;
-  // cp.async needs 16-byte aligned shared destinations: the prefetch area
+  // bulk copies need 16-byte aligned shared destinations: the prefetch area
   // starts at the next 16-byte boundary after the transform buffers, and PF
-  // (a multiple of 4 floats) keeps every team's area aligned
+  // (a multiple of 4 floats) keeps every team's area aligned; one mbarrier
+  // per team follows
   static constexpr size_t PF_OFF = ((sizeof(float2) * ((size_t)C::TW + (size_t)C::TEAMS * Plan<NX>::LEN)) + 15) & ~(size_t)15;
   static_assert(PF % 4 == 0, "prefetch rows must keep 16-byte alignment");
-  static constexpr size_t SMEM = PF_OFF + sizeof(float) * (size_t)C::TEAMS * PF;
+  static constexpr size_t BAR_OFF = PF_OFF + sizeof(float) * (size_t)C::TEAMS * PF;
+  static constexpr size_t SMEM = BAR_OFF + sizeof(uint64_t) * (size_t)C::TEAMS;
+  static constexpr int POLLS = 1 << 20;
 };
 
 // Start copying dn / abs row yd of the slice (and the recorded field row) into
-// the team's prefetch area; returns false when the rows are not 16-byte
-// aligned (the caller then reads them from global memory)
+// the team's prefetch area: one lane arms the team's mbarrier with the byte
+// count and issues one bulk (TMA) copy per row; returns false when the rows
+// are not 16-byte aligned (the caller then reads them from global memory)
 template <int NX, int MODE>
-__device__ __forceinline__ bool ms_prefetch(const MsArgs& a, float* pf, int yd, int y, int lane, int lpv) {
+__device__ __forceinline__ bool ms_prefetch(const MsArgs& a, float* pf, uint64_t* bar, int yd, int y, int lane) {
   const size_t off = (size_t)a.slice * a.ny * a.nx + (size_t)yd * a.nx;
   const float* dn = a.dn + off;
   // MS_FLUOR: the second and third rows are the fluorescence and the phases
@@ -104,15 +108,18 @@ __device__ __forceinline__ bool ms_prefetch(const MsArgs& a, float* pf, int yd, 
   }
   if (!ok) return false;
   constexpr int NXA = MsRowCfg<NX, MODE>::NXA;
-  for (int i = lane; i < a.nx / 4; i += lpv) {
-    cp_async16(pf + 4 * i, dn + 4 * i);
-    cp_async16(pf + NXA + 4 * i, ab + 4 * i);
-    if constexpr (MODE == MS_FLUOR) cp_async16(pf + 2 * NXA + 4 * i, ph + 4 * i);
+  if (lane == 0) {
+    const unsigned rb = (unsigned)a.nx * 4u;
+    unsigned bytes = 2u * rb;
+    if constexpr (MODE == MS_FLUOR) bytes += rb;
+    if constexpr (MODE == MS_BWD) bytes += (unsigned)a.px * 8u;
+    bulk_fence();  // the previous row's reads of this area precede the new writes
+    bulk_expect(bar, bytes);
+    bulk_copy_g2s(pf, dn, rb, bar);
+    bulk_copy_g2s(pf + NXA, ab, rb, bar);
+    if constexpr (MODE == MS_FLUOR) bulk_copy_g2s(pf + 2 * NXA, ph, rb, bar);
+    if constexpr (MODE == MS_BWD) bulk_copy_g2s(pf + 2 * NXA, u, (unsigned)a.px * 8u, bar);
   }
-  if constexpr (MODE == MS_BWD) {
-    for (int i = lane; i < a.px / 2; i += lpv) cp_async16(pf + 2 * NXA + 4 * i, u + 2 * i);
-  }
-  cp_async_commit();
   return true;
 }
 
@@ -127,6 +134,13 @@ __global__ void __launch_bounds__(RowCfg<NX>::THREADS, RowCfg<NX>::MINB) k_ms_ro
   float2* s = sm + C::TW + team * Plan<NX>::LEN;
   float* pf = reinterpret_cast<float*>(reinterpret_cast<char*>(sm) + MsRowCfg<NX, MODE>::PF_OFF) +
               (size_t)team * MsRowCfg<NX, MODE>::PF;
+  uint64_t* bar = reinterpret_cast<uint64_t*>(reinterpret_cast<char*>(sm) + MsRowCfg<NX, MODE>::BAR_OFF) + team;
+  if constexpr (MODE == MS_FWD || MODE == MS_BWD || MODE == MS_FLUOR) {
+    if (lane == 0) bulk_mbar_init(bar);
+    asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+    __syncthreads();
+  }
+  unsigned bphase = 0;  // parity of this team's next prefetch completion
   // MS_FINAL only produces the cropped rows
   const int r0 = MODE == MS_FINAL ? a.pad_y : 0;
   const int nrows = MODE == MS_FINAL ? a.ny : a.py;
@@ -168,10 +182,15 @@ __global__ void __launch_bounds__(RowCfg<NX>::THREADS, RowCfg<NX>::MINB) k_ms_ro
     }
     if constexpr (MODE == MS_FWD || MODE == MS_BWD || MODE == MS_FLUOR) {
     // the slice's rows stream into shared memory while the inverse transform runs
-    const bool pre = yin && ms_prefetch<NX, MODE>(a, pf, yd, y, lane, C::LPV);
+    bool pre = yin && ms_prefetch<NX, MODE>(a, pf, bar, yd, y, lane);
     auto sst = [&](int k, float2 v, int) { s[pad_idx(k)] = v; };
     team_fft<NX, true>(s, tw, lane, team, load_row, sst);
-    if (pre) cp_async_wait_all();
+    if (pre) {
+      // the rows landed during the inverse transform; past the (generous)
+      // poll limit the lane reads them from global memory instead
+      pre = bulk_wait(bar, bphase, MsRowCfg<NX, MODE>::POLLS);
+      bphase ^= 1u;
+    }
     team_sync<C::LPV>(team);
     if constexpr (MODE == MS_FLUOR) {
       constexpr int NXA = MsRowCfg<NX, MODE>::NXA;
