@@ -128,9 +128,9 @@ extern "C" cx_status cx_prop2d(const cx_prop2d_desc* d, const cx_plane* planes_d
   float2* T = static_cast<float2*>(workspace);
   float2* T2 = reinterpret_cast<float2*>(static_cast<char*>(workspace) + align256(ws_T_bytes(a)));
   cudaStream_t st = static_cast<cudaStream_t>(stream);
-  if ((s = dispatch_rows_fwd(a.px, static_cast<const float2*>(u_in), T, a, st)) != CX_OK) return s;
+  if ((s = prop_rows_fwd(static_cast<const float2*>(u_in), T, a, st)) != CX_OK) return s;
   if ((s = prop_cols(a.py, T, T2, a, st)) != CX_OK) return s;
-  return dispatch_rows_inv(a.px, T2, static_cast<float2*>(u_out), a, st);
+  return prop_rows_inv(T2, static_cast<float2*>(u_out), a, st);
 }
 
 extern "C" cx_status cx_prop2d_ptrs(const cx_prop2d_desc* d, const cx_plane* planes_dev,
@@ -160,9 +160,9 @@ extern "C" cx_status cx_prop2d_ptrs(const cx_prop2d_desc* d, const cx_plane* pla
   float2* T = static_cast<float2*>(workspace);
   float2* T2 = reinterpret_cast<float2*>(static_cast<char*>(workspace) + align256(ws_T_bytes(a)));
   cudaStream_t st = static_cast<cudaStream_t>(stream);
-  if ((s = dispatch_rows_fwd(a.px, nullptr, T, a, st)) != CX_OK) return s;
+  if ((s = prop_rows_fwd(nullptr, T, a, st)) != CX_OK) return s;
   if ((s = prop_cols(a.py, T, T2, a, st)) != CX_OK) return s;
-  return dispatch_rows_inv(a.px, T2, nullptr, a, st);
+  return prop_rows_inv(T2, nullptr, a, st);
 }
 
 extern "C" cx_status cx_fill_propagator(const cx_prop2d_desc* d, const cx_plane* planes_dev, void* H_out,

@@ -305,4 +305,16 @@ cx_status dispatch_cols_tc(int n, const float2* T, float2* T2, const Prop2DArgs&
 inline cx_status prop_cols(int n, const float2* T, float2* T2, const Prop2DArgs& a, cudaStream_t st) {
   return a.precision == CX_PREC_SPLIT16 ? dispatch_cols_tc(n, T, T2, a, st) : dispatch_cols(n, T, T2, a, st);
 }
+// CX_PREC_SPLIT16 row passes on the tensor cores where the padded row length
+// is compiled in (1024, 1280); other lengths keep the FP32 butterflies
+bool prop_tc_rows_supported(int px);
+cx_status dispatch_rows_tc(bool inverse, const float2* in, float2* out, const Prop2DArgs& a, cudaStream_t st);
+inline cx_status prop_rows_fwd(const float2* u, float2* T, const Prop2DArgs& a, cudaStream_t st) {
+  return a.precision == CX_PREC_SPLIT16 && prop_tc_rows_supported(a.px) ? dispatch_rows_tc(false, u, T, a, st)
+                                                                         : dispatch_rows_fwd(a.px, u, T, a, st);
+}
+inline cx_status prop_rows_inv(const float2* T2, float2* out, const Prop2DArgs& a, cudaStream_t st) {
+  return a.precision == CX_PREC_SPLIT16 && prop_tc_rows_supported(a.px) ? dispatch_rows_tc(true, T2, out, a, st)
+                                                                         : dispatch_rows_inv(a.px, T2, out, a, st);
+}
 }  // namespace cx

@@ -354,7 +354,7 @@ extern "C" cx_status cx_psf_4f(const cx_psf_desc* d, const cx_psf_spectrum* spec
   for (int z0 = 0; z0 < a.nz; z0 += zc) {
     a.z0 = z0;
     a.zc = (a.nz - z0) < zc ? (a.nz - z0) : zc;
-    if ((s = psf_dispatch_rows(a.nx, a, st)) != CX_OK) return s;
+    if ((s = psf_rows_pass(a, st)) != CX_OK) return s;
     if ((s = psf_cols(a, st)) != CX_OK) return s;
   }
   return CX_OK;
@@ -396,7 +396,7 @@ extern "C" cx_status cx_psf_4f_stage(const cx_psf_desc* d, const cx_psf_spectrum
     return CX_ERR_INVALID;
   }
   a.zc = (a.nz - a.z0) < zc ? (a.nz - a.z0) : zc;
-  return stage == 0 ? psf_dispatch_rows(a.nx, a, st) : psf_cols(a, st);
+  return stage == 0 ? psf_rows_pass(a, st) : psf_cols(a, st);
 }
 
 // ---------------------------------------------------------------------------

@@ -322,4 +322,12 @@ cx_status psf_dispatch_cols_tc(int n, const PsfArgs& a, cudaStream_t st);
 inline cx_status psf_cols(const PsfArgs& a, cudaStream_t st) {
   return a.precision == CX_PREC_SPLIT16 ? psf_dispatch_cols_tc(a.ny, a, st) : psf_dispatch_cols(a.ny, a, st);
 }
+// CX_PREC_SPLIT16 row pass on the tensor cores where the row length is
+// compiled in (1024, 1280); other lengths keep the FP32 butterflies
+bool psf_tc_rows_supported(int nx);
+cx_status psf_dispatch_rows_tc(int n, const PsfArgs& a, cudaStream_t st);
+inline cx_status psf_rows_pass(const PsfArgs& a, cudaStream_t st) {
+  return a.precision == CX_PREC_SPLIT16 && psf_tc_rows_supported(a.nx) ? psf_dispatch_rows_tc(a.nx, a, st)
+                                                                        : psf_dispatch_rows(a.nx, a, st);
+}
 }  // namespace cx

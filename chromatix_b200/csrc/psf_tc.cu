@@ -126,6 +126,147 @@ static cx_status launch_psf_cols_tc(const PsfArgs& a, cudaStream_t st) {
   return CX_OK;
 }
 
+// Row pass with the row FFTs on the tensor cores: eight row spectra per tile
+// (consecutive items (z, compact row) as in k_psf_rows_tab), the table source
+// M * CX * row factor evaluated in the loader (ifftshift along x), the
+// four-step row transform of tc_fft_rows_tile, the row spectrum stored for
+// live rows only (rows outside the pupil transform zeros and store nothing).
+struct PsfTcRow {
+  const float2* mrow;
+  const float2* cxz;
+  float2* dst;
+  float2 cy;
+  int xlo, nc, live, pad;
+};
+
+template <int N1, int N2>
+struct PsfTcRowCfg {
+  using F = TcFft<N1, N2>;
+  static constexpr int N = F::N;
+  static constexpr size_t TW_BYTES = sizeof(float2) * N;
+  static constexpr size_t SMEM = F::SMEM + TW_BYTES + 64 + 256 + 8 * sizeof(PsfTcRow);
+};
+
+template <int N1, int N2>
+__global__ void __launch_bounds__(256, 1) k_psf_rows_tc(PsfArgs a, const float2* __restrict__ twN) {
+  using F = TcFft<N1, N2>;
+  using C = PsfTcRowCfg<N1, N2>;
+  constexpr int N = F::N;
+  extern __shared__ __align__(128) uint8_t smem[];
+  TcFftSmem S;
+  S.A = smem;
+  S.B1 = smem + F::A_BYTES;
+  S.B2 = S.B1 + F::B1_BYTES;
+  float2* tw = reinterpret_cast<float2*>(S.B2 + F::B2_BYTES);
+  S.bar = reinterpret_cast<uint64_t*>(reinterpret_cast<uint8_t*>(tw) + C::TW_BYTES);
+  uint32_t* tslot = reinterpret_cast<uint32_t*>(S.bar + 1);
+  S.red = reinterpret_cast<float*>(S.bar + 8);
+  PsfTcRow* rp = reinterpret_cast<PsfTcRow*>(S.red + 64);
+  const int tid = threadIdx.x;
+
+  tc_fft_build_b<N1>(S.B1, false, tid, blockDim.x);
+  tc_fft_build_b<N2>(S.B2, false, tid, blockDim.x);
+  for (int i = tid; i < N; i += blockDim.x) tw[i] = twN[i];
+  if ((tid >> 5) == 0) {
+    tc::tmem_alloc(tslot, F::TMEM_COLS);
+    tc::tmem_relinquish();
+  }
+  if (tid == 0) {
+    tc::mbar_init(S.bar, 1);
+    tc::mbar_init_fence();
+  }
+  tc::fence_smem_to_async();
+  tc::fence_before_sync();
+  __syncthreads();
+  tc::fence_after_sync();
+  const uint32_t tmem = *tslot;
+  uint32_t phase = 0;
+
+  const long total = (long)a.zc * a.rowsum;
+  const long tiles = (total + 7) / 8;
+  const double PI = 3.141592653589793238462643383279502884;
+  for (long t = blockIdx.x; t < tiles; t += gridDim.x) {
+    if (tid < 8) {
+      const long item0 = t * 8 + tid;
+      const long item = item0 < total ? item0 : total - 1;
+      const int zl = (int)(item / a.rowsum);
+      const int rem = (int)(item % a.rowsum);
+      int w = 0;
+      while (w + 1 < a.W && rem >= a.prefix[w + 1]) ++w;
+      const PsfWv& p = a.wv[w];
+      const int y = a.ylo[w] + (rem - a.prefix[w]);
+      const bool live = item0 < total && y >= support_lo(a, w) && y < support_hi(a, w);
+      const double z = a.z[a.z0 + zl];
+      const double gyo = p.dy * ((double)y - (double)a.ny * 0.5) - a.offy;
+      const double qz = -PI * (z / a.f_obj) / p.L2;
+      PsfTcRow r;
+      r.mrow = a.M + a.mprefix[w] + (size_t)(y - a.ylo[w]) * a.ncols[w];
+      r.cxz = a.CX + (size_t)(a.z0 + zl) * a.csum + a.cprefix[w];
+      r.dst = a.T + ((size_t)zl * a.rowsum + rem) * a.nx;
+      r.cy = expi_precise(qz * gyo * gyo);
+      r.xlo = a.xlo[w];
+      r.nc = live ? a.ncols[w] : 0;
+      r.live = live ? 1 : 0;
+      r.pad = 0;
+      rp[tid] = r;
+    }
+    __syncthreads();
+    auto load8 = [&](int v, int n, float2* o) {
+      const PsfTcRow& r = rp[v];
+      // ifftshift along x: eight consecutive FFT inputs are eight consecutive
+      // field columns (N / 2 and n are multiples of 8), then the box column
+      const int c0 = add_mod(n, N / 2, N) - r.xlo;
+#pragma unroll
+      for (int q = 0; q < 8; ++q) {
+        const int c = c0 + q;
+        o[q] = (unsigned)c < (unsigned)r.nc ? cmul(cmul(r.mrow[c], r.cxz[c]), r.cy) : make_float2(0.f, 0.f);
+      }
+    };
+    auto store = [&](int v, int k, float2 X) {
+      if (rp[v].live) rp[v].dst[k] = X;
+    };
+    if (!tc_fft_rows_tile<F>(S, tmem, phase, tw, load8, store)) {
+      // an MMA wait ran out: mark this CTA's remaining row spectra invalid
+      // (NaN; the column pass carries them into the intensity) and let the
+      // MMAs in flight finish (bounded) before tensor memory is freed
+      tc::mbar_wait(S.bar, phase ^ 1u, F::POLLS);
+      const float nan = __int_as_float(0x7fc00000);
+      for (long u = t; u < tiles; u += gridDim.x)
+        for (int idx = tid; idx < 8 * N; idx += blockDim.x) {
+          const long item = u * 8 + idx / N;
+          if (item < total) a.T[item * a.nx + idx % N] = make_float2(nan, nan);
+        }
+      break;
+    }
+  }
+  tc::fence_before_sync();
+  __syncthreads();
+  if ((tid >> 5) == 0) tc::tmem_dealloc(tmem, F::TMEM_COLS);
+}
+
+template <int N1, int N2>
+static cx_status launch_psf_rows_tc(const PsfArgs& a, cudaStream_t st) {
+  using C = PsfTcRowCfg<N1, N2>;
+  auto k = k_psf_rows_tc<N1, N2>;
+  CX_CUDA_TRY(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)C::SMEM));
+  const long tiles = ((long)a.zc * a.rowsum + 7) / 8;
+  int grid = sm_count();
+  if (tiles < grid) grid = (int)tiles;
+  k<<<grid, 256, C::SMEM, st>>>(a, a.twg + tw_offset(C::N));
+  CX_LAUNCH_CHECK();
+  return CX_OK;
+}
+
+bool psf_tc_rows_supported(int nx) { return nx == 1280 || nx == 1024; }
+
+cx_status psf_dispatch_rows_tc(int n, const PsfArgs& a, cudaStream_t st) {
+  if (!psf_tc_rows_supported(n)) {
+    set_error("split-precision PSF row pass: %d columns not compiled in (1024 or 1280)", n);
+    return CX_ERR_UNSUPPORTED;
+  }
+  return n == 1280 ? launch_psf_rows_tc<40, 32>(a, st) : launch_psf_rows_tc<32, 32>(a, st);
+}
+
 bool psf_tc_supported(int ny, int nx) { return (ny == 1280 || ny == 1024) && nx % 8 == 0 && nx >= 8; }
 
 cx_status psf_dispatch_cols_tc(int n, const PsfArgs& a, cudaStream_t st) {

@@ -513,4 +513,146 @@ __device__ bool tc_fft_mult_tile(const TcFftSmem& S, uint32_t tmem, uint32_t& ph
   return true;
 }
 
+// Row FFTs of length N = L1 L2 (L1 = F::N1, L2 = F::N2) on eight rows: the
+// same two GEMM stages, tile shapes, DFT matrices and shared-memory layout as
+// the column form with the index maps exchanged, because a row's contiguous
+// index must form the MN-major 16-byte chunks:
+//   n = na + L2 nb (na < L2 contiguous, nb < L1),  k = L1 ka + kb,
+//   X[L1 ka + kb] = sum_na W_L2^(na ka) W_N^(na kb) sum_nb W_L1^(nb kb) x[na + L2 nb].
+// Stage 1 rows (v, na), a DFT of length L1 over nb; stage 2 rows (v, kb), a
+// DFT of length L2 over na.  load8(v, n, out[8]): elements n .. n+7 of input
+// row v (n a multiple of 8); store(v, k, X): output bin k of row v, staged
+// through shared memory so rows leave contiguous.
+// Each row is scaled by its own power of two.
+template <class F, class Load8, class Store>
+__device__ bool tc_fft_rows_tile(const TcFftSmem& S, uint32_t tmem, uint32_t& phase, const float2* __restrict__ tw,
+                                 Load8 load8, Store store) {
+  constexpr int L1 = F::N1, L2 = F::N2, N = F::N, K1 = F::K1, K2 = F::K2;
+  constexpr int CPR = N / 8;  // 8-element chunks per row
+  static_assert(L2 % 8 == 0, "a chunk of 8 shares nb");
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const uint32_t wl = (uint32_t)((warp & 3) * 32) << 16;
+
+  // ---- load: chunk c = tid + 256 i is row c / CPR, elements 8 (c % CPR) ..
+  float2 xv[F::RPT][8];
+  float mx[8];
+#pragma unroll
+  for (int v = 0; v < 8; ++v) mx[v] = 0.f;
+#pragma unroll
+  for (int i = 0; i < F::RPT; ++i) {
+    const int c = tid + i * F::THREADS;
+    const int v = c / CPR, n0 = (c - v * CPR) * 8;
+    load8(v, n0, xv[i]);
+    float m = 0.f;
+#pragma unroll
+    for (int q = 0; q < 8; ++q) m = fmaxf(m, fmaxf(fabsf(xv[i][q].x), fabsf(xv[i][q].y)));
+#pragma unroll
+    for (int r = 0; r < 8; ++r) mx[r] = (r == v) ? fmaxf(mx[r], m) : mx[r];
+  }
+#pragma unroll
+  for (int v = 0; v < 8; ++v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) mx[v] = fmaxf(mx[v], __shfl_xor_sync(0xffffffffu, mx[v], o));
+  }
+  if (lane == 0) {
+#pragma unroll
+    for (int v = 0; v < 8; ++v) S.red[warp * 8 + v] = mx[v];
+  }
+  __syncthreads();
+  float sc[8];
+#pragma unroll
+  for (int v = 0; v < 8; ++v) {
+    float m = S.red[v];
+#pragma unroll
+    for (int w = 1; w < 8; ++w) m = fmaxf(m, S.red[w * 8 + v]);
+    int e = 0;
+    if (m > 0.f) frexpf(m, &e);
+    sc[v] = ldexpf(1.f, 9 - e);
+  }
+
+  // ---- stage-1 A (MN-major): row m = L2 v + na, column (re | im) of nb
+  uint8_t* Ahi = S.A;
+#pragma unroll
+  for (int i = 0; i < F::RPT; ++i) {
+    const int c = tid + i * F::THREADS;
+    const int v = c / CPR, n0 = (c - v * CPR) * 8;
+    const int na0 = n0 % L2, nb = n0 / L2;  // the chunk's 8 elements share nb (L2 % 8 == 0)
+    float s = sc[0];
+#pragma unroll
+    for (int r = 1; r < 8; ++r) s = (r == v) ? sc[r] : s;
+    float re[8], im[8];
+#pragma unroll
+    for (int q = 0; q < 8; ++q) {
+      re[q] = xv[i][q].x * s;
+      im[q] = xv[i][q].y * s;
+    }
+    const int m0 = v * L2 + na0;
+    const uint32_t tile = (uint32_t)(m0 >> 7) * F::A1_TILE;
+    tc_store_chunk(Ahi + tile, Ahi + F::T1 * F::A1_TILE + tile, tc::off_mnmajor(128, m0 & 127, nb), re);
+    tc_store_chunk(Ahi + tile, Ahi + F::T1 * F::A1_TILE + tile, tc::off_mnmajor(128, m0 & 127, L1 + nb), im);
+  }
+  if (!tc_gemm<K1, F::T1>(S, tmem, phase, S.A, F::A1_TILE, 1, S.B1, F::POLLS)) return false;
+
+  // ---- stage-1 result: thread = row (v, na); twiddle W_N^(na kb); stage-2 A
+  // (MN-major): row (v, kb) = L1 v + kb, column (re | im) of na
+  {
+    const int t = warp >> 2;
+    const int m = t * 128 + (warp & 3) * 32 + lane;
+    const int v = m / L2, na = m - v * L2;
+    float d[K1];
+#pragma unroll
+    for (int c = 0; c < K1; c += 16) tc::tmem_ld16(tmem + wl + t * K1 + c, d + c);
+    tc::tmem_wait_ld();
+#pragma unroll
+    for (int c = 0; c < L1 / 8; ++c) {
+      float re[8], im[8];
+#pragma unroll
+      for (int q = 0; q < 8; ++q) {
+        const int kb = 8 * c + q;
+        const float2 w = tw[na * kb];  // na kb < N
+        re[q] = d[kb] * w.x - d[L1 + kb] * w.y;
+        im[q] = d[kb] * w.y + d[L1 + kb] * w.x;
+      }
+      const int m2 = v * L1 + 8 * c;
+      const uint32_t tile = (uint32_t)(m2 >> 7) * F::A2_TILE;
+      tc_store_chunk(Ahi + tile, Ahi + F::T2 * F::A2_TILE + tile, tc::off_mnmajor(128, m2 & 127, na), re);
+      tc_store_chunk(Ahi + tile, Ahi + F::T2 * F::A2_TILE + tile, tc::off_mnmajor(128, m2 & 127, L2 + na), im);
+    }
+  }
+  if (!tc_gemm<K2, F::T2>(S, tmem, phase, S.A, F::A2_TILE, 1, S.B2, F::POLLS)) return false;
+
+  // ---- stage-2 result: row (v, kb) holds X[L1 ka + kb], ka < L2; stage the
+  // rows column-major by bin (lanes hold consecutive kb: conflict-free)
+  float2* stage = reinterpret_cast<float2*>(S.A);
+#pragma unroll
+  for (int j0 = 0; j0 < F::T2; j0 += 2) {
+    const int j = j0 + (warp >> 2);
+    if (j < F::T2) {
+      float d[K2];
+#pragma unroll
+      for (int c = 0; c < K2; c += 16) tc::tmem_ld16(tmem + wl + j * K2 + c, d + c);
+      tc::tmem_wait_ld();
+      const int m2 = j * 128 + (warp & 3) * 32 + lane;
+      if (m2 < F::M2) {
+        const int v = m2 / L1, kb = m2 - v * L1;
+        float mv = S.red[v];
+#pragma unroll
+        for (int w = 1; w < 8; ++w) mv = fmaxf(mv, S.red[w * 8 + v]);
+        int e = 0;
+        if (mv > 0.f) frexpf(mv, &e);
+        const float isc = ldexpf(1.f, e - 9);
+        // the staged rows overwrite stage 2's operand, which the completed GEMM no longer reads
+#pragma unroll
+        for (int ka = 0; ka < L2; ++ka) stage[v * N + L1 * ka + kb] = make_float2(d[ka] * isc, d[L2 + ka] * isc);
+      }
+    }
+  }
+  tc::fence_before_sync();
+  __syncthreads();
+  // lanes take consecutive bins: conflict-free reads, contiguous row stores
+  for (int e = tid; e < 8 * N; e += F::THREADS) store(e / N, e % N, stage[e]);
+  __syncthreads();
+  return true;
+}
+
 }  // namespace cx

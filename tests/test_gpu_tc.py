@@ -63,8 +63,8 @@ def test_split16_rejects_unsupported_length():
 
 @pytest.mark.parametrize("N", [1280, 1024])
 def test_split16_psf_matches_fp64_oracle(N):
-    """The 4f PSF with its column transforms on the tensor cores (precision
-    "split16") against the FP64 oracle, at the headline configuration's optics
+    """The 4f PSF with its row and column transforms on the tensor cores
+    (precision "split16") against the FP64 oracle, at the headline configuration's optics
     (f_obj 8 mm, f_tube 200 mm, NA 0.6, n 1.33, 3 wavelengths, 6.5 um camera
     pitch) on 3 defocus planes: relative L2 <= 1e-5, and within 3x of the
     plain FP32 path's own error."""
