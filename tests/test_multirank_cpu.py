@@ -49,3 +49,26 @@ def test_max_over_ranks_single_process():
     import bench
 
     assert bench.max_over_ranks([3.0, 4.0]) == [3.0, 4.0]
+
+
+def test_gpus_flag_launches_one_rank_per_gpu(monkeypatch):
+    """``bench.py --gpus N`` outside a launcher starts N ranks through
+    torch.distributed.run on 127.0.0.1 with the same arguments, and exits
+    with the launcher's status."""
+    import sys
+
+    import bench
+
+    calls = []
+    monkeypatch.setattr(bench.subprocess, "call", lambda cmd: calls.append(cmd) or 7)
+    monkeypatch.delenv("WORLD_SIZE", raising=False)
+    monkeypatch.setattr(sys, "argv", ["bench.py", "--gpus", "4", "--steps", "3", "--warmup", "3"])
+    with pytest.raises(SystemExit) as ex:
+        bench.main()
+    assert ex.value.code == 7
+    (cmd,) = calls
+    assert cmd[1:3] == ["-m", "torch.distributed.run"]
+    assert "--nproc-per-node=4" in cmd and "--nnodes=1" in cmd
+    assert cmd[cmd.index("--master-addr") + 1] == "127.0.0.1"
+    assert cmd[-6:] == ["--gpus", "4", "--steps", "3", "--warmup", "3"]
+    assert cmd[-7].endswith("bench.py")
