@@ -241,14 +241,14 @@ extern "C" cx_status cx_multislice_forward(const cx_ms_desc* d, const void* u_in
   a.ox = d->pad;
   a.record = ck ? 1 : 0;
   a.rec = ck;
-  if ((s = ms_dispatch_rows(p.px, a, st)) != CX_OK) return s;
+  if ((s = ms_rows(a, st)) != CX_OK) return s;
   if ((s = col_pass(p, planes + 0, F, -1.0, true, st, Htab)) != CX_OK) return s;
   a.mode = MS_FWD;
   for (int i = 1; i <= p.D; ++i) {
     a.slice = i - 1;  // u_i = t_{i-1} P(u_{i-1})
     a.record = (ck && i < p.D && i % p.K == 0) ? 1 : 0;
     a.rec = a.record ? ck + (size_t)(i / p.K) * field : nullptr;
-    if ((s = ms_dispatch_rows(p.px, a, st)) != CX_OK) return s;
+    if ((s = ms_rows(a, st)) != CX_OK) return s;
     if (i < p.D && (s = col_pass(p, planes + 0, F, -1.0, true, st, Htab)) != CX_OK) return s;
   }
   // defocus back to the chosen plane, NA mask, crop (samples.py:265-282)
@@ -256,7 +256,7 @@ extern "C" cx_status cx_multislice_forward(const cx_ms_desc* d, const void* u_in
   a.mode = MS_FINAL;
   a.record = 0;
   a.dst = static_cast<float2*>(u_out);
-  return ms_dispatch_rows(p.px, a, st);
+  return ms_rows(a, st);
 }
 
 extern "C" cx_status cx_multislice_backward(const cx_ms_desc* d, const float* dn, const float* ab,
@@ -303,7 +303,7 @@ extern "C" cx_status cx_multislice_backward(const cx_ms_desc* d, const float* dn
   g.oy = d->pad;
   g.ox = d->pad;
   g.record = 0;
-  if ((s = ms_dispatch_rows(p.px, g, st)) != CX_OK) return s;
+  if ((s = ms_rows(g, st)) != CX_OK) return s;
   if ((s = col_pass(p, planes + 3, G, na_mask(d), false, st)) != CX_OK) return s;
 
   MsArgs f = ms_args(d, p);
@@ -320,14 +320,14 @@ extern "C" cx_status cx_multislice_backward(const cx_ms_desc* d, const float* dn
     f.oy = 0;
     f.ox = 0;
     f.record = 0;
-    if ((s = ms_dispatch_rows(p.px, f, st)) != CX_OK) return s;
+    if ((s = ms_rows(f, st)) != CX_OK) return s;
     if ((s = col_pass(p, planes + 0, F, -1.0, true, st, Htab)) != CX_OK) return s;
     f.mode = MS_FWD;
     for (int i = i0 + 1; i <= i1; ++i) {
       f.slice = i - 1;
       f.record = 1;
       f.rec = seg + (size_t)(i - i0 - 1) * seg_stride;
-      if ((s = ms_dispatch_rows(p.px, f, st)) != CX_OK) return s;
+      if ((s = ms_rows(f, st)) != CX_OK) return s;
       if (i < i1 && (s = col_pass(p, planes + 0, F, -1.0, true, st, Htab)) != CX_OK) return s;
     }
     // adjoint through slices i1-1 .. i0
@@ -337,14 +337,14 @@ extern "C" cx_status cx_multislice_backward(const cx_ms_desc* d, const float* dn
       g.rec_u = seg + (size_t)(i - i0) * seg_stride;
       g.gdn = grad_dn + (size_t)i * d->ny * d->nx;
       g.gab = grad_ab + (size_t)i * d->ny * d->nx;
-      if ((s = ms_dispatch_rows(p.px, g, st)) != CX_OK) return s;
+      if ((s = ms_rows(g, st)) != CX_OK) return s;
       if ((s = col_pass(p, planes + 1, G, -1.0, true, st, Htab, true)) != CX_OK) return s;
     }
   }
   if (grad_u_in) {
     g.mode = MS_FINAL;
     g.dst = static_cast<float2*>(grad_u_in);
-    return ms_dispatch_rows(p.px, g, st);
+    return ms_rows(g, st);
   }
   return CX_OK;
 }

@@ -256,5 +256,14 @@ __global__ void __launch_bounds__(RowCfg<NX>::THREADS, RowCfg<NX>::MINB) k_ms_ro
 }
 
 cx_status ms_dispatch_rows(int n, const MsArgs& a, cudaStream_t st);
+// CX_PREC_SPLIT16 row passes on the tensor cores (multislice_tc.cu) where the
+// padded row length is compiled in; other lengths and the fluorescent step
+// keep the FP32 butterflies
+bool ms_tc_rows_supported(int px, int mode);
+cx_status ms_dispatch_rows_tc(const MsArgs& a, cudaStream_t st);
+inline cx_status ms_rows(const MsArgs& a, cudaStream_t st) {
+  return a.precision == CX_PREC_SPLIT16 && ms_tc_rows_supported(a.px, a.mode) ? ms_dispatch_rows_tc(a, st)
+                                                                              : ms_dispatch_rows(a.px, a, st);
+}
 
 }  // namespace cx

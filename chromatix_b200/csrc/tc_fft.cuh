@@ -523,8 +523,11 @@ __device__ bool tc_fft_mult_tile(const TcFftSmem& S, uint32_t tmem, uint32_t& ph
 // DFT of length L2 over na.  load8(v, n, out[8]): elements n .. n+7 of input
 // row v (n a multiple of 8); store(v, k, X): output bin k of row v, staged
 // through shared memory so rows leave contiguous.
-// Each row is scaled by its own power of two.
-template <class F, class Load8, class Store>
+// Each row is scaled by its own power of two.  STORE = false leaves the
+// output in shared memory (tc_rows_staged: row v, bin k at [v N + k]) for the
+// next call's loader, which reads all of it into registers before its first
+// operand write; store is then not called.
+template <class F, bool STORE = true, class Load8, class Store>
 __device__ bool tc_fft_rows_tile(const TcFftSmem& S, uint32_t tmem, uint32_t& phase, const float2* __restrict__ tw,
                                  Load8 load8, Store store) {
   constexpr int L1 = F::N1, L2 = F::N2, N = F::N, K1 = F::K1, K2 = F::K2;
@@ -649,10 +652,17 @@ __device__ bool tc_fft_rows_tile(const TcFftSmem& S, uint32_t tmem, uint32_t& ph
   }
   tc::fence_before_sync();
   __syncthreads();
-  // lanes take consecutive bins: conflict-free reads, contiguous row stores
-  for (int e = tid; e < 8 * N; e += F::THREADS) store(e / N, e % N, stage[e]);
-  __syncthreads();
+  if constexpr (STORE) {
+    // lanes take consecutive bins: conflict-free reads, contiguous row stores
+    for (int e = tid; e < 8 * N; e += F::THREADS) store(e / N, e % N, stage[e]);
+    __syncthreads();
+  }
   return true;
+}
+
+// the rows a tc_fft_rows_tile<F, false> call left in shared memory
+__device__ __forceinline__ const float2* tc_rows_staged(const TcFftSmem& S) {
+  return reinterpret_cast<const float2*>(S.A);
 }
 
 }  // namespace cx
