@@ -308,7 +308,8 @@ def gpu_arm(args):
         if rank == 0:
             line["latency_ms"] = serve["latency_ms"]
             line["serve"] = {k: serve[k] for k in ("value", "unit", "requests", "achieved_req_s", "seconds",
-                                                   "rate_req_s", "offered_device_load")}
+                                                   "rate_req_s", "offered_device_load", "graph_replays",
+                                                   "graph_captures_during_stream")}
     if rank == 0:
         print(json.dumps(line), flush=True)
     if dist:
@@ -859,11 +860,13 @@ def run_serve_stream(dev, rank, world, dist, rate, seconds, accuracy=False):
                        z=float(rng.uniform(1, 500)), wavelength=float(rng.uniform(0.4, 0.7)), n=1.33,
                        zoom=float(rng.uniform(0.25, 4)), out_shape=(512, 512), t_arrival=t)
 
-    # warm-up: every (op, N) once
+    # warm-up: every (op, N) once, then the launch graphs of every batch size
+    # on every stream (captured before the stream, as a server does at start)
     for op in SERVE_OPS:
         for N in SERVE_SIDES:
             srv.submit(Request(op=op, u=fields[N][0], dx=0.3, z=100.0, wavelength=0.5, zoom=2.0))
     srv.drain()
+    srv.warmup(ops=tuple(op for op in SERVE_OPS if op != "czt_zoom"), sides=SERVE_SIDES, n=1.33)
     torch.cuda.synchronize(dev)
     # device time of each (op, N) request run alone (3 repeats): the offered
     # device load of the stream is rate * the mean over the uniform mix
@@ -878,6 +881,7 @@ def run_serve_stream(dev, rank, world, dist, rate, seconds, accuracy=False):
     offered_load = rate * float(np.mean(list(service.values()))) / 1e3
     for c in (srv.host_s, srv.gpu_ms, srv.batches):
         c.clear()
+    cap0, rep0 = srv.graph_captures, srv.graph_replays
     if dist:
         dist.barrier()
     n_req = max(1, int(rate * seconds))
@@ -920,7 +924,8 @@ def run_serve_stream(dev, rank, world, dist, rate, seconds, accuracy=False):
            "service_ms_alone": service, "offered_device_load": round(offered_load, 3),
            "launch_host_ms_by_op": {k: round(v * 1e3, 1) for k, v in srv.host_s.items()},
            "device_ms_by_op": {k: round(v, 1) for k, v in srv.gpu_ms.items()},
-           "batches_by_op": dict(srv.batches), "clocks": clk.summary()}
+           "batches_by_op": dict(srv.batches), "graph_replays": srv.graph_replays - rep0,
+           "graph_captures_during_stream": srv.graph_captures - cap0, "clocks": clk.summary()}
     if accuracy and rank == 0:
         out["rel_err_vs_fp64"] = serve_accuracy(keep)
     return out

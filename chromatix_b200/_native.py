@@ -22,6 +22,11 @@ c_void_p = ctypes.c_void_p
 c_size_t = ctypes.c_size_t
 
 CX_OK = 0
+CX_ERR_INVALID = 1
+CX_ERR_UNSUPPORTED = 2
+CX_ERR_CUDA = 3
+CX_ERR_WORKSPACE = 4
+CX_ERR_NOT_CONVERGED = 5
 CX_PREC_ACCURATE = 0
 CX_PREC_REF32 = 1
 CX_KERNEL_TRANSFER = 0

@@ -506,12 +506,14 @@ def _pad_fn():
             def forward(ctx, u, dims, cval):
                 batch, ny, nx, C, py, px = dims
                 ctx.dims = dims
+                ctx.in_shape = tuple(u.shape)
                 return _pad_native(u, batch, ny, nx, C, py, px, cval)
 
             @staticmethod
             def backward(ctx, g):
                 batch, ny, nx, C, py, px = ctx.dims
-                return g[:, py:py + ny, px:px + nx, :].contiguous(), None, None
+                g = g.reshape(batch, ny + 2 * py, nx + 2 * px, C)
+                return g[:, py:py + ny, px:px + nx, :].reshape(ctx.in_shape), None, None
 
         _PAD_FN = _Pad
     return _PAD_FN
