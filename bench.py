@@ -205,7 +205,9 @@ def gpu_arm(args):
     # ("split16": column transforms as FP16 hi + lo DFT contractions) on the
     # same workload; the line reports the faster form that meets the 1e-5
     # bar against the FP64 oracle (errors checked outside the timed region)
-    forms = ["accurate"] if args.no_split16 else ["accurate", "split16"]
+    forms = ["accurate"] if args.no_split16 else [f for f in ("accurate", "split16") if f in args.forms.split(",")]
+    if not forms:
+        raise SystemExit("--forms: name at least one of accurate, split16")
     ms_form, clk_form = {}, {}
     for p in forms:
         mode["p"] = p
@@ -218,7 +220,7 @@ def gpu_arm(args):
             acc_form[p] = accuracy_check(dev, p)
     ms_form = dict(zip(forms, max_over_ranks([ms_form[p] for p in forms], dist, dev)))
     ok = [p for p in forms if acc_form.get(p, {}).get("rel_err_vs_fp64", 0.0) <= 1e-5]
-    best = min(ok or ["accurate"], key=lambda p: ms_form[p])
+    best = min(ok or forms[:1], key=lambda p: ms_form[p])
     if dist:
         # every rank times the same form (rank 0's accuracy decides)
         import torch.distributed as _d
@@ -272,8 +274,8 @@ def gpu_arm(args):
             "warmup": args.warmup, "ms_per_step": round(ms, 4), "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None,
             "dtype": ("c64/f32 (FP64 phase arguments)" if best == "accurate" else
-                      "c64/f32 (FP64 phase arguments; column transforms as FP16 hi+lo tensor-core DFT contractions, "
-                      "FP32 accumulation)"),
+                      "c64/f32 (FP64 phase arguments; row and column transforms as FP16 hi+lo tensor-core DFT "
+                      "contractions, FP32 accumulation)"),
             "data": "synthetic (seeded)",
             "config": dict(CONFIG, l2="flushed between timed steps (256 MB write)",
                            parallelism=f"replicas x{world}" if world > 1 else "single GPU"),
@@ -288,7 +290,8 @@ def gpu_arm(args):
             "transform_form": best,
             "forms": {p: {"ms_per_step": round(ms_form[p], 4),
                           "value": round(PX_PER_STEP * world / (ms_form[p] * 1e-3) / 1e6, 1),
-                          "speedup_vs_fp32": round(ms_form["accurate"] / ms_form[p], 3),
+                          "speedup_vs_fp32": (round(ms_form["accurate"] / ms_form[p], 3) if "accurate" in ms_form
+                                              else None),
                           "rel_err_vs_fp64": acc_form.get(p, {}).get("rel_err_vs_fp64"),
                           "clocks": clk_form[p].summary()} for p in forms},
             "compute": {"fp32_fft_gflop_per_step": round(flops / 1e9, 2),
@@ -1076,6 +1079,8 @@ def main():
                     help="skip the error against the FP64 oracle (computed outside the timed region)")
     ap.add_argument("--no-serve", action="store_true", help="psf: skip the short serving stream (latency_ms)")
     ap.add_argument("--no-split16", action="store_true", help="psf: time the plain FP32 transform form only")
+    ap.add_argument("--forms", default="accurate,split16",
+                    help="psf: transform forms to time (comma list of accurate, split16)")
     ap.add_argument("--headline-serve-seconds", type=float, default=1.0,
                     help="psf: length of the serving stream whose latency the headline line reports")
     ap.add_argument("--workload", default="psf",

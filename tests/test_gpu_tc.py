@@ -110,8 +110,11 @@ def test_split16_propagation_512_pad_256_matches_fp64(method, mode):
     from oracle import chromatix_oracle as O
     from tests.helpers import oracle_field, rand_field, rel
 
+    from chromatix_b200.core.field import ScalarField
+    from chromatix_b200.core.spectrum import Spectrum
+
     u = np.stack([rand_field((512, 512), seed=s) for s in (1, 2, 3)])
-    f = cx.Field.build(torch.as_tensor(u, device="cuda"), 0.3, 0.532)
+    f = ScalarField(torch.as_tensor(u, device="cuda"), 0.3, 0.0, Spectrum.build(0.532))
     kw = dict(mode=mode)
     with cx.precision("split16"):
         if method == "transfer":
