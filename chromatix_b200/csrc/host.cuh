@@ -98,6 +98,13 @@ constexpr int kTwTotal = tw_total();
 // their device address; kernels receive it in their argument structs.
 cx_status ensure_twiddles(const float2** table);
 
+// The real-expanded forward DFT matrices of the split-precision tensor-core
+// transforms (lengths 32 and 40): 2R x 2R, K-major canonical layout, FP16 hi
+// then lo, built on the host in FP64 and uploaded with the twiddle tables.
+// Device address of length R's matrices (after ensure_twiddles), else null.
+constexpr uint32_t tc_dft_mat_bytes(int R) { return 2u * (uint32_t)(2 * R) * (uint32_t)(2 * R) * 2u; }
+const uint8_t* tc_dft_mats(int R);
+
 template <int N>
 __device__ __forceinline__ void load_twiddles(float2* tw, const float2* __restrict__ table, int tid, int nthreads) {
   constexpr int off = tw_offset(N);

@@ -10,6 +10,13 @@
 
 namespace cx {
 
+// X H(ky, kx) out of line: the propagator's branches (kernel kinds, FP64
+// phase) inlined at each of a tile's unrolled bins would overflow the
+// instruction cache
+__device__ __noinline__ float2 prop_mult(float2 X, int ky, int kx, const Prop2DArgs* a, const cx_plane* pl) {
+  return cmul(X, prop_kernel(ky, kx, *a, *pl));
+}
+
 template <int N1, int N2>
 struct PropTcCfg {
   using F = TcFft<N1, N2>;
@@ -20,7 +27,7 @@ struct PropTcCfg {
 
 template <int N1, int N2>
 __global__ void __launch_bounds__(256, 1) k_prop_cols_tc(const float2* T, float2* T2, Prop2DArgs a,
-                                                         const float2* __restrict__ twN) {
+                                                         const float2* __restrict__ twN, TcMats mats) {
   using F = TcFft<N1, N2>;
   using C = PropTcCfg<N1, N2>;
   constexpr int N = F::N;
@@ -35,8 +42,8 @@ __global__ void __launch_bounds__(256, 1) k_prop_cols_tc(const float2* T, float2
   S.red = reinterpret_cast<float*>(S.bar + 8);
   const int tid = threadIdx.x;
 
-  tc_fft_build_b<N1>(S.B1, false, tid, blockDim.x);
-  tc_fft_build_b<N2>(S.B2, false, tid, blockDim.x);
+  tc_fft_copy_b(S.B1, mats.b1, F::B1_BYTES, tid, blockDim.x);
+  tc_fft_copy_b(S.B2, mats.b2, F::B2_BYTES, tid, blockDim.x);
   for (int i = tid; i < N; i += blockDim.x) tw[i] = twN[i];
   if ((tid >> 5) == 0) {
     tc::tmem_alloc(tslot, F::TMEM_COLS);
@@ -79,7 +86,7 @@ __global__ void __launch_bounds__(256, 1) k_prop_cols_tc(const float2* T, float2
         for (int k = 0; k < 8; ++k) o[k] = make_float2(0.f, 0.f);
       }
     };
-    auto mult = [&](int k, int v, float2 X) { return cmul(X, prop_kernel(k, x0 + v, a, pl)); };
+    auto mult = [&](int k, int v, float2 X) { return prop_mult(X, k, x0 + v, &a, &pl); };
     auto store_row = [&](int n, const float2* row) {
       const int r = n - a.out_y0;
       if (r >= 0 && r < a.out_ny) {
@@ -120,7 +127,9 @@ static cx_status launch_prop_cols_tc(const float2* T, float2* T2, const Prop2DAr
   const long items = (long)(a.px / 8) * a.n_out_planes;
   int grid = sm_count();
   if (items < grid) grid = (int)items;
-  k<<<grid, 256, C::SMEM, st>>>(T, T2, a, a.twg + tw_offset(C::N));
+  TcMats mats;
+  if (const cx_status e = tc_mats(N1, N2, &mats)) return e;
+  k<<<grid, 256, C::SMEM, st>>>(T, T2, a, a.twg + tw_offset(C::N), mats);
   CX_LAUNCH_CHECK();
   return CX_OK;
 }
@@ -145,7 +154,7 @@ struct PropTcRowCfg {
 
 template <int N1, int N2, bool INV>
 __global__ void __launch_bounds__(256, 1) k_prop_rows_tc(const float2* in, float2* out, Prop2DArgs a,
-                                                         const float2* __restrict__ twN) {
+                                                         const float2* __restrict__ twN, TcMats mats) {
   using F = TcFft<N1, N2>;
   using C = PropTcRowCfg<N1, N2>;
   constexpr int N = F::N;
@@ -161,8 +170,8 @@ __global__ void __launch_bounds__(256, 1) k_prop_rows_tc(const float2* in, float
   PropTcRow* rp = reinterpret_cast<PropTcRow*>(S.red + 64);
   const int tid = threadIdx.x;
 
-  tc_fft_build_b<N1>(S.B1, false, tid, blockDim.x);
-  tc_fft_build_b<N2>(S.B2, false, tid, blockDim.x);
+  tc_fft_copy_b(S.B1, mats.b1, F::B1_BYTES, tid, blockDim.x);
+  tc_fft_copy_b(S.B2, mats.b2, F::B2_BYTES, tid, blockDim.x);
   for (int i = tid; i < N; i += blockDim.x) tw[i] = twN[i];
   if ((tid >> 5) == 0) {
     tc::tmem_alloc(tslot, F::TMEM_COLS);
@@ -272,7 +281,9 @@ static cx_status launch_prop_rows_tc(const float2* in, float2* out, const Prop2D
   const long tiles = ((long)(INV ? a.n_out_planes : a.n_in_planes) * (INV ? a.out_ny : a.ny) + 7) / 8;
   int grid = sm_count();
   if (tiles < grid) grid = (int)tiles;
-  k<<<grid, 256, C::SMEM, st>>>(in, out, a, a.twg + tw_offset(C::N));
+  TcMats mats;
+  if (const cx_status e = tc_mats(N1, N2, &mats)) return e;
+  k<<<grid, 256, C::SMEM, st>>>(in, out, a, a.twg + tw_offset(C::N), mats);
   CX_LAUNCH_CHECK();
   return CX_OK;
 }

@@ -19,7 +19,7 @@ struct PsfTcCfg {
 };
 
 template <int N1, int N2>
-__global__ void __launch_bounds__(256, 1) k_psf_cols_tc(PsfArgs a, const float2* __restrict__ twN) {
+__global__ void __launch_bounds__(256, 1) k_psf_cols_tc(PsfArgs a, const float2* __restrict__ twN, TcMats mats) {
   using F = TcFft<N1, N2>;
   using C = PsfTcCfg<N1, N2>;
   constexpr int N = F::N, ACC = C::ACC;
@@ -35,8 +35,8 @@ __global__ void __launch_bounds__(256, 1) k_psf_cols_tc(PsfArgs a, const float2*
   S.red = reinterpret_cast<float*>(S.bar + 8);
   const int tid = threadIdx.x;
 
-  tc_fft_build_b<N1>(S.B1, false, tid, blockDim.x);
-  tc_fft_build_b<N2>(S.B2, false, tid, blockDim.x);
+  tc_fft_copy_b(S.B1, mats.b1, F::B1_BYTES, tid, blockDim.x);
+  tc_fft_copy_b(S.B2, mats.b2, F::B2_BYTES, tid, blockDim.x);
   for (int i = tid; i < N; i += blockDim.x) tw[i] = twN[i];
   if ((tid >> 5) == 0) {
     tc::tmem_alloc(tslot, F::TMEM_COLS);
@@ -121,7 +121,9 @@ static cx_status launch_psf_cols_tc(const PsfArgs& a, cudaStream_t st) {
   const long items = (long)(a.nx / 8) * a.zc;
   int grid = sm_count();
   if (items < grid) grid = (int)items;
-  k<<<grid, 256, C::SMEM, st>>>(a, a.twg + tw_offset(C::N));
+  TcMats mats;
+  if (const cx_status e = tc_mats(N1, N2, &mats)) return e;
+  k<<<grid, 256, C::SMEM, st>>>(a, a.twg + tw_offset(C::N), mats);
   CX_LAUNCH_CHECK();
   return CX_OK;
 }
@@ -148,7 +150,7 @@ struct PsfTcRowCfg {
 };
 
 template <int N1, int N2>
-__global__ void __launch_bounds__(256, 1) k_psf_rows_tc(PsfArgs a, const float2* __restrict__ twN) {
+__global__ void __launch_bounds__(256, 1) k_psf_rows_tc(PsfArgs a, const float2* __restrict__ twN, TcMats mats) {
   using F = TcFft<N1, N2>;
   using C = PsfTcRowCfg<N1, N2>;
   constexpr int N = F::N;
@@ -164,8 +166,8 @@ __global__ void __launch_bounds__(256, 1) k_psf_rows_tc(PsfArgs a, const float2*
   PsfTcRow* rp = reinterpret_cast<PsfTcRow*>(S.red + 64);
   const int tid = threadIdx.x;
 
-  tc_fft_build_b<N1>(S.B1, false, tid, blockDim.x);
-  tc_fft_build_b<N2>(S.B2, false, tid, blockDim.x);
+  tc_fft_copy_b(S.B1, mats.b1, F::B1_BYTES, tid, blockDim.x);
+  tc_fft_copy_b(S.B2, mats.b2, F::B2_BYTES, tid, blockDim.x);
   for (int i = tid; i < N; i += blockDim.x) tw[i] = twN[i];
   if ((tid >> 5) == 0) {
     tc::tmem_alloc(tslot, F::TMEM_COLS);
@@ -252,7 +254,9 @@ static cx_status launch_psf_rows_tc(const PsfArgs& a, cudaStream_t st) {
   const long tiles = ((long)a.zc * a.rowsum + 7) / 8;
   int grid = sm_count();
   if (tiles < grid) grid = (int)tiles;
-  k<<<grid, 256, C::SMEM, st>>>(a, a.twg + tw_offset(C::N));
+  TcMats mats;
+  if (const cx_status e = tc_mats(N1, N2, &mats)) return e;
+  k<<<grid, 256, C::SMEM, st>>>(a, a.twg + tw_offset(C::N), mats);
   CX_LAUNCH_CHECK();
   return CX_OK;
 }

@@ -56,6 +56,21 @@ struct TcFft {
   static_assert(N1 <= 64, "stage-1 output range stays inside FP16");
 };
 
+// device addresses of a transform's two DFT matrices (tc_dft_mats)
+struct TcMats {
+  const uint8_t* b1;
+  const uint8_t* b2;
+};
+inline cx_status tc_mats(int n1, int n2, TcMats* m) {
+  m->b1 = tc_dft_mats(n1);
+  m->b2 = tc_dft_mats(n2);
+  if (!m->b1 || !m->b2) {
+    set_error("tensor-core DFT matrices of lengths %d / %d are not on the device (cx_init)", n1, n2);
+    return CX_ERR_CUDA;
+  }
+  return CX_OK;
+}
+
 struct TcFftSmem {
   uint8_t* A;   // A1 / A2 (hi tiles then lo tiles)
   uint8_t* B1;  // hi then lo
@@ -81,6 +96,15 @@ __device__ void tc_fft_build_b(uint8_t* B, bool inverse, int tid, int nthreads) 
     *reinterpret_cast<__half*>(B + tc::off_kmajor(K, j, k)) = h;
     *reinterpret_cast<__half*>(B + K * K * 2 + tc::off_kmajor(K, j, k)) = l;
   }
+}
+
+// copy the prebuilt DFT matrices (tc_dft_mats: hi then lo, `bytes` in all)
+// into shared memory, 16 bytes per thread and step
+__device__ __forceinline__ void tc_fft_copy_b(uint8_t* dst, const uint8_t* __restrict__ src, uint32_t bytes, int tid,
+                                              int nthreads) {
+  const uint4* s4 = reinterpret_cast<const uint4*>(src);
+  uint4* d4 = reinterpret_cast<uint4*>(dst);
+  for (uint32_t i = tid; i < bytes / 16; i += nthreads) d4[i] = s4[i];
 }
 
 // 8 values (one 16-byte chunk of an operand) split and stored as hi / lo
