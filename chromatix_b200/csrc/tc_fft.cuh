@@ -107,6 +107,16 @@ __device__ __forceinline__ void tc_fft_copy_b(uint8_t* dst, const uint8_t* __res
   for (uint32_t i = tid; i < bytes / 16; i += nthreads) d4[i] = s4[i];
 }
 
+// The input row a thread loads as its i-th chunk q = tid + 256 i of a column
+// tile: n1 varies fastest across threads, so the eight lanes of a 16-byte
+// store phase write the stage-1 operand's consecutive K columns (16 bytes
+// apart: no bank conflicts); the global loads are whole 64-byte row pieces
+// either way.
+template <class F>
+__device__ __forceinline__ int tc_col_row(int q) {
+  return F::N2 * (q % F::N1) + q / F::N1;
+}
+
 // 8 values (one 16-byte chunk of an operand) split and stored as hi / lo
 __device__ __forceinline__ void tc_store_chunk(uint8_t* hi_base, uint8_t* lo_base, uint32_t off, const float* v8) {
   uint32_t hi[4], lo[4];
@@ -179,7 +189,7 @@ __device__ bool tc_fft_tile(const TcFftSmem& S, uint32_t tmem, uint32_t& phase, 
   for (int v = 0; v < 8; ++v) mx[v] = 0.f;
 #pragma unroll
   for (int i = 0; i < F::RPT; ++i) {
-    load8(tid + i * F::THREADS, xv[i]);
+    load8(tc_col_row<F>(tid + i * F::THREADS), xv[i]);
 #pragma unroll
     for (int v = 0; v < 8; ++v) mx[v] = fmaxf(mx[v], fmaxf(fabsf(xv[i][v].x), fabsf(xv[i][v].y)));
   }
@@ -209,8 +219,8 @@ __device__ bool tc_fft_tile(const TcFftSmem& S, uint32_t tmem, uint32_t& phase, 
   uint8_t* A1lo = S.A + F::T1 * F::A1_TILE;
 #pragma unroll
   for (int i = 0; i < F::RPT; ++i) {
-    const int n = tid + i * F::THREADS;
-    const int n1 = n / N2, n2 = n % N2;
+    const int q = tid + i * F::THREADS;
+    const int n1 = q % N1, n2 = q / N1;  // input row N2 n1 + n2 (tc_col_row)
     const int t = n2 >> 4;  // 16 values of n2 per 128-row tile
     const uint32_t tile = (uint32_t)t * F::A1_TILE;
     float re[8], im[8];
@@ -369,7 +379,7 @@ __device__ bool tc_fft_mult_tile(const TcFftSmem& S, uint32_t tmem, uint32_t& ph
   for (int v = 0; v < 8; ++v) mx[v] = 0.f;
 #pragma unroll
   for (int i = 0; i < F::RPT; ++i) {
-    load8(tid + i * F::THREADS, xv[i]);
+    load8(tc_col_row<F>(tid + i * F::THREADS), xv[i]);
 #pragma unroll
     for (int v = 0; v < 8; ++v) mx[v] = fmaxf(mx[v], fmaxf(fabsf(xv[i][v].x), fabsf(xv[i][v].y)));
   }
@@ -396,8 +406,8 @@ __device__ bool tc_fft_mult_tile(const TcFftSmem& S, uint32_t tmem, uint32_t& ph
   uint8_t* Ahi = S.A;
 #pragma unroll
   for (int i = 0; i < F::RPT; ++i) {
-    const int n = tid + i * F::THREADS;
-    const int n1 = n / N2, n2 = n % N2;
+    const int q = tid + i * F::THREADS;
+    const int n1 = q % N1, n2 = q / N1;  // input row N2 n1 + n2 (tc_col_row)
     const uint32_t tile = (uint32_t)(n2 >> 4) * F::A1_TILE;
     float re[8], im[8];
 #pragma unroll
@@ -560,7 +570,8 @@ __device__ bool tc_fft_rows_tile(const TcFftSmem& S, uint32_t tmem, uint32_t& ph
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const uint32_t wl = (uint32_t)((warp & 3) * 32) << 16;
 
-  // ---- load: chunk c = tid + 256 i is row c / CPR, elements 8 (c % CPR) ..
+  // ---- load: chunk c = tid + 256 i is row v = c / CPR; its 8 elements start at
+  // n0 = 8 (r / L1) + L2 (r % L1), r = c % CPR (a chunk per (n_a group, n_b))
   float2 xv[F::RPT][8];
   float mx[8];
 #pragma unroll
@@ -568,7 +579,8 @@ __device__ bool tc_fft_rows_tile(const TcFftSmem& S, uint32_t tmem, uint32_t& ph
 #pragma unroll
   for (int i = 0; i < F::RPT; ++i) {
     const int c = tid + i * F::THREADS;
-    const int v = c / CPR, n0 = (c - v * CPR) * 8;
+    const int v = c / CPR, r = c - v * CPR;
+    const int n0 = 8 * (r / L1) + L2 * (r % L1);  // nb = r % L1 fastest (conflict-free operand stores)
     load8(v, n0, xv[i]);
     float m = 0.f;
 #pragma unroll
@@ -602,8 +614,8 @@ __device__ bool tc_fft_rows_tile(const TcFftSmem& S, uint32_t tmem, uint32_t& ph
 #pragma unroll
   for (int i = 0; i < F::RPT; ++i) {
     const int c = tid + i * F::THREADS;
-    const int v = c / CPR, n0 = (c - v * CPR) * 8;
-    const int na0 = n0 % L2, nb = n0 / L2;  // the chunk's 8 elements share nb (L2 % 8 == 0)
+    const int v = c / CPR, r = c - v * CPR;
+    const int na0 = 8 * (r / L1), nb = r % L1;  // the chunk's 8 elements share nb (L2 % 8 == 0)
     float s = sc[0];
 #pragma unroll
     for (int r = 1; r < 8; ++r) s = (r == v) ? sc[r] : s;
