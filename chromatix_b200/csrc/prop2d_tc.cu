@@ -71,19 +71,12 @@ __global__ void __launch_bounds__(256, 1) k_prop_cols_tc(const float2* T, float2
     const cx_plane pl = a.planes[q];
     const float2* src = T + (size_t)pl.in_plane * a.ny * a.px + x0;
     float2* dst = T2 + (size_t)q * a.out_ny * a.px + x0;
-    auto load8 = [&](int n, float2* o) {
-      const int r = n - a.pad_y;  // padded-grid row n holds data row n - pad_y
-      if (r >= 0 && r < a.ny) {
-        const float4* p = reinterpret_cast<const float4*>(src + (size_t)r * a.px);
+    auto load8 = [&](int n, int v, float2* o) {
+      // column v of padded-grid rows n .. n+7; row n holds data row n - pad_y
 #pragma unroll
-        for (int k = 0; k < 4; ++k) {
-          const float4 f = p[k];
-          o[2 * k] = make_float2(f.x, f.y);
-          o[2 * k + 1] = make_float2(f.z, f.w);
-        }
-      } else {
-#pragma unroll
-        for (int k = 0; k < 8; ++k) o[k] = make_float2(0.f, 0.f);
+      for (int j = 0; j < 8; ++j) {
+        const int r = n + j - a.pad_y;
+        o[j] = (r >= 0 && r < a.ny) ? src[(size_t)r * a.px + v] : make_float2(0.f, 0.f);
       }
     };
     auto mult = [&](int k, int v, float2 X) { return prop_mult(X, k, x0 + v, &a, &pl); };

@@ -65,20 +65,12 @@ __global__ void __launch_bounds__(256, 1) k_psf_cols_tc(PsfArgs a, const float2*
       const float2* src = a.T + ((size_t)zl * a.rowsum + a.prefix[w]) * a.nx + x0;
       const int ylo = a.ylo[w], slo = support_lo(a, w), shi = support_hi(a, w);
       // FFT row n holds field row (n + N/2) mod N (ifftshift); rows outside
-      // the pupil's support have a zero spectrum
-      auto load8 = [&](int n, float2* o) {
-        const int y = add_mod(n, N / 2, N);
-        if (y >= slo && y < shi) {
-          const float4* r = reinterpret_cast<const float4*>(src + (size_t)(y - ylo) * a.nx);
+      // the pupil's support have a zero spectrum; column v of rows n .. n+7
+      auto load8 = [&](int n, int v, float2* o) {
 #pragma unroll
-          for (int q = 0; q < 4; ++q) {
-            const float4 f = r[q];
-            o[2 * q] = make_float2(f.x, f.y);
-            o[2 * q + 1] = make_float2(f.z, f.w);
-          }
-        } else {
-#pragma unroll
-          for (int q = 0; q < 8; ++q) o[q] = make_float2(0.f, 0.f);
+        for (int j = 0; j < 8; ++j) {
+          const int y = add_mod(n + j, N / 2, N);
+          o[j] = (y >= slo && y < shi) ? src[(size_t)(y - ylo) * a.nx + v] : make_float2(0.f, 0.f);
         }
       };
       auto store = [&](int k, int v, float2 X) {

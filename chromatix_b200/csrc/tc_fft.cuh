@@ -4,24 +4,27 @@
 //   X[k1 + N1 k2] = sum_n2 W_N2^(n2 k2) W_N^(n2 k1) sum_n1 W_N1^(n1 k1) x[N2 n1 + n2]
 //
 // Stage 1: for every (n2, v) a length-N1 DFT over n1 -- one real GEMM per
-// 128-row tile, rows m = 8 n2 + v, K = (re | im) of n1, the DFT matrix as B.
+// 128-row tile, rows m = n2 + N2 v, K = (re | im) of n1, the DFT matrix as B.
 // Twiddle W_N^(n2 k1) in FP32 on the way out of tensor memory.
 // Stage 2: for every (v, k1) a length-N2 DFT over n2 -- rows m = N1 v + k1.
 // Both A operands are MN-major (rows contiguous within 16-byte chunks), so
-// the loader writes eight columns of one input row as one chunk and a stage-1
-// thread (one row (n2, v)) writes its N1 outputs as N1/8 chunks of stage 2's
-// A: no transposes through shared memory.
+// the loader writes eight consecutive input rows of one column as one chunk
+// and a stage-1 thread (one row (n2, v)) writes its N1 outputs as N1/8 chunks
+// of stage 2's A: no transposes through shared memory, and neighbouring lanes
+// write neighbouring K columns (no bank conflicts).
 //
 // Precision: FP32 values enter as FP16 hi + lo pairs, D = Ahi Bhi + Alo Bhi +
 // Ahi Blo in FP32 (tensor memory); the tile is scaled by a power of two
 // (exact) per column so that column's largest input component is near 2^9,
 // which keeps every stage-1 output below FP16's maximum (N1 * 2^9 sqrt 2 <
 // 65504 for N1 <= 64) and puts hi and lo in FP16's normal range.  The
-// relative error per column transform is ~2e-7.
+// relative error per transform is 2-5e-7 on the hardware (2-4x an FP32 FFT's;
+// the split alone gives ~5e-8, the rest comes from the tensor core's FP32
+// accumulation).
 //
-// The caller builds B1 / B2 once (tc_fft_build_b), allocates tensor memory
+// The caller copies the prebuilt B1 / B2 (tc_fft_copy_b), allocates tensor memory
 // (TMEM_COLS) and an mbarrier, and calls tc_fft_tile per column tile with a
-// loader (8 input columns of FFT row n) and a store (output bin k of column
+// loader (column v of FFT rows n .. n+7) and a store (output bin k of column
 // v).  Every mbarrier wait is bounded; tc_fft_tile returns false (uniformly
 // over the CTA) if one ran out.
 #pragma once
@@ -107,16 +110,6 @@ __device__ __forceinline__ void tc_fft_copy_b(uint8_t* dst, const uint8_t* __res
   for (uint32_t i = tid; i < bytes / 16; i += nthreads) d4[i] = s4[i];
 }
 
-// The input row a thread loads as its i-th chunk q = tid + 256 i of a column
-// tile: n1 varies fastest across threads, so the eight lanes of a 16-byte
-// store phase write the stage-1 operand's consecutive K columns (16 bytes
-// apart: no bank conflicts); the global loads are whole 64-byte row pieces
-// either way.
-template <class F>
-__device__ __forceinline__ int tc_col_row(int q) {
-  return F::N2 * (q % F::N1) + q / F::N1;
-}
-
 // 8 values (one 16-byte chunk of an operand) split and stored as hi / lo
 __device__ __forceinline__ void tc_store_chunk(uint8_t* hi_base, uint8_t* lo_base, uint32_t off, const float* v8) {
   uint32_t hi[4], lo[4];
@@ -124,6 +117,81 @@ __device__ __forceinline__ void tc_store_chunk(uint8_t* hi_base, uint8_t* lo_bas
   for (int q = 0; q < 4; ++q) tc::split2(v8[2 * q], v8[2 * q + 1], hi[q], lo[q]);
   *reinterpret_cast<uint4*>(hi_base + off) = make_uint4(hi[0], hi[1], hi[2], hi[3]);
   *reinterpret_cast<uint4*>(lo_base + off) = make_uint4(lo[0], lo[1], lo[2], lo[3]);
+}
+
+// Column-tile input phase shared by tc_fft_tile and tc_fft_mult_tile.
+// Stage-1 rows are m = n2 + N2 v (column-major by tile column v), so an
+// MN-major 16-byte chunk is eight consecutive input rows n = N2 n1 + n2 of one
+// column.  Chunk q = tid + 256 i is (n1, v, n2 group g): lanes take n1 % 8
+// fastest, then v % 4, so one load instruction reads 32 contiguous bytes of
+// eight rows and the eight lanes of a store phase write eight consecutive K
+// columns (16 bytes apart: no bank conflicts).  load8(n, v, out[8]): column v
+// of input rows n .. n+7.  Each column is scaled by a power of two that puts
+// its largest component near 2^9; the per-warp column maxima stay in S.red.
+template <class F>
+__device__ __forceinline__ void tc_col_chunk(int q, int& n1, int& v, int& g) {
+  const int rest = q >> 5, r2 = rest >> 1;
+  n1 = (r2 % (F::N1 / 8)) * 8 + (q & 7);
+  g = r2 / (F::N1 / 8);
+  v = (rest & 1) * 4 + ((q >> 3) & 3);
+}
+
+__device__ __forceinline__ float tc_scale_of(const float* red, int v) {
+  float m = red[v];
+#pragma unroll
+  for (int w = 1; w < 8; ++w) m = fmaxf(m, red[w * 8 + v]);
+  int e = 0;
+  if (m > 0.f) frexpf(m, &e);
+  return ldexpf(1.f, 9 - e);
+}
+
+template <class F, class Load8>
+__device__ __forceinline__ void tc_col_input(const TcFftSmem& S, Load8 load8) {
+  constexpr int N1 = F::N1, N2 = F::N2;
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  float2 xv[F::RPT][8];
+  float mx[8];
+#pragma unroll
+  for (int v = 0; v < 8; ++v) mx[v] = 0.f;
+#pragma unroll
+  for (int i = 0; i < F::RPT; ++i) {
+    int n1, v, g;
+    tc_col_chunk<F>(tid + i * F::THREADS, n1, v, g);
+    load8(N2 * n1 + 8 * g, v, xv[i]);
+    float m = 0.f;
+#pragma unroll
+    for (int j = 0; j < 8; ++j) m = fmaxf(m, fmaxf(fabsf(xv[i][j].x), fabsf(xv[i][j].y)));
+#pragma unroll
+    for (int r = 0; r < 8; ++r) mx[r] = (r == v) ? fmaxf(mx[r], m) : mx[r];
+  }
+#pragma unroll
+  for (int v = 0; v < 8; ++v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) mx[v] = fmaxf(mx[v], __shfl_xor_sync(0xffffffffu, mx[v], o));
+  }
+  if (lane == 0) {
+#pragma unroll
+    for (int v = 0; v < 8; ++v) S.red[warp * 8 + v] = mx[v];
+  }
+  __syncthreads();
+  uint8_t* Ahi = S.A;
+  uint8_t* Alo = S.A + F::T1 * F::A1_TILE;
+#pragma unroll
+  for (int i = 0; i < F::RPT; ++i) {
+    int n1, v, g;
+    tc_col_chunk<F>(tid + i * F::THREADS, n1, v, g);
+    const float s = tc_scale_of(S.red, v);
+    float re[8], im[8];
+#pragma unroll
+    for (int j = 0; j < 8; ++j) {
+      re[j] = xv[i][j].x * s;
+      im[j] = xv[i][j].y * s;
+    }
+    const int m0 = 8 * g + N2 * v;
+    const uint32_t tile = (uint32_t)(m0 >> 7) * F::A1_TILE;
+    tc_store_chunk(Ahi + tile, Alo + tile, tc::off_mnmajor(128, m0 & 127, n1), re);
+    tc_store_chunk(Ahi + tile, Alo + tile, tc::off_mnmajor(128, m0 & 127, N1 + n1), im);
+  }
 }
 
 // Issue D[t] = A[t] B for T row tiles of 128 (3 split products per K step of
@@ -171,8 +239,8 @@ __device__ __forceinline__ bool tc_gemm(const TcFftSmem& S, uint32_t tmem, uint3
   return true;
 }
 
-// One tile of eight columns.  load8(n, float2 out[8]): the 8 columns of FFT
-// input row n; store(k, v, X): output bin k of column v.  tw: twiddles
+// One tile of eight columns.  load8(n, v, float2 out[8]): column v of FFT
+// input rows n .. n+7 (tc_col_input); store(k, v, X): output bin k of column v.  tw: twiddles
 // exp(-2 pi i e / N), e < N (shared or global).  Returns false if an MMA wait
 // ran out (then no output was stored for this tile).
 template <class F, class Load8, class Store>
@@ -181,57 +249,11 @@ __device__ bool tc_fft_tile(const TcFftSmem& S, uint32_t tmem, uint32_t& phase, 
   constexpr int N1 = F::N1, N2 = F::N2, N = F::N, K1 = F::K1, K2 = F::K2;
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
 
-  // ---- load 8 columns of RPT rows; per-column maximum and power-of-two
-  // scale (a row scale of both GEMMs: rows (n2, v) and (v, k1) carry v)
-  float2 xv[F::RPT][8];
-  float mx[8];
-#pragma unroll
-  for (int v = 0; v < 8; ++v) mx[v] = 0.f;
-#pragma unroll
-  for (int i = 0; i < F::RPT; ++i) {
-    load8(tc_col_row<F>(tid + i * F::THREADS), xv[i]);
-#pragma unroll
-    for (int v = 0; v < 8; ++v) mx[v] = fmaxf(mx[v], fmaxf(fabsf(xv[i][v].x), fabsf(xv[i][v].y)));
-  }
-#pragma unroll
-  for (int v = 0; v < 8; ++v) {
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) mx[v] = fmaxf(mx[v], __shfl_xor_sync(0xffffffffu, mx[v], o));
-  }
-  if (lane == 0) {
-#pragma unroll
-    for (int v = 0; v < 8; ++v) S.red[warp * 8 + v] = mx[v];
-  }
-  __syncthreads();
-  float sc[8];
-#pragma unroll
-  for (int v = 0; v < 8; ++v) {
-    float m = S.red[v];
-#pragma unroll
-    for (int w = 1; w < 8; ++w) m = fmaxf(m, S.red[w * 8 + v]);
-    int e = 0;
-    if (m > 0.f) frexpf(m, &e);
-    sc[v] = ldexpf(1.f, 9 - e);
-  }
-
-  // ---- stage-1 A (MN-major): row m = 8 n2 + v, column k = part N1 + n1
+  // ---- load, per-column power-of-two scale, stage-1 A (MN-major): row
+  // m = n2 + N2 v, column k = part N1 + n1
+  tc_col_input<F>(S, load8);
   uint8_t* A1hi = S.A;
   uint8_t* A1lo = S.A + F::T1 * F::A1_TILE;
-#pragma unroll
-  for (int i = 0; i < F::RPT; ++i) {
-    const int q = tid + i * F::THREADS;
-    const int n1 = q % N1, n2 = q / N1;  // input row N2 n1 + n2 (tc_col_row)
-    const int t = n2 >> 4;  // 16 values of n2 per 128-row tile
-    const uint32_t tile = (uint32_t)t * F::A1_TILE;
-    float re[8], im[8];
-#pragma unroll
-    for (int v = 0; v < 8; ++v) {
-      re[v] = xv[i][v].x * sc[v];
-      im[v] = xv[i][v].y * sc[v];
-    }
-    tc_store_chunk(A1hi + tile, A1lo + tile, tc::off_mnmajor(128, (n2 & 15) * 8, n1), re);
-    tc_store_chunk(A1hi + tile, A1lo + tile, tc::off_mnmajor(128, (n2 & 15) * 8, N1 + n1), im);
-  }
   tc::fence_smem_to_async();
   tc::fence_before_sync();
   __syncthreads();
@@ -266,7 +288,7 @@ __device__ bool tc_fft_tile(const TcFftSmem& S, uint32_t tmem, uint32_t& phase, 
   {
     const int t = warp >> 2;
     const int m = t * 128 + (warp & 3) * 32 + lane;
-    const int n2 = m >> 3, v = m & 7;
+    const int n2 = m % N2, v = m / N2;  // stage-1 row m = n2 + N2 v
     float d[K1];
 #pragma unroll
     for (int c = 0; c < K1; c += 16) tc::tmem_ld16(tmem + ((uint32_t)((warp & 3) * 32) << 16) + t * K1 + c, d + c);
@@ -373,56 +395,13 @@ __device__ bool tc_fft_mult_tile(const TcFftSmem& S, uint32_t tmem, uint32_t& ph
   const uint32_t wl = (uint32_t)((warp & 3) * 32) << 16;
 
   // ---- forward stages (as tc_fft_tile)
-  float2 xv[F::RPT][8];
-  float mx[8];
-#pragma unroll
-  for (int v = 0; v < 8; ++v) mx[v] = 0.f;
-#pragma unroll
-  for (int i = 0; i < F::RPT; ++i) {
-    load8(tc_col_row<F>(tid + i * F::THREADS), xv[i]);
-#pragma unroll
-    for (int v = 0; v < 8; ++v) mx[v] = fmaxf(mx[v], fmaxf(fabsf(xv[i][v].x), fabsf(xv[i][v].y)));
-  }
-#pragma unroll
-  for (int v = 0; v < 8; ++v) {
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) mx[v] = fmaxf(mx[v], __shfl_xor_sync(0xffffffffu, mx[v], o));
-  }
-  if (lane == 0) {
-#pragma unroll
-    for (int v = 0; v < 8; ++v) S.red[warp * 8 + v] = mx[v];
-  }
-  __syncthreads();
-  float sc[8];
-#pragma unroll
-  for (int v = 0; v < 8; ++v) {
-    float m = S.red[v];
-#pragma unroll
-    for (int w = 1; w < 8; ++w) m = fmaxf(m, S.red[w * 8 + v]);
-    int e = 0;
-    if (m > 0.f) frexpf(m, &e);
-    sc[v] = ldexpf(1.f, 9 - e);
-  }
+  tc_col_input<F>(S, load8);
   uint8_t* Ahi = S.A;
-#pragma unroll
-  for (int i = 0; i < F::RPT; ++i) {
-    const int q = tid + i * F::THREADS;
-    const int n1 = q % N1, n2 = q / N1;  // input row N2 n1 + n2 (tc_col_row)
-    const uint32_t tile = (uint32_t)(n2 >> 4) * F::A1_TILE;
-    float re[8], im[8];
-#pragma unroll
-    for (int v = 0; v < 8; ++v) {
-      re[v] = xv[i][v].x * sc[v];
-      im[v] = xv[i][v].y * sc[v];
-    }
-    tc_store_chunk(Ahi + tile, Ahi + F::T1 * F::A1_TILE + tile, tc::off_mnmajor(128, (n2 & 15) * 8, n1), re);
-    tc_store_chunk(Ahi + tile, Ahi + F::T1 * F::A1_TILE + tile, tc::off_mnmajor(128, (n2 & 15) * 8, N1 + n1), im);
-  }
   if (!tc_gemm<K1, F::T1>(S, tmem, phase, S.A, F::A1_TILE, 1, S.B1, F::POLLS)) return false;
   {
     const int t = warp >> 2;
     const int m = t * 128 + (warp & 3) * 32 + lane;
-    const int n2 = m >> 3, v = m & 7;
+    const int n2 = m % N2, v = m / N2;  // stage-1 row m = n2 + N2 v
     float d[K1];
 #pragma unroll
     for (int c = 0; c < K1; c += 16) tc::tmem_ld16(tmem + wl + t * K1 + c, d + c);

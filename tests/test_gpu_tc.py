@@ -158,8 +158,11 @@ def test_split16_propagation_1280_grid_and_adjoint():
 
 def test_split16_multislice_1024_forward_and_gradient():
     """Multislice at 1024^2 (the differentiable configuration's grid, 8 slices)
-    with the slice loop's column passes on the tensor cores: forward <= 1e-5
-    and dL/d dn <= 1e-4 against the FP64 restatement."""
+    with the slice loop's row and column transforms on the tensor cores,
+    against the FP64 restatement.  Each slice runs four split-precision
+    transforms (2-5e-7 each on the hardware) and their errors add up slice by
+    slice, so the bars are depth-scaled: forward <= 5e-5 and dL/d dn <= 5e-4
+    at 8 slices (the FP32 path's bars are 1e-5 / 1e-4 at any depth)."""
     import torch
 
     import chromatix_b200 as cx
@@ -182,6 +185,8 @@ def test_split16_multislice_1024_forward_and_gradient():
                                          0.2, 0, checkpoint_every=4)
         loss = ((out.u.abs() ** 2 - torch.as_tensor(target, device="cuda", dtype=torch.float32)) ** 2).sum()
         loss.backward()
-    assert rel(out.u.detach().cpu().numpy(), uo64) < 1e-5
+    e_fwd = rel(out.u.detach().cpu().numpy(), uo64)
+    e_grad = rel(dn_t.grad.cpu().numpy(), gdn64)
+    assert e_fwd < 5e-5, (e_fwd, e_grad)
     assert abs(float(loss) - L64) / L64 < 1e-4
-    assert rel(dn_t.grad.cpu().numpy(), gdn64) < 1e-4
+    assert e_grad < 5e-4, (e_fwd, e_grad)
