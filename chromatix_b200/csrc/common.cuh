@@ -93,6 +93,28 @@ __device__ __forceinline__ void bulk_copy_g2s(void* smem, const void* gmem, unsi
                "l"(gmem), "r"(bytes), "r"(b)
                : "memory");
 }
+// L2 policy for data read or written once per pass (slice rows, records):
+// evicted first, so that the state that every pass reuses stays in L2
+__device__ __forceinline__ uint64_t l2_evict_first() {
+  uint64_t p;
+  asm volatile("createpolicy.fractional.L2::evict_first.b64 %0, 1.0;\n" : "=l"(p));
+  return p;
+}
+// bulk copy global -> shared with an L2 cache policy
+__device__ __forceinline__ void bulk_copy_g2s_hint(void* smem, const void* gmem, unsigned bytes, uint64_t* bar,
+                                                   uint64_t policy) {
+  const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+  const unsigned b = (unsigned)__cvta_generic_to_shared(bar);
+  asm volatile(
+      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes.L2::cache_hint [%0], [%1], %2, [%3], %4;\n" ::"r"(s),
+      "l"(gmem), "r"(bytes), "r"(b), "l"(policy)
+      : "memory");
+}
+// 8-byte global store with an L2 cache policy
+__device__ __forceinline__ void st_hint(float2* p, float2 v, uint64_t policy) {
+  asm volatile("st.global.L2::cache_hint.v2.f32 [%0], {%1, %2}, %3;\n" ::"l"(p), "f"(v.x), "f"(v.y), "l"(policy)
+               : "memory");
+}
 // shared-memory reads by the generic proxy are ordered before later bulk writes
 __device__ __forceinline__ void bulk_fence() { asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory"); }
 // bounded wait for the phase with parity `phase`; false after `polls` polls

@@ -115,10 +115,12 @@ __device__ __forceinline__ bool ms_prefetch(const MsArgs& a, float* pf, uint64_t
     if constexpr (MODE == MS_BWD) bytes += (unsigned)a.px * 8u;
     bulk_fence();  // the previous row's reads of this area precede the new writes
     bulk_expect(bar, bytes);
-    bulk_copy_g2s(pf, dn, rb, bar);
-    bulk_copy_g2s(pf + NXA, ab, rb, bar);
-    if constexpr (MODE == MS_FLUOR) bulk_copy_g2s(pf + 2 * NXA, ph, rb, bar);
-    if constexpr (MODE == MS_BWD) bulk_copy_g2s(pf + 2 * NXA, u, (unsigned)a.px * 8u, bar);
+    // read once per pass: evict first (the field state and the propagator stay in L2)
+    const uint64_t pol = l2_evict_first();
+    bulk_copy_g2s_hint(pf, dn, rb, bar, pol);
+    bulk_copy_g2s_hint(pf + NXA, ab, rb, bar, pol);
+    if constexpr (MODE == MS_FLUOR) bulk_copy_g2s_hint(pf + 2 * NXA, ph, rb, bar, pol);
+    if constexpr (MODE == MS_BWD) bulk_copy_g2s_hint(pf + 2 * NXA, u, (unsigned)a.px * 8u, bar, pol);
   }
   return true;
 }
@@ -212,6 +214,7 @@ __global__ void __launch_bounds__(RowCfg<NX>::THREADS, RowCfg<NX>::MINB) k_ms_ro
       }
     } else if constexpr (MODE == MS_FWD) {
       float2* rrow = a.record ? a.rec + (size_t)y * a.px : nullptr;
+      const uint64_t rpol = l2_evict_first();  // records are read back once, by the adjoint
 #pragma unroll 2
       for (int k = lane; k < NX; k += C::LPV) {
         float2 v = s[pad_idx(k)];
@@ -222,7 +225,7 @@ __global__ void __launch_bounds__(RowCfg<NX>::THREADS, RowCfg<NX>::MINB) k_ms_ro
           const float abv = pre ? pf[MsRowCfg<NX, MODE>::NXA + xd] : a.ab[idx];
           v = cmul(v, ms_transmittance(a, dnv, abv));
         }
-        if (a.record) rrow[k] = v;
+        if (a.record) st_hint(rrow + k, v, rpol);
         s[pad_idx(k)] = v;
       }
     } else {  // MS_BWD
