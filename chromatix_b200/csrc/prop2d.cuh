@@ -183,6 +183,99 @@ __device__ __forceinline__ float2 prop_kernel(int ky, int kx, const Prop2DArgs& 
   return a.conj_h ? cconj(h) : h;
 }
 
+// Per-plane constants of the accurate propagator, formed once per plane (per
+// column tile) instead of per element: the frequency steps as reciprocals
+// (f = k * (1 / (N d)) is within an ulp of k / (N d)), the ASM phase scale
+// K = 2 pi |z| n / lambda, (lambda / n)^2 and the Fresnel phase factor.
+struct PropK {
+  double iy, ix, K, q2, tz;
+  int fast;  // the short-distance FP32 branch of prop_kernel_accurate applies
+};
+
+__device__ __forceinline__ PropK prop_consts(const Prop2DArgs& a, const cx_plane& pl) {
+  const double pi = 3.141592653589793238462643383279502884;
+  PropK c;
+  c.iy = 1.0 / ((double)a.py * pl.dy);
+  c.ix = 1.0 / ((double)a.px * pl.dx);
+  c.K = 2.0 * pi * fabs(pl.z) * a.n_med / pl.wavelength;
+  const double q = pl.wavelength / a.n_med;
+  c.q2 = q * q;
+  c.tz = -pi * pl.wavelength / a.n_med * pl.z;
+  c.fast = (!a.precise && a.kernel == CX_KERNEL_ASM && c.K <= 8.0 && !a.bandlimit && pl.shift_y == 0.0 &&
+            pl.shift_x == 0.0)
+               ? 1
+               : 0;
+  return c;
+}
+
+// prop_kernel_accurate for the transfer and ASM kinds with the per-plane
+// constants hoisted (same branches and operation order otherwise)
+__device__ __forceinline__ float2 prop_kernel_accurate_k(int ky, int kx, const Prop2DArgs& a, const cx_plane& pl,
+                                                         const PropK& c) {
+  const double pi = 3.141592653589793238462643383279502884;
+  const double fy = (double)freq_index(ky, a.py) * c.iy;
+  const double fx = (double)freq_index(kx, a.px) * c.ix;
+  if (c.fast) {
+    const double gy = fy - a.ky0, gx = fx - a.kx0;
+    const float kern = (float)(1.0 - c.q2 * (gy * gy + gx * gx));
+    float amp = 1.f, ph = 0.f;
+    if (kern >= 0.f || a.remove_evanescent) {
+      ph = (float)c.K * sqrtf(fmaxf(kern, 0.f));
+    } else {
+      amp = __expf(-(float)c.K * sqrtf(-kern));
+    }
+    float sn, cs;
+    __sincosf(ph - 6.2831853071795865f * rintf(ph * 0.15915494309189534f), &sn, &cs);
+    if (pl.z < 0.0) sn = -sn;
+    return make_float2(amp * cs, amp * sn);
+  }
+  const double gy = fy - a.ky0, gx = fx - a.kx0;
+  const double s = gy * gy + gx * gx;
+  if (a.kernel == CX_KERNEL_TRANSFER) {
+    const double ph = c.tz * s;
+    if (a.precise) {
+      double sd, cd;
+      sincos(ph, &sd, &cd);
+      return make_float2((float)cd, (float)sd);
+    }
+    return expi_reduced(ph);
+  }
+  if (a.bandlimit && (fabs(fy - pl.bl_y0) > pl.bl_hy || fabs(fx - pl.bl_x0) > pl.bl_hx)) return make_float2(0.f, 0.f);
+  const double kern = 1.0 - c.q2 * s;
+  const double sh = 2.0 * pi * (fy * pl.shift_y + fx * pl.shift_x);
+  double amp = 1.0, ph;
+  if (kern >= 0.0 || a.remove_evanescent) {
+    ph = c.K * sqrt(kern > 0.0 ? kern : 0.0) + sh;
+  } else {
+    amp = exp(-c.K * sqrt(-kern));
+    ph = sh;
+  }
+  if (pl.z < 0.0) ph = -ph;
+  if (a.precise) {
+    double sd, cd;
+    sincos(ph, &sd, &cd);
+    return make_float2((float)(amp * cd), (float)(amp * sd));
+  }
+  float2 e = expi_reduced(ph);
+  return make_float2((float)amp * e.x, (float)amp * e.y);
+}
+
+// prop_kernel with the per-plane constants c = prop_consts(a, pl)
+__device__ __forceinline__ float2 prop_kernel_k(int ky, int kx, const Prop2DArgs& a, const cx_plane& pl,
+                                                const PropK& c) {
+  if (outside_na(ky, kx, a, pl)) return make_float2(0.f, 0.f);
+  float2 h;
+  if (a.kernel == CX_KERNEL_EXPLICIT)
+    h = a.H[((size_t)pl.h_plane * a.py + ky) * a.px + kx];
+  else if (a.precision == CX_PREC_REF32)
+    h = prop_kernel_ref32(ky, kx, a, pl);
+  else if (a.kernel == CX_KERNEL_SAS)
+    h = prop_kernel_accurate(ky, kx, a, pl);
+  else
+    h = prop_kernel_accurate_k(ky, kx, a, pl, c);
+  return a.conj_h ? cconj(h) : h;
+}
+
 // --------------------------------------------------------------------------
 // pass A: forward row FFT with zero padding in the loader
 // --------------------------------------------------------------------------
@@ -238,6 +331,7 @@ __global__ void __launch_bounds__(ColCfg<NY>::THREADS, ColCfg<NY>::MINB) k_prop_
     const int q = (int)(t / tiles_x);
     const int x0 = (int)(t % tiles_x) * V;
     const cx_plane pl = a.planes[q];
+    const PropK kc = prop_consts(a, pl);
     const int p_in = pl.in_plane;
     __syncthreads();
     // cooperative, coalesced load of the ny data rows of this column tile
@@ -249,7 +343,7 @@ __global__ void __launch_bounds__(ColCfg<NY>::THREADS, ColCfg<NY>::MINB) k_prop_
     auto load1 = [&](int n) -> float2 {
       return (n >= a.pad_y && n < a.pad_y + a.ny) ? s[pad_idx(n)] : make_float2(0.f, 0.f);
     };
-    auto store1 = [&](int k, float2 v, int) { s[pad_idx(k)] = valid ? cmul(v, prop_kernel(k, kx, a, pl)) : v; };
+    auto store1 = [&](int k, float2 v, int) { s[pad_idx(k)] = valid ? cmul(v, prop_kernel_k(k, kx, a, pl, kc)) : v; };
     team_fft_ex<NY, false, false, true, C::LPV, C::CTA>(s, tw, lane, team, load1, store1);
     team_barrier<C::LPV, C::CTA>(team);
     auto load2 = [&](int n) -> float2 { return s[pad_idx(n)]; };

@@ -13,8 +13,9 @@ namespace cx {
 // X H(ky, kx) out of line: the propagator's branches (kernel kinds, FP64
 // phase) inlined at each of a tile's unrolled bins would overflow the
 // instruction cache
-__device__ __noinline__ float2 prop_mult(float2 X, int ky, int kx, const Prop2DArgs* a, const cx_plane* pl) {
-  return cmul(X, prop_kernel(ky, kx, *a, *pl));
+__device__ __noinline__ float2 prop_mult(float2 X, int ky, int kx, const Prop2DArgs* a, const cx_plane* pl,
+                                         const PropK* c) {
+  return cmul(X, prop_kernel_k(ky, kx, *a, *pl, *c));
 }
 
 template <int N1, int N2>
@@ -79,7 +80,8 @@ __global__ void __launch_bounds__(256, 1) k_prop_cols_tc(const float2* T, float2
         o[j] = (r >= 0 && r < a.ny) ? src[(size_t)r * a.px + v] : make_float2(0.f, 0.f);
       }
     };
-    auto mult = [&](int k, int v, float2 X) { return prop_mult(X, k, x0 + v, &a, &pl); };
+    const PropK kc = prop_consts(a, pl);
+    auto mult = [&](int k, int v, float2 X) { return prop_mult(X, k, x0 + v, &a, &pl, &kc); };
     auto store_row = [&](int n, const float2* row) {
       const int r = n - a.out_y0;
       if (r >= 0 && r < a.out_ny) {

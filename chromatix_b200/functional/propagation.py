@@ -134,63 +134,19 @@ class _PropPlan:
         return _PropPlan(d, planes, self.out_shape, adj_out, self.chromatic, self.H)
 
 
-# Intermediates (row spectra + filtered column spectra) of one cx_prop2d call
-# are kept below this size when the batch allows it, so that the three passes
-# hand them on through the L2 cache instead of HBM.
-L2_CHUNK_BYTES = 64 << 20
-
-
-def _chunk_fields(plan: _PropPlan) -> int:
-    """Batch elements (fields of W planes) per cx_prop2d call: all of them
-    unless the batch maps plane q to input plane q (so that a range of fields
-    is self-contained) and its intermediates exceed L2_CHUNK_BYTES."""
-    d = plan.desc
-    W = int(d.n_wv)
-    n = int(d.n_in_planes)
-    if n != int(d.n_out_planes) or n // W < 2 or not np.array_equal(plan.planes["in_plane"], np.arange(n)):
-        return max(1, n // W)
-    py, px = d.ny + 2 * d.pad_y, d.nx + 2 * d.pad_x
-    out_ny = d.ny if d.mode_same else py - 2 * d.crop_y
-    per_field = 8 * W * px * (int(d.ny) + int(out_ny))
-    return int(max(1, min(n // W, L2_CHUNK_BYTES // per_field)))
-
-
 def _launch_prop2d(plan: _PropPlan, u_in):
     torch = nat.torch_mod()
     L = nat.lib()
     d = plan.desc
+    ws_bytes = nat.c_size_t(0)
+    nat.check(L.cx_prop2d_workspace_size(d, ws_bytes))
     dev = u_in.device
     u_in = u_in.contiguous()
     u_out = torch.empty(plan.out_shape, dtype=torch.complex64, device=dev)
-    W = int(d.n_wv)
-    n_fields = int(d.n_in_planes) // W
-    cf = _chunk_fields(plan)
-    if cf >= n_fields:
-        ws_bytes = nat.c_size_t(0)
-        nat.check(L.cx_prop2d_workspace_size(d, ws_bytes))
-        ws = nat.workspace(ws_bytes.value, dev)
-        planes_dev = nat.to_device_bytes(plan.planes, dev)
-        nat.check(L.cx_prop2d(d, nat.ptr(planes_dev), nat.ptr(u_in), nat.ptr(u_out), nat.ptr(plan.H), nat.ptr(ws),
-                              ws_bytes.value, nat.stream_handle(dev)))
-        return u_out
-    # fields [f0, f0 + cf) per call: the input / output planes of a field are
-    # contiguous (W interleaved channels), and plane q reads input plane q
-    dc = nat.cx_prop2d_desc.from_buffer_copy(d)
-    dc.n_in_planes = dc.n_out_planes = cf * W
-    ws_bytes = nat.c_size_t(0)
-    nat.check(L.cx_prop2d_workspace_size(dc, ws_bytes))
     ws = nat.workspace(ws_bytes.value, dev)
-    planes = plan.planes.copy()
-    planes["in_plane"] = np.arange(planes.size) % (cf * W)
-    planes_dev = nat.to_device_bytes(planes, dev)
-    in_field = u_in.numel() // n_fields * 8
-    out_field = u_out.numel() // n_fields * 8
-    stream = nat.stream_handle(dev)
-    for f0 in range(0, n_fields, cf):
-        nf = min(cf, n_fields - f0)
-        dc.n_in_planes = dc.n_out_planes = nf * W
-        nat.check(L.cx_prop2d(dc, nat.ptr(planes_dev) + f0 * W * planes.itemsize, nat.ptr(u_in) + f0 * in_field,
-                              nat.ptr(u_out) + f0 * out_field, nat.ptr(plan.H), nat.ptr(ws), ws_bytes.value, stream))
+    planes_dev = nat.to_device_bytes(plan.planes, dev)
+    nat.check(L.cx_prop2d(d, nat.ptr(planes_dev), nat.ptr(u_in), nat.ptr(u_out), nat.ptr(plan.H), nat.ptr(ws),
+                          ws_bytes.value, nat.stream_handle(dev)))
     return u_out
 
 

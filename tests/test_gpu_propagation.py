@@ -272,26 +272,21 @@ def test_absorbing_boundary_is_a_no_op_like_the_reference(boundary):
 
 
 @pytest.mark.parametrize("mode", ["full", "same"])
-def test_l2_chunked_batch_matches_lone_fields_and_adjoint(mode):
-    """A batch of 12 fields (512^2, pad 256) runs as L2-sized chunks of fields
-    (three cx_prop2d calls, the last one partial): every field equals its lone
-    propagation bit for bit, and the gradient of the chunked call equals the
-    lone fields' gradients."""
+def test_batch_matches_lone_fields_and_adjoint(mode):
+    """A batch of 12 fields (512^2, pad 256) in one call: every field equals
+    its lone propagation bit for bit (planes are independent work units), and
+    the batch's gradient equals the lone fields' gradients."""
     import torch
 
     from chromatix_b200.core.field import ScalarField
     from chromatix_b200.core.spectrum import Spectrum
     import chromatix_b200.functional as cf
-    from chromatix_b200.functional import propagation as P
 
     B = 12
     u = np.stack([rand_field((512, 512), seed=40 + b) for b in range(B)])
     ut = torch.as_tensor(u, device="cuda")
     spec = Spectrum.build(0.532)
     batch = cf.asm_propagate(ScalarField(ut, 0.3, 0.0, spec), 50.0, 1.33, 256, mode=mode).u
-    py = 1024
-    per_field = 8 * py * (512 + (py if mode == "full" else 512))
-    assert P.L2_CHUNK_BYTES // per_field < B  # the batch is split
     for b in (0, 4, 5, 11):
         lone = cf.asm_propagate(ScalarField(ut[b], 0.3, 0.0, spec), 50.0, 1.33, 256, mode=mode).u
         assert torch.equal(batch[b], lone), b
