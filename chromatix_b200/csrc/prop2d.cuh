@@ -313,15 +313,8 @@ __global__ void __launch_bounds__(RowCfg<NX>::THREADS, RowCfg<NX>::MINB) k_prop_
 // --------------------------------------------------------------------------
 // pass B: column FFT -> x H -> column IFFT on V-column tiles
 // --------------------------------------------------------------------------
-// CTAs per SM the column pass is compiled for: four at 1024 rows (64
-// registers, 32 of 64 warps) -- the pass is latency-bound at three
 template <int NY>
-constexpr int prop_cols_minb() {
-  return NY == 1024 ? 4 : ColCfg<NY>::MINB;
-}
-
-template <int NY>
-__global__ void __launch_bounds__(ColCfg<NY>::THREADS, prop_cols_minb<NY>()) k_prop_cols(const float2* __restrict__ T,
+__global__ void __launch_bounds__(ColCfg<NY>::THREADS, ColCfg<NY>::MINB) k_prop_cols(const float2* __restrict__ T,
                                                                   float2* __restrict__ T2, Prop2DArgs a) {
   using C = ColCfg<NY>;
   constexpr int V = C::V, LEN = C::LEN;
