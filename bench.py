@@ -464,6 +464,17 @@ def psf_published_arm(args):
 
     with ClockSampler(0) as clk:
         ms = _device_timer(torch, dev, args.steps, args.warmup)(step)
+    acc = None
+    if not args.no_accuracy:
+        # outside the timed region: the first and last planes against the FP64 oracle
+        from oracle import chromatix_oracle as O
+
+        O.set_fft_workers(os.cpu_count())
+        I = step().reshape(n_z, N, N)
+        zz = z.cpu().numpy()[[0, n_z - 1]]
+        ref = O.ff_lens(O.phase_change(O.objective_point_source((N, N), 0.3, 0.532, zz, 100.0, 1.33, 0.8),
+                                       np.ones((N, N), np.float32)), 100.0, 1.33).intensity
+        acc = float(f"{O.rel_l2(I[[0, n_z - 1]].cpu().numpy(), np.asarray(ref).reshape(2, N, N)):.3g}")
     px = n_z * N * N
     published_ms = 25.06
     value = px / (ms * 1e-3) / 1e6
@@ -474,7 +485,7 @@ def psf_published_arm(args):
                        "l2": "flushed between timed steps"},
                       vs_baseline=round(value / (px / (published_ms * 1e-3) / 1e6), 2),
                       baseline={"ms": published_ms, "hardware": "1x A100 (docs/parallelism.md:79)"},
-                      clocks=clk.summary())
+                      rel_err_vs_fp64=acc, accuracy_planes="z[0], z[127]", clocks=clk.summary())
     print(json.dumps(line), flush=True)
 
 
@@ -500,6 +511,18 @@ def microscope_published_arm(args):
                        fft_lengths=args.conv_lengths)
     with ClockSampler(0) as clk:
         ms = _device_timer(torch, dev, args.steps, args.warmup)(lambda: scope(volume, z))
+    acc = None
+    if not args.no_accuracy:
+        # outside the timed region: the same microscope on a 4-plane volume
+        # (z = -4, -4/3, 4/3, 4 um) against the FP64 oracle
+        from oracle import chromatix_oracle as O
+
+        O.set_fft_workers(os.cpu_count())
+        z4 = torch.linspace(-4, 4, 4, dtype=torch.float64, device=dev)
+        img = scope(volume[:4].contiguous(), z4).cpu().numpy()
+        ref, _ = O.microscope_image(np.ones((4,) + shape), shape, spacing, 100.0, np.zeros(shape), 100.0, 1.33, 0.8,
+                                    0.532, z4.cpu().numpy(), reduce_axis=0)
+        acc = float(f"{O.rel_l2(img, np.asarray(ref).reshape(img.shape)):.3g}")
     published = 172.86 if n_z == 128 else None
     line = _base_line(f"ms, Microscope image of a {n_z} x 1536^2 volume (the reference's published benchmark: 128)",
                       round(ms, 3), "ms", args.steps, args.warmup, ms, "c64/f32",
@@ -508,7 +531,7 @@ def microscope_published_arm(args):
                        "conv_lengths": args.conv_lengths},
                       higher_is_better=False, vs_baseline=round(published / ms, 1) if published else None,
                       baseline={"ms": published, "hardware": "1x A100 (docs/parallelism.md:182)"},
-                      clocks=clk.summary())
+                      rel_err_vs_fp64=acc, accuracy_case="the same microscope on 4 planes", clocks=clk.summary())
     print(json.dumps(line), flush=True)
 
 
@@ -532,18 +555,33 @@ def next_rows_arm(args):
     def crand(shape):
         return torch.complex(torch.randn(shape, generator=g, device=dev), torch.randn(shape, generator=g, device=dev))
 
-    def emit(name, ms, nbytes, cfg):
+    def emit(name, ms, nbytes, cfg, err=None):
         achieved = nbytes / (ms * 1e-3) / 1e9
+        extra = {} if err is None else {"rel_err_vs_fp64": float(f"{err:.3g}")}
         line = _base_line(f"ms, {name}", round(ms, 4), "ms", args.steps, args.warmup, ms, "c64/f32",
                           dict(cfg, l2="flushed between timed steps"), higher_is_better=False,
                           roofline={"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
-                                    "frac": round(achieved / peak, 4), "traffic": None, "peak_source": src})
+                                    "frac": round(achieved / peak, 4), "traffic": None, "peak_source": src},
+                          **extra)
         print(json.dumps(line), flush=True)
+
+    check = not args.no_accuracy
+    if check:
+        # errors against the FP64 oracle are computed outside the timed regions
+        from oracle import chromatix_oracle as O
+
+        O.set_fft_workers(os.cpu_count())
 
     u = crand((512, 512, 3))
     f = cx.Field.build(u, 0.3, 0.532)
-    ms = timer(lambda: cf.high_na_ff_lens(f, 100.0, 1.33, 0.8, output_shape=(512, 512), output_dx=0.1))
-    emit("high_na_ff_lens 512^2 vector field", ms, 2 * u.numel() * 8, {"workload": "high_na_ff_lens"})
+    hna = lambda: cf.high_na_ff_lens(f, 100.0, 1.33, 0.8, output_shape=(512, 512), output_dx=0.1)  # noqa: E731
+    ms = timer(hna)
+    err = None
+    if check:
+        ref, _ = O.high_na_ff_lens(u.cpu().numpy().astype(np.complex128), 0.3, 0.532, 100.0, 1.33, 0.8,
+                                   output_shape=(512, 512), output_dx=0.1)
+        err = O.rel_l2(hna().u.cpu().numpy(), ref)
+    emit("high_na_ff_lens 512^2 vector field", ms, 2 * u.numel() * 8, {"workload": "high_na_ff_lens"}, err)
 
     D, N = 64, 256
     fl = torch.rand((D, N, N), generator=g, device=dev)
@@ -551,20 +589,32 @@ def next_rows_arm(args):
     fs = cx.Field.build(crand((N, N)), 0.3, 0.532)
     ms = timer(lambda: cf.fluorescent_multislice_thick_sample(fs, fl, dn, 1.33, 0.5, 64, 7))
     emit("fluorescent multislice 256^2, 64 slices, pad 64", ms, 3 * D * N * N * 4 + N * N * 8,
-         {"workload": "fluorescent_multislice"})
+         {"workload": "fluorescent_multislice",
+          "accuracy": "tests/test_gpu_fluorescence.py (FP64 oracle with the same seeded phases, 2e-5)"})
 
     D2 = 32
     pot = 0.02 * torch.rand((D2, N, N, 3, 3), generator=g, device=dev)
     fv = cx.Field.build(crand((N, N, 3)), 0.2, 0.55)
-    ms = timer(lambda: cf.polarized_multislice_thick_sample(fv, pot, 1.33, 0.5, 1.0))
+    pol = lambda: cf.polarized_multislice_thick_sample(fv, pot, 1.33, 0.5, 1.0)  # noqa: E731
+    ms = timer(pol)
+    err = None
+    if check:
+        ref = O.polarized_multislice_thick_sample(fv.u.cpu().numpy().astype(np.complex128), 0.2, 0.55,
+                                                  pot.cpu().numpy().astype(np.float64), 1.33, 0.5, 1.0)
+        err = O.rel_l2(pol().u.cpu().numpy(), ref)
     emit("polarized multislice 256^2 vector field, 32 slices", ms, pot.numel() * 4 + 2 * N * N * 24,
-         {"workload": "polarized_multislice"})
+         {"workload": "polarized_multislice"}, err)
 
     ur = crand((16, 1024, 1024))
     fr = cx.ScalarField(ur, 0.5, 0.0, cx.MonoSpectrum(0.532))
     abcd = cf.compute_free_space_abcd(30.0) @ cf.compute_thin_spherical_lens_abcd(50.0)
-    ms = timer(lambda: cf.ray_transfer(fr, abcd, 1.0, 1.5))
-    emit("ray_transfer 16 x 1024^2", ms, 2 * ur.numel() * 8, {"workload": "ray_transfer"})
+    ray = lambda: cf.ray_transfer(fr, abcd, 1.0, 1.5)  # noqa: E731
+    ms = timer(ray)
+    err = None
+    if check:
+        ref = O.ray_transfer(O.field_build(ur[0].cpu().numpy().astype(np.complex128), 0.5, 0.532), abcd, 1.0, 1.5).u
+        err = O.rel_l2(ray().u[0].cpu().numpy(), np.asarray(ref).reshape(1024, 1024))
+    emit("ray_transfer 16 x 1024^2", ms, 2 * ur.numel() * 8, {"workload": "ray_transfer", "accuracy": "field 0"}, err)
 
 
 def rescaled_published_arm(args):
@@ -593,6 +643,16 @@ def rescaled_published_arm(args):
 
         ms = _device_timer(torch, dev, args.steps, args.warmup)(step)
         res[name] = {"ms": round(ms, 4), "published_ms": published, "speedup": round(published / ms, 1)}
+        if not args.no_accuracy:
+            # outside the timed region: against the FP64 oracle of the same branch
+            from oracle import chromatix_oracle as O
+
+            O.set_fft_workers(os.cpu_count())
+            of = O.plane_wave((1024, 1024), dxi, lam, pupil=lambda f: O.square_pupil(f, w))
+            ref = O.asm_propagate(of, z, 1, (512, 512), mode="same", bandlimit=True,
+                                  output_dx=np.asarray(of.dx) / 4, shift_yx=(0.0, w / 2), use_czt=use_czt).u
+            out = step().u.cpu().numpy()
+            res[name]["rel_err_vs_fp64"] = float(f"{O.rel_l2(out, np.asarray(ref).reshape(out.shape)):.3g}")
     # the same notebook's high-resolution comparison (cells 10, 19): a 4096^2
     # plane wave at dx / 4 through the same aperture, pad 2048 (an 8192^2
     # transform), band-limited ASM, mode "same"; published 92.4 ms
@@ -609,6 +669,17 @@ def rescaled_published_arm(args):
                                 "hardware": "unstated GPU (notebook output)"},
                       cases=res)
     print(json.dumps(line), flush=True)
+
+
+def _asm_oracle_err(kind, u0, out0):
+    """Relative L2 error of one propagated 512^2 field (pad 256, z 100 um,
+    lambda 0.532, n 1.33, dx 0.3, mode full) against the FP64 oracle."""
+    from oracle import chromatix_oracle as O
+
+    O.set_fft_workers(os.cpu_count())
+    f = O.field_build(u0, 0.3, 0.532)
+    ref = (O.asm_propagate if kind == "asm_propagate" else O.transfer_propagate)(f, 100.0, 1.33, 256).u
+    return float(O.rel_l2(out0, np.asarray(ref).reshape(out0.shape)))
 
 
 def asm_arm(args):
@@ -646,6 +717,10 @@ def asm_arm(args):
             res[key] = {"ms": round(ms, 4), "Mpx_s": round(B * 1024 * 1024 / (ms * 1e-3) / 1e6, 1),
                                        "achieved_GBs": round(alg / (ms * 1e-3) / 1e9, 1),
                                        "frac": round(alg / (ms * 1e-3) / 1e9 / hbm, 4)}
+            if not args.no_accuracy:
+                # outside the timed region: field 0 of the batch against the FP64 oracle
+                out0 = step().u.reshape(B, 1024, 1024)[0].cpu().numpy()
+                res[key]["rel_err_vs_fp64"] = float(f"{_asm_oracle_err(kind, u[0].cpu().numpy(), out0):.3g}")
     main = res["asm_propagate/batch64"]
     line = _base_line("Mpx/s, ASM propagation 512^2 -> 1024^2 (batch 64)", main["Mpx_s"], "Mpx/s", args.steps,
                       args.warmup, main["ms"], "c64 (FP64 phase arguments)",
@@ -654,7 +729,7 @@ def asm_arm(args):
                       roofline={"bound": "hbm", "achieved": main["achieved_GBs"], "peak": hbm, "unit": "GB/s",
                                 "frac": main["frac"], "peak_source": src,
                                 "algorithmic_bytes_per_field": 512 * 512 * 8 + 1024 * 1024 * 8},
-                      cases=res)
+                      rel_err_vs_fp64=main.get("rel_err_vs_fp64"), cases=res)
     print(json.dumps(line), flush=True)
 
 
