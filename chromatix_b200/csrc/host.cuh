@@ -104,6 +104,8 @@ cx_status ensure_twiddles(const float2** table);
 // Device address of length R's matrices (after ensure_twiddles), else null.
 constexpr uint32_t tc_dft_mat_bytes(int R) { return 2u * (uint32_t)(2 * R) * (uint32_t)(2 * R) * 2u; }
 const uint8_t* tc_dft_mats(int R);
+// device counter of tensor-core MMA waits that ran out (cx_tc_timeouts)
+int* tc_timeout_counter();
 
 template <int N>
 __device__ __forceinline__ void load_twiddles(float2* tw, const float2* __restrict__ table, int tid, int nthreads) {

@@ -143,6 +143,7 @@ __global__ void __launch_bounds__(256, 1) k_ms_rows_tc(MsArgs a, const float2* _
     // (NaN) and let the MMAs in flight finish (bounded) before tensor memory
     // is freed
     tc::mbar_wait(S.bar, phase ^ 1u, F::POLLS);
+    tc_note_timeout(mats);
     const float nan = __int_as_float(0x7fc00000);
     for (long u = t; u < tiles; u += gridDim.x) {
       const int y0 = r0 + (int)u * 8;

@@ -101,6 +101,7 @@ __global__ void __launch_bounds__(256, 1) k_prop_cols_tc(const float2* T, float2
     // an MMA wait ran out: mark this CTA's unfinished output tiles invalid
     // (NaN) and let the MMAs in flight finish (bounded) before freeing tensor memory
     tc::mbar_wait(S.bar, phase ^ 1u, F::POLLS);
+    tc_note_timeout(mats);
     const float nan = __int_as_float(0x7fc00000);
     for (; t < total; t += gridDim.x) {
       const int q = (int)(t / tiles_x), x0 = (int)(t % tiles_x) * 8;
@@ -244,6 +245,7 @@ __global__ void __launch_bounds__(256, 1) k_prop_rows_tc(const float2* in, float
       // an MMA wait ran out: mark this CTA's remaining rows invalid (NaN) and
       // let the MMAs in flight finish (bounded) before tensor memory is freed
       tc::mbar_wait(S.bar, phase ^ 1u, F::POLLS);
+      tc_note_timeout(mats);
       const float nan = __int_as_float(0x7fc00000);
       for (long u = t; u < tiles; u += gridDim.x) {
         for (int idx = tid; idx < 8 * N; idx += blockDim.x) {

@@ -93,6 +93,7 @@ __global__ void __launch_bounds__(256, 1) k_psf_cols_tc(PsfArgs a, const float2*
     // an MMA wait ran out: mark this CTA's remaining output as invalid (NaN),
     // let the MMAs in flight finish (bounded) before the tensor memory is freed
     tc::mbar_wait(S.bar, phase ^ 1u, F::POLLS);
+    tc_note_timeout(mats);
     for (long t = blockIdx.x; t < total; t += gridDim.x) {
       const int zl = (int)(t / tiles_x), x0 = (int)(t % tiles_x) * 8;
       float* outz = a.out + (size_t)(a.z0 + zl) * a.ny * a.nx;
@@ -224,6 +225,7 @@ __global__ void __launch_bounds__(256, 1) k_psf_rows_tc(PsfArgs a, const float2*
       // (NaN; the column pass carries them into the intensity) and let the
       // MMAs in flight finish (bounded) before tensor memory is freed
       tc::mbar_wait(S.bar, phase ^ 1u, F::POLLS);
+      tc_note_timeout(mats);
       const float nan = __int_as_float(0x7fc00000);
       for (long u = t; u < tiles; u += gridDim.x)
         for (int idx = tid; idx < 8 * N; idx += blockDim.x) {

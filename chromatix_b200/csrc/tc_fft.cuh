@@ -63,11 +63,13 @@ struct TcFft {
 struct TcMats {
   const uint8_t* b1;
   const uint8_t* b2;
+  int* timeouts;  // bumped once per CTA whose MMA wait ran out (cx_tc_timeouts)
 };
 inline cx_status tc_mats(int n1, int n2, TcMats* m) {
   m->b1 = tc_dft_mats(n1);
   m->b2 = tc_dft_mats(n2);
-  if (!m->b1 || !m->b2) {
+  m->timeouts = tc_timeout_counter();
+  if (!m->b1 || !m->b2 || !m->timeouts) {
     set_error("tensor-core DFT matrices of lengths %d / %d are not on the device (cx_init)", n1, n2);
     return CX_ERR_CUDA;
   }
@@ -99,6 +101,11 @@ __device__ void tc_fft_build_b(uint8_t* B, bool inverse, int tid, int nthreads) 
     *reinterpret_cast<__half*>(B + tc::off_kmajor(K, j, k)) = h;
     *reinterpret_cast<__half*>(B + K * K * 2 + tc::off_kmajor(K, j, k)) = l;
   }
+}
+
+// a CTA gave up on an MMA wait: count it once for the host (cx_tc_timeouts)
+__device__ __forceinline__ void tc_note_timeout(const TcMats& m) {
+  if (threadIdx.x == 0) atomicAdd(m.timeouts, 1);
 }
 
 // copy the prebuilt DFT matrices (tc_dft_mats: hi then lo, `bytes` in all)

@@ -20,6 +20,14 @@ constexpr int kTcLens[] = {32, 40};
 constexpr uint32_t kTcMatTotal = tc_dft_mat_bytes(32) + tc_dft_mat_bytes(40);
 static __device__ uint4 g_tc_mats[kTcMatTotal / 16];
 static const uint8_t* g_tc_addr[64] = {nullptr};
+static __device__ int g_tc_timeouts;
+static int* g_tc_timeouts_addr[64] = {nullptr};
+
+int* tc_timeout_counter() {
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return nullptr;
+  return g_tc_timeouts_addr[dev];
+}
 
 // row j = output (re | im), column k = input (re | im) of the length-R DFT
 // exp(-2 pi i n k / R), as tc_fft_build_b lays it out on the device
@@ -93,6 +101,9 @@ cx_status ensure_twiddles(const float2** table) {
   void* q = nullptr;
   CX_CUDA_TRY(cudaGetSymbolAddress(&q, g_tc_mats));
   g_tc_addr[dev] = static_cast<const uint8_t*>(q);
+  void* c = nullptr;
+  CX_CUDA_TRY(cudaGetSymbolAddress(&c, g_tc_timeouts));
+  g_tc_timeouts_addr[dev] = static_cast<int*>(c);
   void* p = nullptr;
   CX_CUDA_TRY(cudaGetSymbolAddress(&p, g_twiddles));
   addr[dev] = static_cast<const float2*>(p);
@@ -103,3 +114,20 @@ cx_status ensure_twiddles(const float2** table) {
 }  // namespace cx
 
 extern "C" cx_status cx_init(void) { return cx::ensure_twiddles(nullptr); }
+
+extern "C" cx_status cx_tc_timeouts(int32_t* count, int32_t reset) {
+  if (!count) {
+    cx::set_error("null count pointer");
+    return CX_ERR_INVALID;
+  }
+  cx_status s = cx::ensure_twiddles(nullptr);
+  if (s != CX_OK) return s;
+  int v = 0;
+  CX_CUDA_TRY(cudaMemcpyFromSymbol(&v, cx::g_tc_timeouts, sizeof(int)));
+  *count = v;
+  if (reset) {
+    const int zero = 0;
+    CX_CUDA_TRY(cudaMemcpyToSymbol(cx::g_tc_timeouts, &zero, sizeof(int)));
+  }
+  return CX_OK;
+}

@@ -609,6 +609,12 @@ cx_status cx_pupil(const cx_ew_desc* d, int32_t kind, const double* wv_params_de
 cx_status cx_dft_split16(const void* x, void* y, int32_t R, int64_t batch, int32_t inverse, int32_t* status_dev,
                          cx_stream_t stream);
 
+/* Number of CTAs of the CX_PREC_SPLIT16 PSF / propagation / multislice
+ * kernels that gave up waiting for a tensor-core MMA on the current device
+ * since the last reset (their output tiles are then NaN).  Synchronises the
+ * device; reset != 0 clears the count after reading it. */
+cx_status cx_tc_timeouts(int32_t* count, int32_t reset);
+
 /* ---------------------------------------------------------------------------
  * misc
  * ------------------------------------------------------------------------- */

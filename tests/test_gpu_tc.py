@@ -190,3 +190,30 @@ def test_split16_multislice_1024_forward_and_gradient():
     assert e_fwd < 5e-5, (e_fwd, e_grad)
     assert abs(float(loss) - L64) / L64 < 1e-4
     assert e_grad < 5e-4, (e_fwd, e_grad)
+
+
+def test_no_tensor_core_wait_ran_out():
+    """After the split-precision runs of this module (and one more PSF here),
+    no CTA gave up on an MMA wait: the device counter cx_tc_timeouts reads 0,
+    and a reset leaves it at 0."""
+    import ctypes as C
+
+    import torch
+
+    import chromatix_b200 as cx
+    import chromatix_b200.functional as cf
+    from chromatix_b200 import _native as nat
+
+    L = nat.lib()
+    L.cx_tc_timeouts.restype = C.c_int32
+    L.cx_tc_timeouts.argtypes = [C.POINTER(C.c_int32), C.c_int32]
+    with cx.precision("split16"):
+        f = cf.objective_point_source((1024, 1024), 0.25, 0.532, np.array([0.0, 2.0]), 8000.0, 1.33, 0.6)
+        I = cf.ff_lens(f, 200000.0, 1.33).intensity
+    torch.cuda.synchronize()
+    assert torch.isfinite(I).all()
+    n = C.c_int32(-1)
+    assert L.cx_tc_timeouts(C.byref(n), 1) == 0
+    assert n.value == 0
+    assert L.cx_tc_timeouts(C.byref(n), 0) == 0
+    assert n.value == 0
