@@ -281,7 +281,10 @@ def gpu_arm(args):
                            parallelism=f"replicas x{world}" if world > 1 else "single GPU"),
             "e2e": {"value": round(e2e_value, 1), "unit": UNIT, "ms_per_step": round(ms_e2e, 4),
                     "h2d_bytes_per_step": int(phase.nbytes + z.nbytes),
-                    "d2h_bytes_per_step": int(NZ * N * N * 4)},
+                    "d2h_bytes_per_step": int(NZ * N * N * 4),
+                    # the intensity stack's device->host copy (overlapped with the transforms) bounds it
+                    "bound": "pcie", "host_link_GBs": round((NZ * N * N * 4 + phase.nbytes + z.nbytes)
+                                                            / (ms_e2e * 1e-3) / 1e9, 1)},
             "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": hbm, "unit": "GB/s",
                          "frac": round(achieved / hbm, 4), "traffic": traffic if best == "accurate" else None,
                          "kernel": ("k_psf_cols<1280> (column FFT + spectral intensity)" if best == "accurate" else
