@@ -749,7 +749,7 @@ def multislice_arm(args):
     import chromatix_b200 as cx
 
     dev = torch.device("cuda", 0)
-    D, N, dz, lam = 256, 1024, 0.2, 0.532
+    D, N, dz, lam = args.ms_slices, 1024, 0.2, 0.532
     g = torch.Generator(device=dev)
     g.manual_seed(0)
     dn = torch.randn((D, N, N), generator=g, device=dev) * 0.02
@@ -818,9 +818,10 @@ def multislice_arm(args):
     r = forms[best]
     line = _base_line("Mpx-slices/s, multislice forward + adjoint gradient", r["Mpx_slices_s"], "Mpx-slices/s",
                       args.steps, args.warmup, r["ms"],
-                      "c64/f32 (FP64 propagator" + ("; column transforms as FP16 hi+lo tensor-core DFT "
-                                                    "contractions, FP32 accumulation)" if best == "split16" else ")"),
-                      {"workload": "multislice 256 x 1024^2, dz 0.2, dx 0.1, lambda 0.532, n 1.33, plane wave, L2 "
+                      "c64/f32 (FP64 propagator" + ("; row and column transforms as FP16 hi+lo tensor-core "
+                                                    "DFT contractions, FP32 accumulation)" if best == "split16"
+                                                    else ")"),
+                      {"workload": f"multislice {D} x 1024^2, dz 0.2, dx 0.1, lambda 0.532, n 1.33, plane wave, L2 "
                                    "loss, grad w.r.t. dn, checkpoint every 16", "l2": "inputs larger than L2"},
                       transform_form=best,
                       roofline={"bound": "hbm", "achieved": round(alg / (r["ms"] * 1e-3) / 1e9, 1), "peak": hbm,
@@ -1171,6 +1172,8 @@ def main():
     ap.add_argument("--micro-planes", type=int, default=128, help="microscope_published: planes (published: 128)")
     ap.add_argument("--conv-lengths", default="smallest", choices=["smallest", "pow2"],
                     help="microscope_published: convolution transform lengths (same image either way)")
+    ap.add_argument("--ms-slices", type=int, default=256,
+                    help="multislice: slices (256 in the benchmark configuration; fewer for profiling captures)")
     ap.add_argument("--mbs-maxiter", type=int, default=4000)
     ap.add_argument("--mbs-side", type=int, default=256, help="mbs: interior grid side (+64 boundary voxels)")
     ap.add_argument("--rate", type=float, default=2000.0, help="serve: mean arrivals per second")
