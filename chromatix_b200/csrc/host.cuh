@@ -5,7 +5,6 @@
 
 #include <cstdarg>
 #include <cstdio>
-#include <cstdlib>
 #include <utility>
 
 #include "../../include/cx_b200.h"
@@ -298,15 +297,6 @@ inline int persistent_grid(K kernel, int threads, size_t smem, long work_items_c
 // the previous kernel in the stream drains; it waits for it with pdl_wait()
 // (common.cuh) before touching shared buffers.  Grids are persistent (every
 // CTA resident), so waiting dependents cannot starve the previous grid.
-// CX_PDL=0 in the environment launches these kernels plainly (stream order)
-inline bool pdl_enabled() {
-  static const bool on = [] {
-    const char* e = std::getenv("CX_PDL");
-    return !(e && e[0] == '0');
-  }();
-  return on;
-}
-
 template <class... P, class... A>
 inline cudaError_t launch_pdl(void (*kernel)(P...), int grid, int threads, size_t smem, cudaStream_t st,
                               A&&... args) {
@@ -319,7 +309,7 @@ inline cudaError_t launch_pdl(void (*kernel)(P...), int grid, int threads, size_
   attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
   attr[0].val.programmaticStreamSerializationAllowed = 1;
   cfg.attrs = attr;
-  cfg.numAttrs = pdl_enabled() ? 1 : 0;
+  cfg.numAttrs = 1;
   return cudaLaunchKernelEx(&cfg, kernel, std::forward<A>(args)...);
 }
 
