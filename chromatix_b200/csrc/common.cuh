@@ -93,14 +93,6 @@ __device__ __forceinline__ void bulk_copy_g2s(void* smem, const void* gmem, unsi
                "l"(gmem), "r"(bytes), "r"(b)
                : "memory");
 }
-// Programmatic dependent launch (kernels launched with launch_pdl): the
-// kernel's prologue (twiddle tables, barriers) may overlap the previous
-// kernel's tail; pdl_wait() blocks until the previous grid has completed and
-// its writes are visible, so it must precede every access to memory another
-// kernel writes or reads.  pdl_trigger() lets the next kernel launch.
-__device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;\n" ::: "memory"); }
-__device__ __forceinline__ void pdl_trigger() { asm volatile("griddepcontrol.launch_dependents;\n" ::: "memory"); }
-
 // L2 policy for data read or written once per pass (slice rows, records):
 // evicted first, so that the state that every pass reuses stays in L2
 __device__ __forceinline__ uint64_t l2_evict_first() {

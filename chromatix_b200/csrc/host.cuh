@@ -5,7 +5,6 @@
 
 #include <cstdarg>
 #include <cstdio>
-#include <utility>
 
 #include "../../include/cx_b200.h"
 #include "fft_engine.cuh"
@@ -291,26 +290,6 @@ inline int persistent_grid(K kernel, int threads, size_t smem, long work_items_c
   if (work_items_ctas < g) g = work_items_ctas;
   if (g < 1) g = 1;
   return (int)g;
-}
-
-// Launch with programmatic stream serialisation: the kernel may begin while
-// the previous kernel in the stream drains; it waits for it with pdl_wait()
-// (common.cuh) before touching shared buffers.  Grids are persistent (every
-// CTA resident), so waiting dependents cannot starve the previous grid.
-template <class... P, class... A>
-inline cudaError_t launch_pdl(void (*kernel)(P...), int grid, int threads, size_t smem, cudaStream_t st,
-                              A&&... args) {
-  cudaLaunchConfig_t cfg = {};
-  cfg.gridDim = dim3((unsigned)grid);
-  cfg.blockDim = dim3((unsigned)threads);
-  cfg.dynamicSmemBytes = smem;
-  cfg.stream = st;
-  cudaLaunchAttribute attr[1];
-  attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
-  attr[0].val.programmaticStreamSerializationAllowed = 1;
-  cfg.attrs = attr;
-  cfg.numAttrs = 1;
-  return cudaLaunchKernelEx(&cfg, kernel, std::forward<A>(args)...);
 }
 
 template <class K>

@@ -143,8 +143,6 @@ __global__ void __launch_bounds__(RowCfg<NX>::THREADS, RowCfg<NX>::MINB) k_ms_ro
     __syncthreads();
   }
   unsigned bphase = 0;  // parity of this team's next prefetch completion
-  pdl_wait();  // the previous pass's writes to the state (and the records) are complete
-  pdl_trigger();
   // MS_FINAL only produces the cropped rows
   const int r0 = MODE == MS_FINAL ? a.pad_y : 0;
   const int nrows = MODE == MS_FINAL ? a.ny : a.py;

@@ -11,7 +11,7 @@ static cx_status launch_ms_rows_mode(const MsArgs& a, cudaStream_t st) {
   CX_CUDA_TRY(set_smem(k, SMEM));
   const long rows = a.mode == MS_FINAL ? a.ny : a.py;
   const long items = (rows + C::TEAMS - 1) / C::TEAMS;
-  CX_CUDA_TRY(launch_pdl(k, persistent_grid(k, C::THREADS, SMEM, items), C::THREADS, SMEM, st, a));
+  k<<<persistent_grid(k, C::THREADS, SMEM, items), C::THREADS, SMEM, st>>>(a);
   CX_LAUNCH_CHECK();
   return CX_OK;
 }

@@ -287,8 +287,6 @@ __global__ void __launch_bounds__(RowCfg<NX>::THREADS, RowCfg<NX>::MINB) k_prop_
   float2* tw = sm;
   load_twiddles<NX>(tw, a.twg, threadIdx.x, blockDim.x);
   __syncthreads();
-  pdl_wait();
-  pdl_trigger();
   const int team = threadIdx.x / C::LPV, lane = threadIdx.x % C::LPV;
   float2* s = sm + C::TW + team * Plan<NX>::LEN;
   const long total = (long)a.n_in_planes * a.ny;
@@ -324,8 +322,6 @@ __global__ void __launch_bounds__(ColCfg<NY>::THREADS, ColCfg<NY>::MINB) k_prop_
   float2* tw = sm;
   float2* tile = sm + C::TW;
   load_twiddles<NY>(tw, a.twg, threadIdx.x, blockDim.x);
-  pdl_wait();
-  pdl_trigger();
   const int team = threadIdx.x / C::LPV, lane = threadIdx.x % C::LPV;
   float2* s = tile + team * LEN;
   const int tiles_x = (a.px + V - 1) / V;
@@ -372,8 +368,6 @@ __global__ void __launch_bounds__(RowCfg<NX>::THREADS, RowCfg<NX>::MINB) k_prop_
   float2* tw = sm;
   load_twiddles<NX>(tw, a.twg, threadIdx.x, blockDim.x);
   __syncthreads();
-  pdl_wait();
-  pdl_trigger();
   const int team = threadIdx.x / C::LPV, lane = threadIdx.x % C::LPV;
   float2* s = sm + C::TW + team * Plan<NX>::LEN;
   const long total = (long)a.n_out_planes * a.out_ny;

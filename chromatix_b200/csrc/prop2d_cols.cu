@@ -10,7 +10,7 @@ static cx_status launch_cols(const float2* T, float2* T2, const Prop2DArgs& a, c
   CX_CUDA_TRY(set_smem(k, C::SMEM));
   const long items = (long)((a.px + C::V - 1) / C::V) * a.n_out_planes;
   const int grid = persistent_grid(k, C::THREADS, C::SMEM, items);
-  CX_CUDA_TRY(launch_pdl(k, grid, C::THREADS, C::SMEM, st, T, T2, a));
+  k<<<grid, C::THREADS, C::SMEM, st>>>(T, T2, a);
   CX_LAUNCH_CHECK();
   return CX_OK;
 }

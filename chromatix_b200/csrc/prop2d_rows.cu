@@ -10,7 +10,7 @@ static cx_status launch_rows_fwd(const float2* u, float2* T, const Prop2DArgs& a
   CX_CUDA_TRY(set_smem(k, C::SMEM));
   const long items = ((long)a.n_in_planes * a.ny + C::TEAMS - 1) / C::TEAMS;
   const int grid = persistent_grid(k, C::THREADS, C::SMEM, items);
-  CX_CUDA_TRY(launch_pdl(k, grid, C::THREADS, C::SMEM, st, u, T, a));
+  k<<<grid, C::THREADS, C::SMEM, st>>>(u, T, a);
   CX_LAUNCH_CHECK();
   return CX_OK;
 }
@@ -22,7 +22,7 @@ static cx_status launch_rows_inv(const float2* T2, float2* out, const Prop2DArgs
   CX_CUDA_TRY(set_smem(k, C::SMEM));
   const long items = ((long)a.n_out_planes * a.out_ny + C::TEAMS - 1) / C::TEAMS;
   const int grid = persistent_grid(k, C::THREADS, C::SMEM, items);
-  CX_CUDA_TRY(launch_pdl(k, grid, C::THREADS, C::SMEM, st, T2, out, a));
+  k<<<grid, C::THREADS, C::SMEM, st>>>(T2, out, a);
   CX_LAUNCH_CHECK();
   return CX_OK;
 }

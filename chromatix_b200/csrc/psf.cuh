@@ -126,8 +126,6 @@ __global__ void __launch_bounds__(PsfRowCfg<NX>::THREADS, PsfRowCfg<NX>::MINB) k
   float2* tw = sm;
   load_twiddles<NX>(tw, a.twg, threadIdx.x, blockDim.x);
   __syncthreads();
-  pdl_wait();
-  pdl_trigger();
   const int team = threadIdx.x / C::LPV, lane = threadIdx.x % C::LPV;
   float2* s = sm + C::TW + team * Plan<NX>::LEN;
   const long total = (long)a.zc * a.rowsum;
@@ -250,8 +248,6 @@ __global__ void __launch_bounds__(ColCfg<NY>::THREADS, ColCfg<NY>::MINB) k_psf_c
   const int team = threadIdx.x / C::LPV, lane = threadIdx.x % C::LPV;
   float2* s = tile + team * LEN;
   float* acc = accs + team * ACC;
-  pdl_wait();
-  pdl_trigger();
   const int tiles_x = (a.nx + V - 1) / V;
   const long total = (long)tiles_x * a.zc;
   for (long t = blockIdx.x; t < total; t += gridDim.x) {

@@ -11,7 +11,7 @@ static cx_status launch_psf_cols(const PsfArgs& a, cudaStream_t st) {
   CX_CUDA_TRY(set_smem(k, PsfColCfg<NY>::SMEM));
   const long items = (long)((a.nx + C::V - 1) / C::V) * a.zc;
   const int grid = persistent_grid(k, C::THREADS, PsfColCfg<NY>::SMEM, items);
-  CX_CUDA_TRY(launch_pdl(k, grid, C::THREADS, PsfColCfg<NY>::SMEM, st, a));
+  k<<<grid, C::THREADS, PsfColCfg<NY>::SMEM, st>>>(a);
   CX_LAUNCH_CHECK();
   return CX_OK;
 }

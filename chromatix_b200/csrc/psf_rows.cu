@@ -15,7 +15,7 @@ static cx_status launch_psf_rows(const PsfArgs& a, cudaStream_t st) {
                       : k_psf_rows_tab<NX, 0>;
     CX_CUDA_TRY(set_smem(k, C::SMEM));
     const int grid = persistent_grid(k, C::THREADS, C::SMEM, (rows + C::TEAMS - 1) / C::TEAMS);
-    CX_CUDA_TRY(launch_pdl(k, grid, C::THREADS, C::SMEM, st, a));
+    k<<<grid, C::THREADS, C::SMEM, st>>>(a);
   } else {
     using C = RowCfg<NX>;
     auto k = k_psf_rows<NX>;
