@@ -189,7 +189,8 @@ __device__ __forceinline__ float2 prop_kernel(int ky, int kx, const Prop2DArgs& 
 // K = 2 pi |z| n / lambda, (lambda / n)^2 and the Fresnel phase factor.
 struct PropK {
   double iy, ix, K, q2, tz;
-  int fast;  // the short-distance FP32 branch of prop_kernel_accurate applies
+  int fast;     // the short-distance FP32 branch of prop_kernel_accurate applies
+  int shifted;  // the plane has a nonzero output shift (linear phase term)
 };
 
 __device__ __forceinline__ PropK prop_consts(const Prop2DArgs& a, const cx_plane& pl) {
@@ -205,11 +206,29 @@ __device__ __forceinline__ PropK prop_consts(const Prop2DArgs& a, const cx_plane
             pl.shift_x == 0.0)
                ? 1
                : 0;
+  c.shifted = (pl.shift_y != 0.0 || pl.shift_x != 0.0) ? 1 : 0;
   return c;
 }
 
+// sqrt(x) for 0 <= x <= 1 to FP64 accuracy from the FP32 hardware estimate
+// and one Newton-Raphson (Heron) step in FP64:
+//   s0 = x_f rsqrt(x_f),  s1 = s0 + (x - s0^2) / (2 s0),
+// with 1 / s0 taken from the same FP32 reciprocal square root.  s0 carries
+// a relative error e ~ 1e-7, so s1 is within ~e^2 + e * |x - s0^2| / s0 ~ 1e-14
+// of sqrt(x) relatively (the ASM phase K sqrt(.) with K <= 1e5 rad then stays
+// within 1e-9 rad).  x below the smallest normal float gives 0 (its root,
+// < 1e-19, times K is far below the phase budget).
+__device__ __forceinline__ double sqrt_unit_f64(double x) {
+  const float xf = (float)x;
+  if (!(xf > 0.f)) return 0.0;
+  const float r = rsqrtf(xf);
+  const double s0 = (double)(xf * r);
+  return fma(fma(-s0, s0, x), 0.5 * (double)r, s0);
+}
+
 // prop_kernel_accurate for the transfer and ASM kinds with the per-plane
-// constants hoisted (same branches and operation order otherwise)
+// constants hoisted (same branches and operation order otherwise; the FP64
+// square root by sqrt_unit_f64)
 __device__ __forceinline__ float2 prop_kernel_accurate_k(int ky, int kx, const Prop2DArgs& a, const cx_plane& pl,
                                                          const PropK& c) {
   const double pi = 3.141592653589793238462643383279502884;
@@ -242,12 +261,12 @@ __device__ __forceinline__ float2 prop_kernel_accurate_k(int ky, int kx, const P
   }
   if (a.bandlimit && (fabs(fy - pl.bl_y0) > pl.bl_hy || fabs(fx - pl.bl_x0) > pl.bl_hx)) return make_float2(0.f, 0.f);
   const double kern = 1.0 - c.q2 * s;
-  const double sh = 2.0 * pi * (fy * pl.shift_y + fx * pl.shift_x);
+  const double sh = c.shifted ? 2.0 * pi * (fy * pl.shift_y + fx * pl.shift_x) : 0.0;
   double amp = 1.0, ph;
   if (kern >= 0.0 || a.remove_evanescent) {
-    ph = c.K * sqrt(kern > 0.0 ? kern : 0.0) + sh;
+    ph = c.K * sqrt_unit_f64(kern) + sh;
   } else {
-    amp = exp(-c.K * sqrt(-kern));
+    amp = exp(-c.K * sqrt_unit_f64(-kern));
     ph = sh;
   }
   if (pl.z < 0.0) ph = -ph;
