@@ -295,6 +295,74 @@ __device__ __forceinline__ float2 prop_kernel_k(int ky, int kx, const Prop2DArgs
   return a.conj_h ? cconj(h) : h;
 }
 
+// The propagator along one column kx, specialised once per tile: the
+// accurate ASM (long-distance FP64 phase, or the short-distance FP32 branch)
+// and transfer kernels without NA mask or band limit take a branch-light
+// path with the column's (f_x - k_x0)^2 formed once and the conjugations
+// (z < 0, conj_h) folded into one sign; everything else goes through
+// prop_kernel_k.  Values equal prop_kernel_k's up to the rounding of the
+// re-associated sums.
+struct PropCol {
+  int mode;    // 0 generic, 1 ASM (FP64 phase), 2 transfer, 3 ASM short-distance branch, 4 table
+  float sgn;   // sign of the phase (z < 0 and conj_h each flip it; transfer: conj_h only)
+  double fx, gx2;
+};
+
+__device__ __forceinline__ PropCol prop_col(const Prop2DArgs& a, const cx_plane& pl, const PropK& c, int kx) {
+  PropCol pc;
+  pc.fx = (double)freq_index(kx, a.px) * c.ix;
+  const double gx = pc.fx - a.kx0;
+  pc.gx2 = gx * gx;
+  const bool plain = a.precision == CX_PREC_ACCURATE && !a.precise && a.na_f2 < 0.0 && a.kernel != CX_KERNEL_EXPLICIT;
+  pc.mode = (a.kernel == CX_KERNEL_EXPLICIT && a.na_f2 < 0.0) ? 4 : 0;
+  if (plain && a.kernel == CX_KERNEL_TRANSFER) pc.mode = 2;
+  if (plain && a.kernel == CX_KERNEL_ASM && !a.bandlimit) pc.mode = c.fast ? 3 : 1;
+  const float cj = a.conj_h ? -1.f : 1.f;
+  pc.sgn = (pc.mode == 2 || pc.mode == 4) ? cj : (pl.z < 0.0 ? -cj : cj);
+  return pc;
+}
+
+__device__ __forceinline__ float2 prop_col_h(int ky, int kx, const PropCol& pc, const Prop2DArgs& a,
+                                             const cx_plane& pl, const PropK& c) {
+  const double pi = 3.141592653589793238462643383279502884;
+  const double fy = (double)freq_index(ky, a.py) * c.iy;
+  const double gy = fy - a.ky0;
+  switch (pc.mode) {
+    case 1: {
+      const double kern = 1.0 - c.q2 * (gy * gy + pc.gx2);
+      const double sh = c.shifted ? 2.0 * pi * (fy * pl.shift_y + pc.fx * pl.shift_x) : 0.0;
+      double amp = 1.0, ph = sh;
+      if (kern >= 0.0 || a.remove_evanescent)
+        ph += c.K * sqrt_unit_f64(kern);
+      else
+        amp = exp(-c.K * sqrt_unit_f64(-kern));
+      const float2 e = expi_reduced(ph);
+      return make_float2((float)amp * e.x, (float)amp * pc.sgn * e.y);
+    }
+    case 2: {
+      const float2 e = expi_reduced(c.tz * (gy * gy + pc.gx2));
+      return make_float2(e.x, pc.sgn * e.y);
+    }
+    case 3: {
+      const float kern = (float)(1.0 - c.q2 * (gy * gy + pc.gx2));
+      float amp = 1.f, ph = 0.f;
+      if (kern >= 0.f || a.remove_evanescent)
+        ph = (float)c.K * sqrtf(fmaxf(kern, 0.f));
+      else
+        amp = __expf(-(float)c.K * sqrtf(-kern));
+      float sn, cs;
+      __sincosf(ph - 6.2831853071795865f * rintf(ph * 0.15915494309189534f), &sn, &cs);
+      return make_float2(amp * cs, amp * pc.sgn * sn);
+    }
+    case 4: {
+      const float2 h = a.H[((size_t)pl.h_plane * a.py + ky) * a.px + kx];
+      return make_float2(h.x, pc.sgn * h.y);
+    }
+    default:
+      return prop_kernel_k(ky, kx, a, pl, c);
+  }
+}
+
 // --------------------------------------------------------------------------
 // pass A: forward row FFT with zero padding in the loader
 // --------------------------------------------------------------------------
@@ -359,10 +427,11 @@ __global__ void __launch_bounds__(ColCfg<NY>::THREADS, ColCfg<NY>::MINB) k_prop_
     __syncthreads();
     const int kx = x0 + team;
     const bool valid = kx < a.px;
+    const PropCol pc = prop_col(a, pl, kc, kx);
     auto load1 = [&](int n) -> float2 {
       return (n >= a.pad_y && n < a.pad_y + a.ny) ? s[pad_idx(n)] : make_float2(0.f, 0.f);
     };
-    auto store1 = [&](int k, float2 v, int) { s[pad_idx(k)] = valid ? cmul(v, prop_kernel_k(k, kx, a, pl, kc)) : v; };
+    auto store1 = [&](int k, float2 v, int) { s[pad_idx(k)] = valid ? cmul(v, prop_col_h(k, kx, pc, a, pl, kc)) : v; };
     team_fft_ex<NY, false, false, true, C::LPV, C::CTA>(s, tw, lane, team, load1, store1);
     team_barrier<C::LPV, C::CTA>(team);
     auto load2 = [&](int n) -> float2 { return s[pad_idx(n)]; };
