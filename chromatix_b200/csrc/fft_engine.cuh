@@ -528,6 +528,20 @@ __host__ __device__ constexpr unsigned edge_zero_mask() {
   return m;
 }
 
+// First-stage zero mask for an input that is nonzero only on the central
+// band [N / 4, 3 N / 4) (a field zero-padded to twice its size on both
+// sides): with a first radix R_0 divisible by 4, the inputs j + r N / R_0 with
+// r < R_0 / 4 or r >= 3 R_0 / 4 are zero.  0 (no mask) otherwise.
+template <int N>
+__host__ __device__ constexpr unsigned center_band_mask() {
+  constexpr int R0 = Plan<N>::P.r[0];
+  unsigned m = 0u;
+  if (R0 % 4 == 0)
+    for (int r = 0; r < R0; ++r)
+      if (r < R0 / 4 || r >= 3 * R0 / 4) m |= 1u << r;
+  return m;
+}
+
 // First-stage zero mask for an input that is nonzero only on [0, N / 2)
 // (zero padding to twice the length): with an even first radix R_0 the
 // inputs r >= R_0 / 2 of every first-stage butterfly (indices
@@ -548,8 +562,8 @@ __host__ __device__ constexpr unsigned lower_half_mask() {
 // functor's code once: for heavy functors (FP64 phase evaluation, sin/cos,
 // transmittances) this keeps the kernel within the instruction cache.
 // Staged store functors receive slot = 0.
-template <int N, bool INV, bool STAGE_LOAD, bool STAGE_STORE, int LPV = Plan<N>::LPV, bool CTA = false, class Load,
-          class Store>
+template <int N, bool INV, bool STAGE_LOAD, bool STAGE_STORE, int LPV = Plan<N>::LPV, bool CTA = false,
+          unsigned ZM = 0u, class Load, class Store>
 __device__ __forceinline__ void team_fft_ex(float2* s, const float2* tw, int lane, int team, Load& load,
                                             Store& store) {
   auto sld = [&](int n) -> float2 { return s[pad_idx(n)]; };
@@ -565,10 +579,11 @@ __device__ __forceinline__ void team_fft_ex(float2* s, const float2* tw, int lan
       Stage<N, LPV, INV, 0, 1, CTA>::run(s, tw, lane, team, sld, store);
     }
   } else {
+    // ZM (first-stage zero mask) applies to the caller's loads only
     if constexpr (STAGE_STORE) {
-      Stage<N, LPV, INV, 0, 1, CTA>::run(s, tw, lane, team, load, sst);
+      Stage<N, LPV, INV, 0, 1, CTA, ZM>::run(s, tw, lane, team, load, sst);
     } else {
-      Stage<N, LPV, INV, 0, 1, CTA>::run(s, tw, lane, team, load, store);
+      Stage<N, LPV, INV, 0, 1, CTA, ZM>::run(s, tw, lane, team, load, store);
     }
   }
   if constexpr (STAGE_STORE) {

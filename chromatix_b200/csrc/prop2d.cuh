@@ -366,7 +366,9 @@ __device__ __forceinline__ float2 prop_col_h(int ky, int kx, const PropCol& pc, 
 // --------------------------------------------------------------------------
 // pass A: forward row FFT with zero padding in the loader
 // --------------------------------------------------------------------------
-template <int NX>
+// BAND: the data columns lie in [NX / 4, 3 NX / 4) (checked on the host), so
+// the first stage skips the zero padding outside that band (center_band_mask)
+template <int NX, bool BAND = false>
 __global__ void __launch_bounds__(RowCfg<NX>::THREADS, RowCfg<NX>::MINB) k_prop_rows_fwd(const float2* __restrict__ u,
                                                                       float2* __restrict__ T, Prop2DArgs a) {
   using C = RowCfg<NX>;
@@ -393,14 +395,16 @@ __global__ void __launch_bounds__(RowCfg<NX>::THREADS, RowCfg<NX>::MINB) k_prop_
     auto store = [&](int k, float2 v, int) {
       if (valid) dst[k] = v;
     };
-    team_fft<NX, false>(s, tw, lane, team, load, store);
+    team_fft<NX, false, Plan<NX>::LPV, false, (BAND ? center_band_mask<NX>() : 0u)>(s, tw, lane, team, load, store);
   }
 }
 
 // --------------------------------------------------------------------------
 // pass B: column FFT -> x H -> column IFFT on V-column tiles
 // --------------------------------------------------------------------------
-template <int NY>
+// BAND: the data rows lie in [NY / 4, 3 NY / 4) of the padded column (checked
+// on the host), so the forward transform's first stage skips the padding
+template <int NY, bool BAND = false>
 __global__ void __launch_bounds__(ColCfg<NY>::THREADS, ColCfg<NY>::MINB) k_prop_cols(const float2* __restrict__ T,
                                                                   float2* __restrict__ T2, Prop2DArgs a) {
   using C = ColCfg<NY>;
@@ -432,7 +436,8 @@ __global__ void __launch_bounds__(ColCfg<NY>::THREADS, ColCfg<NY>::MINB) k_prop_
       return (n >= a.pad_y && n < a.pad_y + a.ny) ? s[pad_idx(n)] : make_float2(0.f, 0.f);
     };
     auto store1 = [&](int k, float2 v, int) { s[pad_idx(k)] = valid ? cmul(v, prop_col_h(k, kx, pc, a, pl, kc)) : v; };
-    team_fft_ex<NY, false, false, true, C::LPV, C::CTA>(s, tw, lane, team, load1, store1);
+    team_fft_ex<NY, false, false, true, C::LPV, C::CTA, (BAND ? center_band_mask<NY>() : 0u)>(s, tw, lane, team,
+                                                                                              load1, store1);
     team_barrier<C::LPV, C::CTA>(team);
     auto load2 = [&](int n) -> float2 { return s[pad_idx(n)]; };
     auto store2 = [&](int k, float2 v, int) { s[pad_idx(k)] = cscale(v, scale); };
@@ -476,6 +481,14 @@ __global__ void __launch_bounds__(RowCfg<NX>::THREADS, RowCfg<NX>::MINB) k_prop_
     team_fft<NX, true>(s, tw, lane, team, load, store);
   }
 }
+
+// the band variants are compiled for lengths of at least 256 whose first
+// radix divides by 4; the data band [pad, pad + n) must lie in [N / 4, 3 N / 4)
+template <int N>
+constexpr bool band_compiled() {
+  return N >= 256 && center_band_mask<N>() != 0u;
+}
+inline bool in_center_band(int N, int pad, int n) { return 4 * pad >= N && 4 * (pad + n) <= 3 * N; }
 
 // dispatchers (defined in prop2d_rows.cu / prop2d_cols.cu)
 cx_status dispatch_rows_fwd(int n, const float2* u, float2* T, const Prop2DArgs& a, cudaStream_t st);

@@ -6,7 +6,10 @@ namespace cx {
 template <int NY>
 static cx_status launch_cols(const float2* T, float2* T2, const Prop2DArgs& a, cudaStream_t st) {
   using C = ColCfg<NY>;
-  auto k = k_prop_cols<NY>;
+  auto k = k_prop_cols<NY, false>;
+  if constexpr (band_compiled<NY>()) {
+    if (in_center_band(NY, a.pad_y, a.ny)) k = k_prop_cols<NY, true>;
+  }
   CX_CUDA_TRY(set_smem(k, C::SMEM));
   const long items = (long)((a.px + C::V - 1) / C::V) * a.n_out_planes;
   const int grid = persistent_grid(k, C::THREADS, C::SMEM, items);

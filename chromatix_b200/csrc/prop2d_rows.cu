@@ -6,7 +6,10 @@ namespace cx {
 template <int NX>
 static cx_status launch_rows_fwd(const float2* u, float2* T, const Prop2DArgs& a, cudaStream_t st) {
   using C = RowCfg<NX>;
-  auto k = k_prop_rows_fwd<NX>;
+  auto k = k_prop_rows_fwd<NX, false>;
+  if constexpr (band_compiled<NX>()) {
+    if (in_center_band(NX, a.pad_x, a.nx)) k = k_prop_rows_fwd<NX, true>;
+  }
   CX_CUDA_TRY(set_smem(k, C::SMEM));
   const long items = ((long)a.n_in_planes * a.ny + C::TEAMS - 1) / C::TEAMS;
   const int grid = persistent_grid(k, C::THREADS, C::SMEM, items);
