@@ -9,6 +9,8 @@ IFFT, the crop in the last FFT's store.
 
 from __future__ import annotations
 
+import collections
+import ctypes
 from typing import Literal
 
 import numpy as np
@@ -80,28 +82,27 @@ def _plan_planes(field: Field, zs, zshape, py, px, shift_yx=(0.0, 0.0), bandlimi
     else:
         z_idx = np.zeros(nb_out, dtype=np.int64)
     W = field.n_wv
-    dxw = field.dx_wv
-    wl = field.spectrum.wavelength
+    dxw = np.asarray(field.dx_wv, dtype=np.float64).reshape(W, 2)
+    wl = np.asarray(field.spectrum.wavelength, dtype=np.float64).reshape(W)
     planes = np.zeros(nb_out * W, dtype=nat.PLANE_DTYPE)
     sy, sx = np.asarray(shift_yx, dtype=np.float64).reshape(2)
-    for ob in range(nb_out):
-        for w in range(W):
-            q = ob * W + w
-            z = float(zs[z_idx[ob]])
-            p = planes[q]
-            planes[q]["z"] = z
-            planes[q]["wavelength"] = wl[w]
-            planes[q]["dy"] = dxw[w, 0]
-            planes[q]["dx"] = dxw[w, 1]
-            planes[q]["shift_y"] = sy
-            planes[q]["shift_x"] = sx
-            planes[q]["in_plane"] = int(in_idx[ob]) * W + w
-            planes[q]["h_plane"] = int(h_index[q]) if h_index is not None else 0
-            if bandlimit:
-                k0, km = _bandlimit_rect(z, wl[w], (sy, sx), dxw[w, 0], dxw[w, 1], py, px, prec)
-                planes[q]["bl_y0"], planes[q]["bl_x0"] = k0
-                planes[q]["bl_hy"], planes[q]["bl_hx"] = km
-            del p
+    # plane q = ob W + w (batch-major, channel innermost)
+    zq = np.repeat(np.asarray(zs, dtype=np.float64).reshape(-1)[z_idx], W)
+    planes["z"] = zq
+    planes["wavelength"] = np.tile(wl, nb_out)
+    planes["dy"] = np.tile(dxw[:, 0], nb_out)
+    planes["dx"] = np.tile(dxw[:, 1], nb_out)
+    planes["shift_y"] = sy
+    planes["shift_x"] = sx
+    planes["in_plane"] = (np.repeat(in_idx.astype(np.int64), W) * W + np.tile(np.arange(W), nb_out))
+    if h_index is not None:
+        planes["h_plane"] = np.asarray(h_index, dtype=np.int64).reshape(-1)[: nb_out * W]
+    if bandlimit:
+        for q in range(nb_out * W):
+            w = q % W
+            k0, km = _bandlimit_rect(float(zq[q]), wl[w], (sy, sx), dxw[w, 0], dxw[w, 1], py, px, prec)
+            planes[q]["bl_y0"], planes[q]["bl_x0"] = k0
+            planes[q]["bl_hy"], planes[q]["bl_hx"] = km
     return planes, out_batch, nb_in, nb_out
 
 
@@ -134,19 +135,46 @@ class _PropPlan:
         return _PropPlan(d, planes, self.out_shape, adj_out, self.chromatic, self.H)
 
 
+# (descriptor bytes, plane table bytes, device) -> (workspace bytes, device
+# plane table, event after its upload): repeated propagations with the same
+# geometry skip the workspace query and the host-to-device copy of their
+# plane table.  The device tables are read-only; a call on another stream
+# waits for the upload's event before its kernels read the table.
+_PLAN_CACHE = collections.OrderedDict()
+_PLAN_CACHE_SIZE = 64
+
+
+def _device_plan(d, planes, dev):
+    torch = nat.torch_mod()
+    key = (ctypes.string_at(ctypes.addressof(d), ctypes.sizeof(d)), planes.tobytes(), dev.index)
+    hit = _PLAN_CACHE.get(key)
+    if hit is not None:
+        _PLAN_CACHE.move_to_end(key)
+        if not torch.cuda.is_current_stream_capturing():
+            torch.cuda.current_stream(dev).wait_event(hit[2])
+        return hit[0], hit[1]
+    ws_bytes = nat.c_size_t(0)
+    nat.check(nat.lib().cx_prop2d_workspace_size(d, ws_bytes))
+    table = nat.to_device_bytes(planes, dev)
+    ev = torch.cuda.Event()
+    ev.record(torch.cuda.current_stream(dev))
+    _PLAN_CACHE[key] = (int(ws_bytes.value), table, ev)
+    if len(_PLAN_CACHE) > _PLAN_CACHE_SIZE:
+        _PLAN_CACHE.popitem(last=False)
+    return int(ws_bytes.value), table
+
+
 def _launch_prop2d(plan: _PropPlan, u_in):
     torch = nat.torch_mod()
     L = nat.lib()
     d = plan.desc
-    ws_bytes = nat.c_size_t(0)
-    nat.check(L.cx_prop2d_workspace_size(d, ws_bytes))
     dev = u_in.device
+    ws_bytes, planes_dev = _device_plan(d, plan.planes, dev)
     u_in = u_in.contiguous()
     u_out = torch.empty(plan.out_shape, dtype=torch.complex64, device=dev)
-    ws = nat.workspace(ws_bytes.value, dev)
-    planes_dev = nat.to_device_bytes(plan.planes, dev)
+    ws = nat.workspace(ws_bytes, dev)
     nat.check(L.cx_prop2d(d, nat.ptr(planes_dev), nat.ptr(u_in), nat.ptr(u_out), nat.ptr(plan.H), nat.ptr(ws),
-                          ws_bytes.value, nat.stream_handle(dev)))
+                          ws_bytes, nat.stream_handle(dev)))
     return u_out
 
 
