@@ -161,29 +161,29 @@ def run_optfft(field: Field, z: float, n: float, pad_width=(0, 0), crop_width=(0
     norms = _optfft_norms(field, z, n, (Py, Px))
     dxw = field.dx_wv
     org = np.asarray(field.origin, dtype=np.float64).reshape(-1, 2)
-    planes = np.zeros(nb * W, dtype=FFT_PLANE_DTYPE)
-    for b in range(nb):
-        for w in range(W):
-            q = b * W + w
-            pre, conj, du, L_sq = norms[w]
-            p = planes[q]
-            p["pre_re"], p["pre_im"] = pre.real, pre.imag
-            post_w = complex(post[w] if np.ndim(post) else post)
-            p["post_re"], p["post_im"] = post_w.real, post_w.imag
-            p["chirp_in"] = 0.0 if chirp_in is None else float(np.atleast_1d(chirp_in)[min(w, np.size(chirp_in) - 1)])
-            p["chirp_out"] = 0.0 if chirp_out is None else float(
-                np.atleast_1d(chirp_out)[min(w, np.size(chirp_out) - 1)])
-            p["dy_in"], p["dx_in"] = dxw[w]
-            p["dy_out"], p["dx_out"] = du
-            p["oy"], p["ox"] = org[min(w, org.shape[0] - 1)]
-            if pupil_D is not None:
-                r = (field.spectrum.central_wavelength / field.spectrum.wavelength[w]) * pupil_D / 2
-                p["pupil_r2"] = r * r
-            else:
-                p["pupil_r2"] = -1.0
-            p["pupil_out_r2"] = -1.0
-            p["in_plane"] = q
-            p["conj"] = conj
+    # one row per wavelength, repeated for every batch element (plane q = b W + w)
+    row = np.zeros(W, dtype=FFT_PLANE_DTYPE)
+    for w in range(W):
+        pre, conj, du, L_sq = norms[w]
+        p = row[w]
+        p["pre_re"], p["pre_im"] = pre.real, pre.imag
+        post_w = complex(post[w] if np.ndim(post) else post)
+        p["post_re"], p["post_im"] = post_w.real, post_w.imag
+        p["chirp_in"] = 0.0 if chirp_in is None else float(np.atleast_1d(chirp_in)[min(w, np.size(chirp_in) - 1)])
+        p["chirp_out"] = 0.0 if chirp_out is None else float(
+            np.atleast_1d(chirp_out)[min(w, np.size(chirp_out) - 1)])
+        p["dy_in"], p["dx_in"] = dxw[w]
+        p["dy_out"], p["dx_out"] = du
+        p["oy"], p["ox"] = org[min(w, org.shape[0] - 1)]
+        if pupil_D is not None:
+            r = (field.spectrum.central_wavelength / field.spectrum.wavelength[w]) * pupil_D / 2
+            p["pupil_r2"] = r * r
+        else:
+            p["pupil_r2"] = -1.0
+        p["pupil_out_r2"] = -1.0
+        p["conj"] = conj
+    planes = np.tile(row, nb)
+    planes["in_plane"] = np.arange(nb * W)
     d = cx_optfft_desc()
     d.ny, d.nx, d.pad_y, d.pad_x, d.crop_y, d.crop_x = ny, nx, py_, px_, cy, cx
     d.n_wv, d.n_in_planes, d.n_out_planes = W, nb * W, nb * W
