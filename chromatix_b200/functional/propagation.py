@@ -142,6 +142,9 @@ class _PropPlan:
 # waits for the upload's event before its kernels read the table.
 _PLAN_CACHE = collections.OrderedDict()
 _PLAN_CACHE_SIZE = 64
+# propagation call parameters -> (descriptor, plane table, output shape);
+# descriptors and tables are never modified after they are built
+_HOST_PLANS = collections.OrderedDict()
 
 
 def _device_plan(d, planes, dev):
@@ -332,8 +335,19 @@ def _run_prop2d(field: Field, kernel: int, zs, zshape, n, pad_width, kykx=(0.0, 
         crop_w = (py_, px_) if mode == "same" else crop
         return _prop2d_general(field, kernel, zs, zshape, n, (py_, px_), kykx, shift_yx, remove_evanescent, bandlimit,
                                mode, crop_w, prec, H=H, h_index=h_index)
-    planes, out_batch, nb_in, nb_out = _plan_planes(field, zs, zshape, py, px, shift_yx, bandlimit, prec, h_index)
     W = field.n_wv
+    key = (kernel, tuple(field.u.shape), field.batch_shape, W, field.chromatic, py_, px_, crop, mode, prec,
+           np.asarray(field.dx_wv, dtype=np.float64).tobytes(),
+           np.asarray(field.spectrum.wavelength, dtype=np.float64).tobytes(),
+           np.asarray(zs, dtype=np.float64).tobytes(), tuple(zshape), float(n), tuple(np.ravel(kykx).tolist()),
+           tuple(np.ravel(shift_yx).tolist()), bool(remove_evanescent), bool(bandlimit),
+           None if h_index is None else np.asarray(h_index).tobytes())
+    hit = _HOST_PLANS.get(key)
+    if hit is not None:
+        _HOST_PLANS.move_to_end(key)
+        d, planes, out_shape = hit
+        return _apply_prop(_PropPlan(d, planes, tuple(field.u.shape), out_shape, field.chromatic, H), field.u)
+    planes, out_batch, nb_in, nb_out = _plan_planes(field, zs, zshape, py, px, shift_yx, bandlimit, prec, h_index)
     d = nat.cx_prop2d_desc()
     d.ny, d.nx, d.pad_y, d.pad_x = ny, nx, py_, px_
     d.n_wv = W
@@ -350,6 +364,9 @@ def _run_prop2d(field: Field, kernel: int, zs, zshape, n, pad_width, kykx=(0.0, 
     d.ky0, d.kx0 = float(ky0), float(kx0)
     oy, ox = (ny, nx) if mode == "same" else (py - 2 * crop[0], px - 2 * crop[1])
     out_shape = tuple(out_batch) + (oy, ox) + ((W,) if field.chromatic else ())
+    _HOST_PLANS[key] = (d, planes, out_shape)
+    if len(_HOST_PLANS) > _PLAN_CACHE_SIZE:
+        _HOST_PLANS.popitem(last=False)
     plan = _PropPlan(d, planes, tuple(field.u.shape), out_shape, field.chromatic, H)
     return _apply_prop(plan, field.u)
 
