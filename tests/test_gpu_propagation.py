@@ -302,3 +302,19 @@ def test_batch_matches_lone_fields_and_adjoint(mode):
         y1 = cf.asm_propagate(ScalarField(u1, 0.3, 0.0, spec), 50.0, 1.33, 256, mode=mode).u
         torch.real(torch.sum(torch.conj(w[b]) * y1)).backward()
         assert torch.equal(ug.grad[b], u1.grad), b
+
+
+@pytest.mark.parametrize("n,pad", [(400, 312), (514, 255), (384, 320)])
+def test_first_stage_band_pruning_edges(n, pad):
+    """1024-point padded grids: data inside the central half [256, 768)
+    (400 + 2*312, 384 + 2*320) take the pruned first stage; 514 + 2*255 puts
+    the data on [255, 769), one row and column past the band, and takes the
+    unpruned transforms.  All match the FP64 oracle at 1e-5, full and same."""
+    import chromatix_b200.functional as cf
+
+    u = rand_field((n, n), seed=n + pad)
+    for mode in ("full", "same"):
+        out = cf.asm_propagate(cuda_field(u, 0.3, 0.532), 80.0, 1.33, pad, mode=mode)
+        ref = O.asm_propagate(oracle_field(u, 0.3, 0.532), 80.0, 1.33, pad, mode=mode)
+        assert out.u.shape == ref.u.shape
+        assert rel(to_np(out.u), ref.u) < 1e-5, (n, pad, mode)
