@@ -435,7 +435,6 @@ struct Stage {
       // the stage with far fewer live registers than a guarded block.
       const int j = (EXACT || lane + it * LPV < NBF) ? lane + it * LPV : NBF - 1;
       {
-#pragma unroll
         if constexpr (FIRST) {
 #pragma unroll
           for (int r = 0; r < R; ++r) v[it][r] = ((ZM >> r) & 1u) ? make_float2(0.f, 0.f) : load(j + r * NBF);
