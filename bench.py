@@ -93,7 +93,17 @@ class ClockSampler:
                                          stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
         except Exception:
             self.proc = None
-        time.sleep(0.3)
+        # wait for the first sample: nvidia-smi's start-up takes driver locks
+        # that would stall this process's first launches inside the timed region
+        if self.proc is not None:
+            import select
+
+            ready, _, _ = select.select([self.proc.stdout], [], [], 10.0)
+            if ready:
+                first = self.proc.stdout.readline()
+                if first.strip():
+                    self.lines.append(first.strip())
+        time.sleep(0.1)
         return self
 
     def __exit__(self, *a):
@@ -105,7 +115,7 @@ class ClockSampler:
             except Exception:
                 self.proc.kill()
                 out = ""
-            self.lines = [ln for ln in (out or "").splitlines() if ln.strip()]
+            self.lines += [ln for ln in (out or "").splitlines() if ln.strip()]
 
     def summary(self):
         samples = [[p.strip() for p in ln.split(",")] for ln in self.lines]

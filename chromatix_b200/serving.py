@@ -345,6 +345,15 @@ class PropagationServer:
                     for B in range(1, batch_cap(N, self.max_batch) + 1):
                         d, wsb = self._prop_desc(op, N, n, B)
                         self._graph(slot, (op, N, float(n), B), d, wsb)
+        # grow each stream's allocator pool to a full batch of outputs per
+        # side now: a fresh cudaMalloc inside a stream's first large batches
+        # stalls the scheduler for tens of milliseconds
+        torch = self.torch
+        for slot in self.slots:
+            with torch.cuda.stream(slot.stream):
+                held = [torch.empty((N, N), dtype=torch.complex64, device=self.device)
+                        for N in sides for _ in range(batch_cap(N, self.max_batch))]
+                del held
         self.torch.cuda.synchronize(self.device)
 
     def _retire(self) -> list:
