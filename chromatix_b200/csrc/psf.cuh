@@ -263,23 +263,14 @@ __global__ void __launch_bounds__(ColCfg<NY>::THREADS, ColCfg<NY>::MINB) k_psf_c
       // field rows [slo, shi) feed FFT rows (y - ny/2) mod ny (ifftshift)
       load_col_tile<V, LEN>(tile, src - (size_t)ylo * a.nx, a.nx, x0, a.nx, slo, shi,
                             [&](int y) { return add_mod(y, NY - NY / 2, NY); });
-      // FFT row n holds field row (n + NY/2) mod NY; the support [slo, shi)
-      // contains the centre row NY/2 (or is empty), so the zero rows are
-      // [n_lo, n_hi) = [shi - NY/2, slo + NY - NY/2).  They are written as
-      // zeros here, except the band the first stage skips (edge_zero_mask),
-      // so the transform reads its inputs without a test per element.
-      {
-        constexpr int R0 = Plan<NY>::P.r[0];
-        const int z_lo = Q > 0 ? Q * (NY / R0) : NY, z_hi = Q > 0 ? (R0 - Q) * (NY / R0) : NY;
-        const int n_lo = shi > slo ? shi - NY / 2 : 0, n_hi = shi > slo ? slo + (NY - NY / 2) : NY;
-        const int cnt = n_hi - n_lo;
-        for (int idx = threadIdx.x; idx < cnt * V; idx += blockDim.x) {
-          const int n = n_lo + idx / V, c = idx % V;
-          if (n < z_lo || n >= z_hi) tile[c * LEN + pad_idx(n)] = make_float2(0.f, 0.f);
-        }
-      }
       __syncthreads();
-      auto load = [&](int n) -> float2 { return s[pad_idx(n)]; };
+      // FFT row n holds field row (n + NY/2) mod NY; the support [slo, shi)
+      // contains the centre row NY/2 (or is empty), so it maps to
+      // n < shi - NY/2 or n >= slo + NY - NY/2
+      const int n_lo = shi - NY / 2, n_hi = slo + (NY - NY / 2);
+      auto load = [&](int n) -> float2 {
+        return (n < n_lo || n >= n_hi) ? s[pad_idx(n)] : make_float2(0.f, 0.f);
+      };
       auto store = [&](int k, float2 v, int) {
         const float e = dens * cabs2(v);
         acc[k] = (w == 0) ? e : acc[k] + e;
