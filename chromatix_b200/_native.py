@@ -7,6 +7,7 @@ for device memory, streams and host<->device copies only.
 
 from __future__ import annotations
 
+import collections
 import ctypes
 import os
 import threading
@@ -278,6 +279,37 @@ def upload(arr: np.ndarray, device):
     torch = torch_mod()
     t = torch.from_numpy(np.ascontiguousarray(arr)).pin_memory()
     return t.to(device, non_blocking=True)
+
+
+# (descriptor type and bytes, plane table bytes, device) -> (workspace bytes,
+# device plane table, event after its upload): repeated calls with the same
+# geometry skip the workspace query and the host-to-device copy of their
+# plane table.  The device tables are read-only; a call on another stream
+# waits for the upload's event before its kernels read the table.
+_TABLES = collections.OrderedDict()
+_TABLES_SIZE = 128
+
+
+def device_table(desc, planes: np.ndarray, device, ws_query):
+    """(workspace bytes, device copy of ``planes``) for a launch described by
+    the ctypes struct ``desc``; ``ws_query(desc)`` returns the workspace size."""
+    torch = torch_mod()
+    key = (type(desc).__name__, ctypes.string_at(ctypes.addressof(desc), ctypes.sizeof(desc)), planes.tobytes(),
+           device.index)
+    hit = _TABLES.get(key)
+    if hit is not None:
+        _TABLES.move_to_end(key)
+        if not torch.cuda.is_current_stream_capturing():
+            torch.cuda.current_stream(device).wait_event(hit[2])
+        return hit[0], hit[1]
+    ws_bytes = int(ws_query(desc))
+    table = to_device_bytes(planes, device)
+    ev = torch.cuda.Event()
+    ev.record(torch.cuda.current_stream(device))
+    _TABLES[key] = (ws_bytes, table, ev)
+    if len(_TABLES) > _TABLES_SIZE:
+        _TABLES.popitem(last=False)
+    return ws_bytes, table
 
 
 def to_device_bytes(arr: np.ndarray, device):

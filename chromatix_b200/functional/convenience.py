@@ -110,14 +110,18 @@ def _launch_optfft(plan: _OptPlan, u):
     torch = nat.torch_mod()
     L = _sigs(nat.lib())
     dev = u.device
-    ws_b = nat.c_size_t(0)
-    nat.check(L.cx_optfft_workspace_size(plan.desc, ws_b))
+
+    def ws_query(d):
+        ws_b = nat.c_size_t(0)
+        nat.check(L.cx_optfft_workspace_size(d, ws_b))
+        return ws_b.value
+
+    ws_bytes, planes_dev = nat.device_table(plan.desc, plan.planes, dev, ws_query)
     u_out = torch.empty(plan.out_shape, dtype=torch.complex64, device=dev)
-    ws = nat.workspace(ws_b.value, dev)
-    planes_dev = nat.to_device_bytes(plan.planes, dev)
+    ws = nat.workspace(ws_bytes, dev)
     u_in = u.contiguous()
     nat.check(L.cx_optical_fft(plan.desc, nat.ptr(planes_dev), nat.ptr(u_in), nat.ptr(u_out), nat.ptr(ws),
-                               ws_b.value, nat.stream_handle(dev)))
+                               ws_bytes, nat.stream_handle(dev)))
     return u_out
 
 

@@ -10,7 +10,6 @@ IFFT, the crop in the last FFT's store.
 from __future__ import annotations
 
 import collections
-import ctypes
 from typing import Literal
 
 import numpy as np
@@ -135,36 +134,16 @@ class _PropPlan:
         return _PropPlan(d, planes, self.out_shape, adj_out, self.chromatic, self.H)
 
 
-# (descriptor bytes, plane table bytes, device) -> (workspace bytes, device
-# plane table, event after its upload): repeated propagations with the same
-# geometry skip the workspace query and the host-to-device copy of their
-# plane table.  The device tables are read-only; a call on another stream
-# waits for the upload's event before its kernels read the table.
-_PLAN_CACHE = collections.OrderedDict()
-_PLAN_CACHE_SIZE = 64
 # propagation call parameters -> (descriptor, plane table, output shape);
 # descriptors and tables are never modified after they are built
 _HOST_PLANS = collections.OrderedDict()
+_PLAN_CACHE_SIZE = 64
 
 
-def _device_plan(d, planes, dev):
-    torch = nat.torch_mod()
-    key = (ctypes.string_at(ctypes.addressof(d), ctypes.sizeof(d)), planes.tobytes(), dev.index)
-    hit = _PLAN_CACHE.get(key)
-    if hit is not None:
-        _PLAN_CACHE.move_to_end(key)
-        if not torch.cuda.is_current_stream_capturing():
-            torch.cuda.current_stream(dev).wait_event(hit[2])
-        return hit[0], hit[1]
-    ws_bytes = nat.c_size_t(0)
-    nat.check(nat.lib().cx_prop2d_workspace_size(d, ws_bytes))
-    table = nat.to_device_bytes(planes, dev)
-    ev = torch.cuda.Event()
-    ev.record(torch.cuda.current_stream(dev))
-    _PLAN_CACHE[key] = (int(ws_bytes.value), table, ev)
-    if len(_PLAN_CACHE) > _PLAN_CACHE_SIZE:
-        _PLAN_CACHE.popitem(last=False)
-    return int(ws_bytes.value), table
+def _prop_ws(d) -> int:
+    ws = nat.c_size_t(0)
+    nat.check(nat.lib().cx_prop2d_workspace_size(d, ws))
+    return ws.value
 
 
 def _launch_prop2d(plan: _PropPlan, u_in):
@@ -172,7 +151,7 @@ def _launch_prop2d(plan: _PropPlan, u_in):
     L = nat.lib()
     d = plan.desc
     dev = u_in.device
-    ws_bytes, planes_dev = _device_plan(d, plan.planes, dev)
+    ws_bytes, planes_dev = nat.device_table(d, plan.planes, dev, _prop_ws)
     u_in = u_in.contiguous()
     u_out = torch.empty(plan.out_shape, dtype=torch.complex64, device=dev)
     ws = nat.workspace(ws_bytes, dev)
