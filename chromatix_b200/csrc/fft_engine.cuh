@@ -31,13 +31,6 @@ __host__ __device__ constexpr Radices make_radices(int N) {
   // stage's shared-memory exchange is then bank-conflict free (a stride-3/5/7
   // write in the first stage is not)
   Radices p{0, {0}};
-  if (N == 1024) {
-    // two radix-32 stages: one shared-memory exchange and one twiddle pass
-    // instead of two, on one-warp teams
-    p.r[p.n++] = 32;
-    p.r[p.n++] = 32;
-    return p;
-  }
   int m = N;
   int n7 = 0, n5 = 0, n3 = 0;
   while (m % 7 == 0) { ++n7; m /= 7; }
@@ -207,36 +200,6 @@ struct DFT<16, INV> {
     }
 #pragma unroll
     for (int i = 0; i < 16; ++i) v[i] = y[i];
-  }
-};
-
-// radix 32 as two radix-16 transforms of the even and odd inputs and one
-// radix-2 step: y_k = E_k + w32^k O_k, y_(k+16) = E_k - w32^k O_k
-template <bool INV>
-struct DFT<32, INV> {
-  __device__ __forceinline__ static void run(float2* v) {
-    // cos(pi k / 16), k = 0..8
-    constexpr float C[9] = {1.0f, 0.98078528040323044913f, 0.92387953251128675613f, 0.83146961230254523708f,
-                            0.70710678118654752440f, 0.55557023301960222474f, 0.38268343236508977173f,
-                            0.19509032201612826785f, 0.0f};
-    float2 e[16], o[16];
-#pragma unroll
-    for (int i = 0; i < 16; ++i) {
-      e[i] = v[2 * i];
-      o[i] = v[2 * i + 1];
-    }
-    DFT<16, INV>::run(e);
-    DFT<16, INV>::run(o);
-#pragma unroll
-    for (int k = 0; k < 16; ++k) {
-      // w32^k = exp(-+ i pi k / 16) = (cos, -+ sin)
-      const float c = k <= 8 ? C[k] : -C[16 - k];
-      const float sn = k <= 8 ? C[8 - k] : C[k - 8];
-      const float2 w = make_float2(c, INV ? sn : -sn);
-      const float2 t = k == 0 ? o[0] : cmul(o[k], w);
-      v[k] = cadd(e[k], t);
-      v[k + 16] = csub(e[k], t);
-    }
   }
 };
 
@@ -422,28 +385,13 @@ __device__ __forceinline__ void apply_twiddles(const float2* tw, int m, float2* 
           v[6] = cmul(v[6], cmul(w4, w2));
         }
       }
-      if constexpr (R == 8 || R == 16 || R == 32) {
+      if constexpr (R == 8 || R == 16) {
         float2 w4 = tw[N + m];  // contiguous copy of tw[4 m] (bank-conflict free)
         if (INV) w4.y = -w4.y;
         v[4] = cmul(v[4], w4);
         v[5] = cmul(v[5], cmul(w4, w1));
         v[6] = cmul(v[6], cmul(w4, w2));
         v[7] = cmul(v[7], cmul(w4, w3));
-        if constexpr (R == 32) {
-          const float2 w8 = cmul(w4, w4);
-          const float2 w12 = cmul(w8, w4);
-          const float2 w16 = cmul(w8, w8);
-          // v[j + 4 q] *= w^(4 q) w^j for q = 2..7, j = 0..3
-#pragma unroll
-          for (int q = 2; q < 8; ++q) {
-            const float2 wq = q == 2 ? w8 : q == 3 ? w12 : q == 4 ? w16 : q == 5 ? cmul(w16, w4)
-                              : q == 6 ? cmul(w16, w8) : cmul(w16, w12);
-            v[4 * q] = cmul(v[4 * q], wq);
-            v[4 * q + 1] = cmul(v[4 * q + 1], cmul(wq, w1));
-            v[4 * q + 2] = cmul(v[4 * q + 2], cmul(wq, w2));
-            v[4 * q + 3] = cmul(v[4 * q + 3], cmul(wq, w3));
-          }
-        }
         if constexpr (R == 16) {
           const float2 w8 = cmul(w4, w4);
           v[8] = cmul(v[8], w8);

@@ -118,15 +118,10 @@ __device__ __forceinline__ void load_twiddles(float2* tw, const float2* __restri
 int sm_count();  // of the current device (capi.cu)
 
 // Register budget of the row / column kernels: about 80 registers per thread
-// (min blocks per SM derived from the CTA size); radix-32 plans hold 32
-// complex values per lane and stage, so their kernels get 128.
-__host__ __device__ constexpr int minb_for(int threads, int regs = 80) {
-  const int b = 65536 / (threads * regs);
+// (min blocks per SM derived from the CTA size).
+__host__ __device__ constexpr int minb_for(int threads) {
+  const int b = 65536 / (threads * 80);
   return b < 1 ? 1 : b;
-}
-template <int N>
-constexpr int regs_for() {
-  return max_radix(N) >= 32 ? 128 : 80;
 }
 
 // Row kernels: about 192 threads (small CTAs: a 1024^2 pass is 1024 rows, so
@@ -138,7 +133,7 @@ struct RowCfg {
   static constexpr int T0 = 192 / LPV > 0 ? 192 / LPV : 1;
   static constexpr int TEAMS = (LPV > 32 && T0 > 15) ? 15 : T0;
   static constexpr int THREADS = TEAMS * LPV;
-  static constexpr int MINB = minb_for(THREADS, regs_for<N>());
+  static constexpr int MINB = minb_for(THREADS);
   static constexpr int TW = tw_len(N);
   static constexpr size_t SMEM = sizeof(float2) * ((size_t)TW + (size_t)TEAMS * Plan<N>::LEN);
 };
@@ -163,7 +158,7 @@ struct RowCfgX {
   static constexpr int TEAMS = teams_for();
   static constexpr int THREADS = TEAMS * LPV;
   static_assert(THREADS <= 1024, "row CTA too large");
-  static constexpr int MINB = minb_for(THREADS, regs_for<N>());
+  static constexpr int MINB = minb_for(THREADS);
   static constexpr int TW = tw_len(N);
   static constexpr size_t SMEM = sizeof(float2) * ((size_t)TW + (size_t)TEAMS * Plan<N>::LEN);
 };
@@ -197,7 +192,7 @@ struct ColCfg {
   static_assert(!CTA || (V * LPV) % 32 == 0, "exact-size teams must fill whole warps");
   static constexpr int LEN = col_len(N, V);
   static constexpr int THREADS = V * LPV;
-  static constexpr int MINB = minb_for(THREADS, regs_for<N>());
+  static constexpr int MINB = minb_for(THREADS);
   static constexpr size_t SMEM = smem_for(V);
 };
 
