@@ -318,3 +318,34 @@ def test_first_stage_band_pruning_edges(n, pad):
         ref = O.asm_propagate(oracle_field(u, 0.3, 0.532), 80.0, 1.33, pad, mode=mode)
         assert out.u.shape == ref.u.shape
         assert rel(to_np(out.u), ref.u) < 1e-5, (n, pad, mode)
+
+
+def test_propagation_replays_from_a_cuda_graph():
+    """asm_propagate captured in a torch CUDA graph (after one warm call, so
+    its plan and device plane table are cached) and replayed on new input
+    data gives the eager result bit for bit."""
+    import torch
+
+    import chromatix_b200.functional as cf
+    from chromatix_b200.core.field import ScalarField
+    from chromatix_b200.core.spectrum import Spectrum
+
+    spec = Spectrum.build(0.532)
+    u_static = torch.as_tensor(rand_field((256, 256), seed=71), device="cuda")
+    f = ScalarField(u_static, 0.3, 0.0, spec)
+    cf.asm_propagate(f, 40.0, 1.33, 128)  # warm: plan, table, workspace size
+    torch.cuda.synchronize()
+    g = torch.cuda.CUDAGraph()
+    s = torch.cuda.Stream()
+    s.wait_stream(torch.cuda.current_stream())
+    with torch.cuda.stream(s):
+        with torch.cuda.graph(g, stream=s):
+            out = cf.asm_propagate(f, 40.0, 1.33, 128).u
+    torch.cuda.current_stream().wait_stream(s)
+    for seed in (72, 73):
+        new = torch.as_tensor(rand_field((256, 256), seed=seed), device="cuda")
+        u_static.copy_(new)
+        g.replay()
+        torch.cuda.synchronize()
+        eager = cf.asm_propagate(ScalarField(new, 0.3, 0.0, spec), 40.0, 1.33, 128).u
+        assert torch.equal(out, eager), seed
