@@ -1,6 +1,7 @@
 // C API of the multislice forward / adjoint (kernels in multislice.cuh and
 // the prop2d column pass).
 #include <cmath>
+#include <mutex>
 
 #include "multislice.cuh"
 
@@ -75,12 +76,32 @@ static cx_status ms_plan(const cx_ms_desc* d, MsPlan* p) {
 
 static size_t al(size_t b) { return (b + 255) & ~(size_t)255; }
 
-// workspace: [planes (4 x cx_plane)] [H table] [F state] ([G state] [K records] for the adjoint)
+// workspace: [planes (4 x cx_plane)] [H table] [F state] ([G state] [2 x K records] for the adjoint:
+// the records of two segments, one being read by the adjoint while the next is recomputed)
 static size_t ms_ws(const MsPlan& p, bool grad) {
   const size_t field = sizeof(float2) * (size_t)p.py * p.px;
   size_t b = al(4 * sizeof(cx_plane)) + 2 * al(field);
-  if (grad) b += al(field) + (size_t)p.K * al(field);
+  if (grad) b += al(field) + 2 * (size_t)p.K * al(field);
   return b;
+}
+
+// Second stream of a device for the adjoint's recomputation chain (created
+// once, non-blocking; ordered against the caller's stream by events only).
+// nullptr if it cannot be created: the adjoint then runs on one stream.
+static cudaStream_t ms_side_stream() {
+  static std::mutex mu;
+  static cudaStream_t side[64] = {};
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) {
+    cudaGetLastError();
+    return nullptr;
+  }
+  std::lock_guard<std::mutex> lock(mu);
+  if (!side[dev] && cudaStreamCreateWithFlags(&side[dev], cudaStreamNonBlocking) != cudaSuccess) {
+    cudaGetLastError();
+    side[dev] = nullptr;
+  }
+  return side[dev];
 }
 
 static MsArgs ms_args(const cx_ms_desc* d, const MsPlan& p) {
@@ -306,13 +327,23 @@ extern "C" cx_status cx_multislice_backward(const cx_ms_desc* d, const float* dn
   if ((s = ms_rows(g, st)) != CX_OK) return s;
   if ((s = col_pass(p, planes + 3, G, na_mask(d), false, st)) != CX_OK) return s;
 
+  // Segment sgi (slices i0 .. i1-1): recompute u_{i0+1} .. u_{i1} from the
+  // checkpoint u_{i0} into records[sgi & 1], then the adjoint through slices
+  // i1-1 .. i0 reads them.  The recomputation of segment sgi - 1 needs only
+  // its checkpoint, so it runs on a second stream (rs) while the adjoint
+  // works through segment sgi (one pass alone fills few SMs: a 1024^2 plane is
+  // 1024 transforms).  Order: adjoint(sgi) waits for recompute(sgi);
+  // recompute(sgi - 2), which overwrites the same record half, waits for
+  // adjoint(sgi).  Both chains run the same kernels on the same data as a
+  // serial run, so the gradients are the same bits.
   MsArgs f = ms_args(d, p);
   f.dn = dn;
   f.ab = ab;
   f.buf = F;
-  for (int sgi = p.nseg - 1; sgi >= 0; --sgi) {
+  auto recompute = [&](int sgi, cudaStream_t q) -> cx_status {
     const int i0 = sgi * p.K, i1 = (i0 + p.K < p.D) ? i0 + p.K : p.D;
-    // recompute u_{i0+1} .. u_{i1} from the checkpoint u_{i0}
+    float2* recs = seg + (size_t)(sgi & 1) * p.K * seg_stride;
+    cx_status e;
     f.mode = MS_LOAD;
     f.src = ck + (size_t)sgi * field;
     f.sy = p.py;
@@ -320,26 +351,78 @@ extern "C" cx_status cx_multislice_backward(const cx_ms_desc* d, const float* dn
     f.oy = 0;
     f.ox = 0;
     f.record = 0;
-    if ((s = ms_rows(f, st)) != CX_OK) return s;
-    if ((s = col_pass(p, planes + 0, F, -1.0, true, st, Htab)) != CX_OK) return s;
+    if ((e = ms_rows(f, q)) != CX_OK) return e;
+    if ((e = col_pass(p, planes + 0, F, -1.0, true, q, Htab)) != CX_OK) return e;
     f.mode = MS_FWD;
     for (int i = i0 + 1; i <= i1; ++i) {
       f.slice = i - 1;
       f.record = 1;
-      f.rec = seg + (size_t)(i - i0 - 1) * seg_stride;
-      if ((s = ms_rows(f, st)) != CX_OK) return s;
-      if (i < i1 && (s = col_pass(p, planes + 0, F, -1.0, true, st, Htab)) != CX_OK) return s;
+      f.rec = recs + (size_t)(i - i0 - 1) * seg_stride;
+      if ((e = ms_rows(f, q)) != CX_OK) return e;
+      if (i < i1 && (e = col_pass(p, planes + 0, F, -1.0, true, q, Htab)) != CX_OK) return e;
     }
-    // adjoint through slices i1-1 .. i0
+    return CX_OK;
+  };
+  auto adjoint = [&](int sgi, cudaStream_t q) -> cx_status {
+    const int i0 = sgi * p.K, i1 = (i0 + p.K < p.D) ? i0 + p.K : p.D;
+    const float2* recs = seg + (size_t)(sgi & 1) * p.K * seg_stride;
+    cx_status e;
     g.mode = MS_BWD;
     for (int i = i1 - 1; i >= i0; --i) {
       g.slice = i;
-      g.rec_u = seg + (size_t)(i - i0) * seg_stride;
+      g.rec_u = recs + (size_t)(i - i0) * seg_stride;
       g.gdn = grad_dn + (size_t)i * d->ny * d->nx;
       g.gab = grad_ab + (size_t)i * d->ny * d->nx;
-      if ((s = ms_rows(g, st)) != CX_OK) return s;
-      if ((s = col_pass(p, planes + 1, G, -1.0, true, st, Htab, true)) != CX_OK) return s;
+      if ((e = ms_rows(g, q)) != CX_OK) return e;
+      if ((e = col_pass(p, planes + 1, G, -1.0, true, q, Htab, true)) != CX_OK) return e;
     }
+    return CX_OK;
+  };
+
+  cudaStream_t rs = ms_side_stream();
+  cudaEvent_t ev[4] = {};  // fork, recomputed (two halves), adjoint done
+  int made = 0;
+  if (rs && rs != st) {
+    for (; made < 4; ++made)
+      if (cudaEventCreateWithFlags(&ev[made], cudaEventDisableTiming) != cudaSuccess) break;
+    if (made < 4) {
+      cudaGetLastError();
+      rs = nullptr;
+    }
+  } else {
+    rs = nullptr;
+  }
+  cudaError_t ce = cudaSuccess;
+  if (rs) {
+    // the recomputation reads the checkpoints, the H table and the planes written on st
+    if ((ce = cudaEventRecord(ev[0], st)) == cudaSuccess) ce = cudaStreamWaitEvent(rs, ev[0], 0);
+  }
+  cudaStream_t q = rs ? rs : st;
+  s = CX_OK;
+  for (int k = 0; k < 2 && k < p.nseg && ce == cudaSuccess && s == CX_OK; ++k) {
+    const int sgi = p.nseg - 1 - k;
+    if ((s = recompute(sgi, q)) == CX_OK && rs) ce = cudaEventRecord(ev[1 + (sgi & 1)], rs);
+  }
+  for (int sgi = p.nseg - 1; sgi >= 0 && ce == cudaSuccess && s == CX_OK; --sgi) {
+    if (rs && (ce = cudaStreamWaitEvent(st, ev[1 + (sgi & 1)], 0)) != cudaSuccess) break;
+    if (!rs && sgi < p.nseg - 2 && (s = recompute(sgi, st)) != CX_OK) break;
+    if ((s = adjoint(sgi, st)) != CX_OK) break;
+    if (rs && sgi >= 2) {
+      if ((ce = cudaEventRecord(ev[3], st)) != cudaSuccess) break;
+      if ((ce = cudaStreamWaitEvent(rs, ev[3], 0)) != cudaSuccess) break;
+      if ((s = recompute(sgi - 2, rs)) != CX_OK) break;
+      ce = cudaEventRecord(ev[1 + (sgi & 1)], rs);
+    }
+  }
+  if (rs && (s != CX_OK || ce != cudaSuccess)) {
+    // failed part-way: st still takes up everything issued on rs
+    if (cudaEventRecord(ev[0], rs) == cudaSuccess) cudaStreamWaitEvent(st, ev[0], 0);
+  }
+  for (int k = 0; k < made; ++k) cudaEventDestroy(ev[k]);
+  if (s != CX_OK) return s;
+  if (ce != cudaSuccess) {
+    set_error("cx_multislice_backward: %s", cudaGetErrorString(ce));
+    return CX_ERR_CUDA;
   }
   if (grad_u_in) {
     g.mode = MS_FINAL;

@@ -138,3 +138,32 @@ def test_return_stack_planes_match_partial_stacks():
         ref = O.multislice_thick_sample(oracle_field(u, 0.1, 0.532), ab[:k], dn[:k], 1.33, 0.2, pad,
                                         reverse_propagate_distance=0.0)
         assert rel(to_np(st.u[k - 1]), ref.u) < 1e-5
+
+
+def test_gradient_independent_of_checkpoint_spacing():
+    """The adjoint recomputes segment s - 1 on a second stream while it works
+    through segment s (double-buffered records).  Any checkpoint spacing must
+    give the gradients of a single segment (no recomputation overlap at all):
+    a race between the two chains would show up as a difference here.  On a
+    power-of-two grid the recomputed records are the forward's bits, so the
+    gradients agree to the last bit."""
+    import torch
+
+    import chromatix_b200.functional as cf
+
+    ny, nx, D = 128, 128, 24
+    lam, dz, n, dx = 0.532, 0.2, 1.33, 0.1
+    u = rand_field((ny, nx), seed=11, amp=(0.9, 1.0))
+    dn, ab = _sample(D, ny, nx, seed=12)
+    tgt = torch.as_tensor(np.random.default_rng(13).uniform(0.5, 1.5, (ny, nx)).astype(np.float32), device="cuda")
+    grads = {}
+    for K in (D, 1, 2, 5, 7):
+        dn_t = torch.as_tensor(dn, device="cuda").requires_grad_(True)
+        ab_t = torch.as_tensor(ab, device="cuda").requires_grad_(True)
+        out = cf.multislice_thick_sample(cuda_field(u, dx, lam), ab_t, dn_t, n, dz, 0, checkpoint_every=K)
+        loss = ((out.u.abs() ** 2 - tgt) ** 2).sum()
+        loss.backward()
+        grads[K] = (dn_t.grad.cpu().numpy(), ab_t.grad.cpu().numpy())
+    for K in (1, 2, 5, 7):
+        np.testing.assert_array_equal(grads[K][0], grads[D][0], err_msg=f"dL/d dn, K={K}")
+        np.testing.assert_array_equal(grads[K][1], grads[D][1], err_msg=f"dL/d abs, K={K}")
