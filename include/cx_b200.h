@@ -251,7 +251,10 @@ cx_status cx_optical_fft_h(const cx_optfft_desc* d, const cx_fft_plane* planes_d
  * u_{i+1} = t_i * IFFT2(H(dz) FFT2(u_i)), t_i = exp(i 2 pi dz/lambda (dn_i + i abs_i)),
  * then the defocus by -reverse_distance (ASM, optional NA mask) and the crop.
  * The adjoint takes g_out = dL/dRe(u_out) + i dL/dIm(u_out) and returns
- * dL/d dn, dL/d abs (and dL/du_in), recomputing each checkpoint segment.
+ * dL/d dn, dL/d abs (and dL/du_in), recomputing each checkpoint segment (the
+ * next segment's recomputation runs on a library-owned second stream of the
+ * current device, joined back into `stream` by events before the call's last
+ * launch; the workspace holds two segments of records).
  * ------------------------------------------------------------------------- */
 typedef struct {
   int32_t ny, nx;            /* field shape (unpadded) */
