@@ -9,6 +9,7 @@ namespace cx {
 
 struct MsPlan {
   int py, px, D, K, nseg;
+  int last;  // slices of the last segment, whose records the forward keeps (no recomputation)
   Prop2DArgs col;  // column pass template (plane pointer set per launch)
 };
 
@@ -45,6 +46,7 @@ static cx_status ms_plan(const cx_ms_desc* d, MsPlan* p) {
   if (K > p->D) K = p->D;
   p->K = K;
   p->nseg = (p->D + K - 1) / K;
+  p->last = p->D - (p->nseg - 1) * K;
   Prop2DArgs& a = p->col;
   a.ny = p->py;
   a.nx = p->px;
@@ -223,7 +225,7 @@ extern "C" cx_status cx_multislice_workspace_size(const cx_ms_desc* d, int32_t n
 extern "C" int32_t cx_multislice_num_checkpoints(const cx_ms_desc* d) {
   MsPlan p;
   if (ms_plan(d, &p) != CX_OK) return -1;
-  return p.nseg;
+  return p.nseg + p.last;
 }
 
 extern "C" cx_status cx_multislice_forward(const cx_ms_desc* d, const void* u_in, const float* dn, const float* ab,
@@ -264,11 +266,21 @@ extern "C" cx_status cx_multislice_forward(const cx_ms_desc* d, const void* u_in
   a.rec = ck;
   if ((s = ms_rows(a, st)) != CX_OK) return s;
   if ((s = col_pass(p, planes + 0, F, -1.0, true, st, Htab)) != CX_OK) return s;
+  // checkpoints: u_0, u_K, u_2K, ... (nseg planes), then u_{i0+1} .. u_D of the
+  // last segment (i0 = (nseg - 1) K), which the adjoint reads without recomputing
   a.mode = MS_FWD;
+  const int i0_last = (p.nseg - 1) * p.K;
   for (int i = 1; i <= p.D; ++i) {
     a.slice = i - 1;  // u_i = t_{i-1} P(u_{i-1})
-    a.record = (ck && i < p.D && i % p.K == 0) ? 1 : 0;
-    a.rec = a.record ? ck + (size_t)(i / p.K) * field : nullptr;
+    a.record = 0;
+    a.rec = nullptr;
+    if (ck && i < p.D && i % p.K == 0) {
+      a.record = 1;
+      a.rec = ck + (size_t)(i / p.K) * field;
+    } else if (ck && i > i0_last) {
+      a.record = 1;
+      a.rec = ck + (size_t)(p.nseg + i - i0_last - 1) * field;
+    }
     if ((s = ms_rows(a, st)) != CX_OK) return s;
     if (i < p.D && (s = col_pass(p, planes + 0, F, -1.0, true, st, Htab)) != CX_OK) return s;
   }
@@ -327,15 +339,18 @@ extern "C" cx_status cx_multislice_backward(const cx_ms_desc* d, const float* dn
   if ((s = ms_rows(g, st)) != CX_OK) return s;
   if ((s = col_pass(p, planes + 3, G, na_mask(d), false, st)) != CX_OK) return s;
 
-  // Segment sgi (slices i0 .. i1-1): recompute u_{i0+1} .. u_{i1} from the
-  // checkpoint u_{i0} into records[sgi & 1], then the adjoint through slices
-  // i1-1 .. i0 reads them.  The recomputation of segment sgi - 1 needs only
-  // its checkpoint, so it runs on a second stream (rs) while the adjoint
-  // works through segment sgi (one pass alone fills few SMs: a 1024^2 plane is
-  // 1024 transforms).  Order: adjoint(sgi) waits for recompute(sgi);
-  // recompute(sgi - 2), which overwrites the same record half, waits for
-  // adjoint(sgi).  Both chains run the same kernels on the same data as a
-  // serial run, so the gradients are the same bits.
+  // Segment sgi (slices i0 .. i1-1): the adjoint through slices i1-1 .. i0
+  // reads u_{i0+1} .. u_{i1}.  The last segment's were recorded by the
+  // forward (after the nseg checkpoints); every other segment's are
+  // recomputed from its checkpoint u_{i0} into records[sgi & 1].  The
+  // recomputation of segment sgi - 1 needs only its checkpoint, so it runs on
+  // a second stream (rs) while the adjoint works through segment sgi (one pass
+  // alone fills few SMs: a 1024^2 plane is 1024 transforms).  Order:
+  // adjoint(sgi) waits for recompute(sgi); recompute(sgi - 2), which
+  // overwrites the same record half, waits for adjoint(sgi) (the last
+  // segment reads no half, so recompute(nseg - 3) starts at once).  Both
+  // chains run the same kernels on the same data as a serial run, so the
+  // gradients are the same bits.
   MsArgs f = ms_args(d, p);
   f.dn = dn;
   f.ab = ab;
@@ -365,12 +380,14 @@ extern "C" cx_status cx_multislice_backward(const cx_ms_desc* d, const float* dn
   };
   auto adjoint = [&](int sgi, cudaStream_t q) -> cx_status {
     const int i0 = sgi * p.K, i1 = (i0 + p.K < p.D) ? i0 + p.K : p.D;
-    const float2* recs = seg + (size_t)(sgi & 1) * p.K * seg_stride;
+    const bool last = sgi == p.nseg - 1;
+    const float2* recs = last ? ck + (size_t)p.nseg * field : seg + (size_t)(sgi & 1) * p.K * seg_stride;
+    const size_t stride = last ? field : seg_stride;
     cx_status e;
     g.mode = MS_BWD;
     for (int i = i1 - 1; i >= i0; --i) {
       g.slice = i;
-      g.rec_u = recs + (size_t)(i - i0) * seg_stride;
+      g.rec_u = recs + (size_t)(i - i0) * stride;
       g.gdn = grad_dn + (size_t)i * d->ny * d->nx;
       g.gab = grad_ab + (size_t)i * d->ny * d->nx;
       if ((e = ms_rows(g, q)) != CX_OK) return e;
@@ -397,17 +414,18 @@ extern "C" cx_status cx_multislice_backward(const cx_ms_desc* d, const float* dn
     // the recomputation reads the checkpoints, the H table and the planes written on st
     if ((ce = cudaEventRecord(ev[0], st)) == cudaSuccess) ce = cudaStreamWaitEvent(rs, ev[0], 0);
   }
-  cudaStream_t q = rs ? rs : st;
   s = CX_OK;
-  for (int k = 0; k < 2 && k < p.nseg && ce == cudaSuccess && s == CX_OK; ++k) {
-    const int sgi = p.nseg - 1 - k;
-    if ((s = recompute(sgi, q)) == CX_OK && rs) ce = cudaEventRecord(ev[1 + (sgi & 1)], rs);
+  if (rs) {
+    for (int t = p.nseg - 2; t >= 0 && t >= p.nseg - 3 && ce == cudaSuccess && s == CX_OK; --t)
+      if ((s = recompute(t, rs)) == CX_OK) ce = cudaEventRecord(ev[1 + (t & 1)], rs);
   }
   for (int sgi = p.nseg - 1; sgi >= 0 && ce == cudaSuccess && s == CX_OK; --sgi) {
-    if (rs && (ce = cudaStreamWaitEvent(st, ev[1 + (sgi & 1)], 0)) != cudaSuccess) break;
-    if (!rs && sgi < p.nseg - 2 && (s = recompute(sgi, st)) != CX_OK) break;
+    if (sgi < p.nseg - 1) {
+      if (rs && (ce = cudaStreamWaitEvent(st, ev[1 + (sgi & 1)], 0)) != cudaSuccess) break;
+      if (!rs && (s = recompute(sgi, st)) != CX_OK) break;
+    }
     if ((s = adjoint(sgi, st)) != CX_OK) break;
-    if (rs && sgi >= 2) {
+    if (rs && sgi >= 2 && sgi <= p.nseg - 2) {
       if ((ce = cudaEventRecord(ev[3], st)) != cudaSuccess) break;
       if ((ce = cudaStreamWaitEvent(rs, ev[3], 0)) != cudaSuccess) break;
       if ((s = recompute(sgi - 2, rs)) != CX_OK) break;

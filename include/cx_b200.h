@@ -45,9 +45,10 @@ typedef enum {
 typedef enum {
   CX_PREC_ACCURATE = 0, /* FP64 phase arguments reduced mod 2pi, FP32 FFT */
   CX_PREC_REF32 = 1,    /* FP32 in the reference's operation order */
-  CX_PREC_SPLIT16 = 2   /* as ACCURATE, with the transform stages of the passes that have a tensor-core
-                           form (the PSF column pass at 1024 / 1280 rows) run as dense DFT contractions on
-                           FP16 hi + lo operands, FP32 accumulation; other entry points reject it */
+  CX_PREC_SPLIT16 = 2   /* as ACCURATE, with the transforms of length 1024 / 1280 run as dense DFT
+                           contractions on the tensor cores (FP16 hi + lo operands, FP32 accumulation):
+                           cx_psf_4f, cx_prop2d(_ptrs) and cx_multislice_* on grids with 1024 or 1280
+                           (padded) rows; other entry points and grids reject it */
 } cx_precision;
 
 typedef enum {
@@ -271,7 +272,9 @@ typedef struct {
 } cx_ms_desc;
 
 cx_status cx_multislice_workspace_size(const cx_ms_desc* d, int32_t need_grad, size_t* bytes);
-/* number of checkpoints the forward writes (each (ny + 2 pad) x (nx + 2 pad) complex64) */
+/* number of planes the forward writes into `checkpoints` (each (ny + 2 pad) x (nx + 2 pad) complex64):
+ * one every K slices, then the fields after each slice of the last segment (which the adjoint
+ * therefore does not recompute) */
 int32_t cx_multislice_num_checkpoints(const cx_ms_desc* d);
 /* dn, abs: (D, ny, nx) float32; u_in, u_out: (ny, nx) complex64; checkpoints may be NULL
  * (forward only). */
