@@ -144,28 +144,71 @@ __global__ void __launch_bounds__(RowCfg<NZ>::THREADS, RowCfg<NZ>::MINB) k_mbs_z
   }
 }
 
+// Asynchronous copy (cp.async, 8 bytes per element) of rows [0, n) x columns
+// [x0, x0 + V) of a row-major matrix (leading dimension ld) into a column tile
+// tile[c * LEN + pad_idx(r)]; columns at or beyond ncols are not copied (their
+// entries are stale and their results are never stored).  The caller commits.
+template <int V, int LEN>
+__device__ __forceinline__ void prefetch_col_tile(float2* tile, const float2* src, long ld, long x0, long ncols,
+                                                  int n) {
+  for (int idx = threadIdx.x; idx < n * V; idx += blockDim.x) {
+    const int r = idx / V, c = idx % V;
+    if (x0 + c < ncols) cp_async8(tile + c * LEN + pad_idx(r), src + (long)r * ld + x0 + c);
+  }
+}
+
 // column tiles along an axis of length N with element stride E: vectors
-// (outer o, inner i), element j at buf + o * ostride + i + j * E; in place
+// (outer o, inner i), element j at buf + o * ostride + i + j * E; in place.
+// Two tiles in shared memory: the copy of the CTA's next tile is in flight
+// (cp.async) while the current one is transformed and stored.
+// At least 8 columns per tile: each row of the strided axis is read and
+// written as one 64-byte segment.
+template <int N>
+struct MbsColCfg {
+  using B = ColCfg<N, false>;
+  static constexpr int LPV = B::LPV, TW = B::TW;
+  static constexpr bool CTA = B::CTA;
+  static constexpr int V = B::V >= 8 ? B::V : (8 * LPV <= 1024 ? 8 : B::V);
+  static constexpr int LEN = col_len(N, V);
+  static constexpr int THREADS = V * LPV;
+  static constexpr int MINB = minb_for(THREADS);
+  static constexpr size_t SMEM = sizeof(float2) * ((size_t)TW + 2 * (size_t)V * LEN);
+  static_assert(SMEM <= 227 * 1024, "two column tiles do not fit in shared memory");
+  static_assert(!CTA, "column teams of the strided passes tile warps");
+};
+
 template <int N, bool INV>
-__global__ void __launch_bounds__(ColCfg<N, false>::THREADS, ColCfg<N, false>::MINB) k_mbs_cols(MbsArgs a, long n_outer,
+__global__ void __launch_bounds__(MbsColCfg<N>::THREADS, MbsColCfg<N>::MINB) k_mbs_cols(MbsArgs a, long n_outer,
                                                                                 int inner, long ostride, long E) {
-  using C = ColCfg<N, false>;
+  using C = MbsColCfg<N>;
   constexpr int V = C::V, LEN = C::LEN;
   extern __shared__ float2 sm[];
   float2* tw = sm;
-  float2* tile = sm + C::TW;
+  float2* tiles = sm + C::TW;  // [2][V][LEN]
   load_twiddles<N>(tw, a.twg, threadIdx.x, blockDim.x);
   const int team = threadIdx.x / C::LPV, lane = threadIdx.x % C::LPV;
-  float2* s = tile + team * LEN;
   const int tiles_i = (inner + V - 1) / V;
   const long total = (long)tiles_i * n_outer;
-  for (long t = blockIdx.x; t < total; t += gridDim.x) {
+  auto prefetch = [&](long t, float2* tile) {
+    const long o = t / tiles_i;
+    prefetch_col_tile<V, LEN>(tile, a.buf + o * ostride, E, (t % tiles_i) * V, inner, N);
+    cp_async_commit();
+  };
+  long t = blockIdx.x;
+  if (t < total) prefetch(t, tiles);
+  for (int b = 0; t < total; t += gridDim.x, b ^= 1) {
+    float2* tile = tiles + b * V * LEN;
     const long o = t / tiles_i;
     const int i0 = (int)(t % tiles_i) * V;
     float2* base = a.buf + o * ostride;
+    if (t + gridDim.x < total) {
+      prefetch(t + gridDim.x, tiles + (b ^ 1) * V * LEN);
+      cp_async_wait_group<1>();
+    } else {
+      cp_async_wait_group<0>();
+    }
     __syncthreads();
-    load_col_tile<V, LEN>(tile, base, E, i0, inner, 0, N, [](int r) { return r; });
-    __syncthreads();
+    float2* s = tile + team * LEN;
     auto load = [&](int j) -> float2 { return s[pad_idx(j)]; };
     auto store = [&](int k, float2 v, int) { s[pad_idx(k)] = v; };
     team_fft<N, INV, C::LPV, C::CTA>(s, tw, lane, team, load, store);
@@ -174,6 +217,7 @@ __global__ void __launch_bounds__(ColCfg<N, false>::THREADS, ColCfg<N, false>::M
       const int r = idx / V, c = idx % V, i = i0 + c;
       if (i < inner) base[(long)r * E + i] = tile[c * LEN + pad_idx(r)];
     }
+    __syncthreads();  // the next iteration's prefetch refills this tile
   }
 }
 
@@ -186,14 +230,16 @@ struct MbsXCfg {
   static constexpr bool CTA = C::CTA;
   // about 128 lanes per component (at least 4 columns), at most 1024 threads;
   // exact-size teams (CTA) fill whole warps
-  static constexpr int V1 = LPV < 32 ? (pow2_floor(128 / LPV) > 4 ? pow2_floor(128 / LPV) : 4) : 4;
+  static constexpr int V1 = LPV < 32 ? (pow2_floor(128 / LPV) > 4 ? pow2_floor(128 / LPV) : 4) : (3 * 8 * LPV <= 1024 ? 8 : 4);
   static constexpr int V0 = (CTA && (3 * V1 * LPV) % 32 != 0 && 3 * 2 * V1 * LPV <= 1024) ? 2 * V1 : V1;
   static constexpr int V = (3 * V0 * LPV <= 1024) ? V0 : ((3 * 2 * LPV <= 1024) ? 2 : 1);
   static_assert(!CTA || (3 * V * LPV) % 32 == 0, "exact-size teams must fill whole warps");
   static constexpr int LEN = col_len(NX, V);
   static constexpr int THREADS = 3 * V * LPV;
   static constexpr int MINB = minb_for(THREADS);
-  static constexpr size_t SMEM = sizeof(float2) * ((size_t)C::TW + 3 * (size_t)V * LEN);
+  // two tiles of three components: the next one is copied in (cp.async) while the current one is processed
+  static constexpr size_t SMEM = sizeof(float2) * ((size_t)C::TW + 2 * 3 * (size_t)V * LEN);
+  static_assert(SMEM <= 227 * 1024, "two x tiles do not fit in shared memory");
 };
 
 template <int NX>
@@ -202,18 +248,28 @@ __global__ void __launch_bounds__(MbsXCfg<NX>::THREADS, MbsXCfg<NX>::MINB) k_mbs
   constexpr int V = Q::V, LEN = Q::LEN, LPV = Q::LPV;
   extern __shared__ float2 sm[];
   float2* tw = sm;
-  float2* tile = sm + ColCfg<NX, false>::TW;  // [comp][V][LEN]
+  float2* tiles_sm = sm + ColCfg<NX, false>::TW;  // [2][comp][V][LEN]
   load_twiddles<NX>(tw, a.twg, threadIdx.x, blockDim.x);
   const int team = threadIdx.x / LPV, lane = threadIdx.x % LPV;  // team = comp * V + column
-  float2* s = tile + team * LEN;
   const long inner = (long)a.Y * a.Z;
   const long tiles = (inner + V - 1) / V;
-  for (long t = blockIdx.x; t < tiles; t += gridDim.x) {
-    const long i0 = t * V;
-    __syncthreads();
+  auto prefetch = [&](long t, float2* tile) {
     for (int c = 0; c < 3; ++c)
-      load_col_tile<V, LEN>(tile + c * V * LEN, a.buf + (size_t)c * a.vox, inner, (int)i0, (int)inner, 0, NX,
-                            [](int r) { return r; });
+      prefetch_col_tile<V, LEN>(tile + c * V * LEN, a.buf + (size_t)c * a.vox, inner, t * V, inner, NX);
+    cp_async_commit();
+  };
+  long t = blockIdx.x;
+  if (t < tiles) prefetch(t, tiles_sm);
+  for (int b = 0; t < tiles; t += gridDim.x, b ^= 1) {
+    const long i0 = t * V;
+    float2* tile = tiles_sm + b * 3 * V * LEN;
+    float2* s = tile + team * LEN;
+    if (t + gridDim.x < tiles) {
+      prefetch(t + gridDim.x, tiles_sm + (b ^ 1) * 3 * V * LEN);
+      cp_async_wait_group<1>();
+    } else {
+      cp_async_wait_group<0>();
+    }
     __syncthreads();
     auto load = [&](int j) -> float2 { return s[pad_idx(j)]; };
     auto store = [&](int k, float2 v, int) { s[pad_idx(k)] = v; };
@@ -271,6 +327,7 @@ __global__ void __launch_bounds__(MbsXCfg<NX>::THREADS, MbsXCfg<NX>::MINB) k_mbs
         if (i < inner) dst[(long)r * inner + i] = src[cc * LEN + pad_idx(r)];
       }
     }
+    __syncthreads();  // the next iteration's prefetch refills this tile
   }
 }
 

@@ -36,11 +36,12 @@ static cx_status launch_z_any(int mode, const MbsArgs& a, cudaStream_t st) {
 
 template <int N, bool INV>
 static cx_status launch_cols(const MbsArgs& a, long n_outer, int inner, long ostride, long E, cudaStream_t st) {
-  using C = ColCfg<N, false>;
+  using C = MbsColCfg<N>;
+  constexpr size_t SMEM = C::SMEM;
   auto k = k_mbs_cols<N, INV>;
-  CX_CUDA_TRY(set_smem(k, C::SMEM));
+  CX_CUDA_TRY(set_smem(k, SMEM));
   const long items = (long)((inner + C::V - 1) / C::V) * n_outer;
-  k<<<persistent_grid(k, C::THREADS, C::SMEM, items), C::THREADS, C::SMEM, st>>>(a, n_outer, inner, ostride, E);
+  k<<<persistent_grid(k, C::THREADS, SMEM, items), C::THREADS, SMEM, st>>>(a, n_outer, inner, ostride, E);
   CX_LAUNCH_CHECK();
   return CX_OK;
 }
