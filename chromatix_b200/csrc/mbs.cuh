@@ -48,10 +48,16 @@ __device__ __forceinline__ float2 mbs_disc(const MbsArgs& a, float2 v, float2 e)
 
 // lines along z: one team per (ix, iy) line, the three components in turn,
 // so the line's permittivity is read from HBM once (kept in shared memory)
-template <int NZ>
+template <int NZ, int MODE = MBS_Z_DISC>
 struct MbsZCfg {
   using C = RowCfg<NZ>;
-  static constexpr size_t SMEM = C::SMEM + sizeof(float2) * (size_t)C::TEAMS * NZ;
+  // MBS_ZI_STEP: per team, the component's x and prec_y rows, copied in by
+  // bulk (TMA) copies while the inverse transform runs, and their mbarrier
+  static constexpr bool PREFETCH = MODE == MBS_ZI_STEP;
+  static constexpr size_t PF_OFF = (C::SMEM + sizeof(float2) * (size_t)C::TEAMS * NZ + 15) & ~(size_t)15;
+  static constexpr size_t BAR_OFF = PF_OFF + (PREFETCH ? sizeof(float2) * 2 * (size_t)C::TEAMS * NZ : 0);
+  static constexpr size_t SMEM = BAR_OFF + (PREFETCH ? sizeof(uint64_t) * (size_t)C::TEAMS : 0);
+  static constexpr int POLLS = 1 << 20;
 };
 
 template <int NZ, int MODE>
@@ -64,6 +70,19 @@ __global__ void __launch_bounds__(RowCfg<NZ>::THREADS, RowCfg<NZ>::MINB) k_mbs_z
   const int team = threadIdx.x / C::LPV, lane = threadIdx.x % C::LPV;
   float2* s = sm + C::TW + team * Plan<NZ>::LEN;
   float2* se = sm + C::TW + C::TEAMS * Plan<NZ>::LEN + team * NZ;  // the line's permittivity
+  using Q = MbsZCfg<NZ, MODE>;
+  float2* pfx = reinterpret_cast<float2*>(reinterpret_cast<char*>(sm) + Q::PF_OFF) + (size_t)team * 2 * NZ;
+  float2* pfp = pfx + NZ;
+  uint64_t* bar = reinterpret_cast<uint64_t*>(reinterpret_cast<char*>(sm) + Q::BAR_OFF) + team;
+  unsigned bphase = 0;
+  // bulk copies need 16-byte aligned rows (even Z, aligned bases)
+  const bool bulk_ok = Q::PREFETCH && (a.Z % 2 == 0) && ((reinterpret_cast<size_t>(a.x) & 15) == 0) &&
+                       ((reinterpret_cast<size_t>(a.prec_y) & 15) == 0);
+  if constexpr (Q::PREFETCH) {
+    if (lane == 0) bulk_mbar_init(bar);
+    asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+    __syncthreads();
+  }
   const long lines = (long)a.X * a.Y;
   const float inv_n = 1.0f / ((float)a.X * (float)a.Y * (float)a.Z);
   double dsum = 0.0, nsum = 0.0;
@@ -93,21 +112,41 @@ __global__ void __launch_bounds__(RowCfg<NZ>::THREADS, RowCfg<NZ>::MINB) k_mbs_z
           const float2* xrow = a.x + off;
           const float2* prow = a.prec_y + off;
           float2* orow = a.x_new + off;
-          auto store = [&](int k, float2 g, int) {
-            const float2 xo = xrow[k];
-            const float2 gk = cscale(g, inv_n);
+          // the x and prec_y rows travel while the inverse transform runs; the
+          // update then reads them from shared memory (or, if the bounded wait
+          // ran out or the rows are not aligned, from global memory)
+          team_sync<C::LPV>(team);  // the previous component's reads of the prefetch rows are complete
+          if (bulk_ok && lane == 0) {
+            const unsigned rb = (unsigned)a.Z * 8u;
+            bulk_fence();
+            bulk_expect(bar, 2u * rb);
+            const uint64_t pol = l2_evict_first();
+            bulk_copy_g2s_hint(pfx, xrow, rb, bar, pol);
+            bulk_copy_g2s_hint(pfp, prow, rb, bar, pol);
+          }
+          auto keep = [&](int k, float2 g, int) { s[pad_idx(k)] = g; };
+          team_fft_ex<NZ, true, false, false>(s, tw, lane, team, load, keep);
+          bool pre = false;
+          if (bulk_ok) {
+            pre = bulk_wait(bar, bphase, Q::POLLS);
+            bphase ^= 1u;
+          }
+          team_sync<C::LPV>(team);
+#pragma unroll 2
+          for (int k = lane; k < NZ; k += C::LPV) {
+            const float2 xo = pre ? pfx[k] : xrow[k];
+            const float2 gk = cscale(s[pad_idx(k)], inv_n);
             const float2 vx = mbs_disc(a, cadd(gk, xo), se[k]);
             if (a.forward_only) {
               orow[k] = make_float2(-vx.x, -vx.y);
-              return;
+              continue;
             }
-            const float2 xn = cadd(cadd(prow[k], vx), xo);
+            const float2 xn = cadd(cadd(pre ? pfp[k] : prow[k], vx), xo);
             orow[k] = xn;
             const float2 dd = csub(xn, xo);
             dsum += (double)dd.x * dd.x + (double)dd.y * dd.y;
             nsum += (double)xn.x * xn.x + (double)xn.y * xn.y;
-          };
-          team_fft_ex<NZ, true, false, true>(s, tw, lane, team, load, store);
+          }
         } else {  // MBS_ZI_PREC: prec_y = -V(G)
           float2* orow = a.x_new + off;
           auto store = [&](int k, float2 g, int) {

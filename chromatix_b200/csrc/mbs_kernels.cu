@@ -11,7 +11,7 @@ namespace cx {
 template <int N, int MODE>
 static cx_status launch_z(const MbsArgs& a, cudaStream_t st) {
   using C = RowCfg<N>;
-  constexpr size_t SMEM = MbsZCfg<N>::SMEM;
+  constexpr size_t SMEM = MbsZCfg<N, MODE>::SMEM;
   auto k = k_mbs_z<N, MODE>;
   CX_CUDA_TRY(set_smem(k, SMEM));
   const long items = ((long)a.X * a.Y + C::TEAMS - 1) / C::TEAMS;
