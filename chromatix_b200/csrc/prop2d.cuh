@@ -403,8 +403,18 @@ __global__ void __launch_bounds__(RowCfg<NX>::THREADS, RowCfg<NX>::MINB) k_prop_
 // pass B: column FFT -> x H -> column IFFT on V-column tiles
 // --------------------------------------------------------------------------
 // BAND: the data rows lie in [NY / 4, 3 NY / 4) of the padded column (checked
-// on the host), so the forward transform's first stage skips the padding
-template <int NY, bool BAND = false>
+// on the host), so the forward transform's first stage skips the padding.
+// HT: the propagator is a table (CX_KERNEL_EXPLICIT without NA mask, e.g. the
+// multislice slice propagator): the tile's V columns of H are copied into
+// shared memory (cp.async) together with the data tile, instead of being read
+// from global memory per element in the transform's last stage.
+template <int NY>
+struct PropColHt {
+  static constexpr size_t SMEM = ColCfg<NY>::SMEM + sizeof(float2) * (size_t)ColCfg<NY>::V * NY;
+  static constexpr bool FITS = SMEM <= 227 * 1024;
+};
+
+template <int NY, bool BAND = false, bool HT = false>
 __global__ void __launch_bounds__(ColCfg<NY>::THREADS, ColCfg<NY>::MINB) k_prop_cols(const float2* __restrict__ T,
                                                                   float2* __restrict__ T2, Prop2DArgs a) {
   using C = ColCfg<NY>;
@@ -412,6 +422,7 @@ __global__ void __launch_bounds__(ColCfg<NY>::THREADS, ColCfg<NY>::MINB) k_prop_
   extern __shared__ float2 sm[];
   float2* tw = sm;
   float2* tile = sm + C::TW;
+  float2* hs = tile + V * LEN;  // HT: [V][NY] propagator columns of the tile
   load_twiddles<NY>(tw, a.twg, threadIdx.x, blockDim.x);
   const int team = threadIdx.x / C::LPV, lane = threadIdx.x % C::LPV;
   float2* s = tile + team * LEN;
@@ -425,9 +436,18 @@ __global__ void __launch_bounds__(ColCfg<NY>::THREADS, ColCfg<NY>::MINB) k_prop_
     const PropK kc = prop_consts(a, pl);
     const int p_in = pl.in_plane;
     __syncthreads();
+    if constexpr (HT) {
+      const float2* Hp = a.H + (size_t)pl.h_plane * a.py * a.px + x0;
+      for (int idx = threadIdx.x; idx < NY * V; idx += blockDim.x) {
+        const int r = idx / V, c = idx % V;
+        if (x0 + c < a.px) cp_async8(hs + c * NY + r, Hp + (size_t)r * a.px + c);
+      }
+      cp_async_commit();
+    }
     // cooperative, coalesced load of the ny data rows of this column tile
     load_col_tile<V, LEN>(tile, T + (size_t)p_in * a.ny * a.px, a.px, x0, a.px, 0, a.ny,
                           [&](int r) { return r + a.pad_y; });
+    if constexpr (HT) cp_async_wait_all();
     __syncthreads();
     const int kx = x0 + team;
     const bool valid = kx < a.px;
@@ -435,7 +455,15 @@ __global__ void __launch_bounds__(ColCfg<NY>::THREADS, ColCfg<NY>::MINB) k_prop_
     auto load1 = [&](int n) -> float2 {
       return (n >= a.pad_y && n < a.pad_y + a.ny) ? s[pad_idx(n)] : make_float2(0.f, 0.f);
     };
-    auto store1 = [&](int k, float2 v, int) { s[pad_idx(k)] = valid ? cmul(v, prop_col_h(k, kx, pc, a, pl, kc)) : v; };
+    const float2* hcol = hs + team * NY;
+    auto store1 = [&](int k, float2 v, int) {
+      if constexpr (HT) {
+        const float2 h = hcol[k];
+        s[pad_idx(k)] = valid ? cmul(v, make_float2(h.x, pc.sgn * h.y)) : v;
+      } else {
+        s[pad_idx(k)] = valid ? cmul(v, prop_col_h(k, kx, pc, a, pl, kc)) : v;
+      }
+    };
     team_fft_ex<NY, false, false, true, C::LPV, C::CTA, (BAND ? center_band_mask<NY>() : 0u)>(s, tw, lane, team,
                                                                                               load1, store1);
     team_barrier<C::LPV, C::CTA>(team);
