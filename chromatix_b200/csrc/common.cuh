@@ -115,6 +115,11 @@ __device__ __forceinline__ void st_hint(float2* p, float2 v, uint64_t policy) {
   asm volatile("st.global.L2::cache_hint.v2.f32 [%0], {%1, %2}, %3;\n" ::"l"(p), "f"(v.x), "f"(v.y), "l"(policy)
                : "memory");
 }
+// hint: start bringing [gmem, gmem + bytes) into L2 (bulk prefetch; the
+// address and the size must be multiples of 16 bytes; no completion to wait on)
+__device__ __forceinline__ void bulk_prefetch_l2(const void* gmem, unsigned bytes) {
+  asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;\n" ::"l"(gmem), "r"(bytes) : "memory");
+}
 // shared-memory reads by the generic proxy are ordered before later bulk writes
 __device__ __forceinline__ void bulk_fence() { asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory"); }
 // bounded wait for the phase with parity `phase`; false after `polls` polls

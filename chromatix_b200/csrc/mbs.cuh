@@ -86,6 +86,30 @@ __global__ void __launch_bounds__(RowCfg<NZ>::THREADS, RowCfg<NZ>::MINB) k_mbs_z
   const long lines = (long)a.X * a.Y;
   const float inv_n = 1.0f / ((float)a.X * (float)a.Y * (float)a.Z);
   double dsum = 0.0, nsum = 0.0;
+  // L2 prefetch of the rows the team reads next (the next component of this
+  // line, or the first of its next line with that line's permittivity),
+  // issued while the current component is transformed
+  const bool l2pf = (a.Z % 2 == 0) && ((reinterpret_cast<size_t>(a.x) & 15) == 0) &&
+                    ((reinterpret_cast<size_t>(a.buf) & 15) == 0) &&
+                    ((reinterpret_cast<size_t>(a.eps) & 15) == 0) &&
+                    ((reinterpret_cast<size_t>(a.prec_y) & 15) == 0);
+  auto prefetch_next = [&](long xy, int comp) {
+    const long nxy = comp < 2 ? xy : xy + (long)gridDim.x * C::TEAMS;
+    const int ncomp = comp < 2 ? comp + 1 : 0;
+    if (!l2pf || lane != 0 || nxy >= lines) return;
+    const unsigned rb = (unsigned)a.Z * 8u;
+    const size_t noff = (size_t)ncomp * a.vox + (size_t)nxy * a.Z;
+    if (ncomp == 0 && MODE != MBS_Z_SCALE) bulk_prefetch_l2(a.eps + (size_t)nxy * a.Z, rb);
+    if constexpr (MODE == MBS_Z_DISC || MODE == MBS_Z_SCALE) {
+      bulk_prefetch_l2(a.x + noff, rb);
+    } else {
+      bulk_prefetch_l2(a.buf + noff, rb);
+      if constexpr (MODE == MBS_ZI_STEP) {
+        bulk_prefetch_l2(a.x + noff, rb);
+        bulk_prefetch_l2(a.prec_y + noff, rb);
+      }
+    }
+  };
   for (long base = (long)blockIdx.x * C::TEAMS; base < lines; base += (long)gridDim.x * C::TEAMS) {
     const long xy = base + team;
     if (xy >= lines) continue;
@@ -98,6 +122,7 @@ __global__ void __launch_bounds__(RowCfg<NZ>::THREADS, RowCfg<NZ>::MINB) k_mbs_z
 #pragma unroll 1
     for (int comp = 0; comp < 3; ++comp) {
       const size_t off = (size_t)comp * a.vox + (size_t)xy * a.Z;
+      prefetch_next(xy, comp);
       float2* brow = a.buf + off;
       if constexpr (MODE == MBS_Z_DISC || MODE == MBS_Z_SCALE) {
         const float2* xrow = a.x + off;
