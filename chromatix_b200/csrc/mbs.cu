@@ -44,7 +44,7 @@ static cx_status mbs_middle(const MbsArgs& a, cudaStream_t st) {
 using namespace cx;
 
 extern "C" cx_status cx_mbs_workspace_size(const cx_mbs_desc* d, size_t* bytes) {
-  MbsArgs a;
+  MbsArgs a{};  // pointers a call does not set stay null
   cx_status s = mbs_args(d, &a);
   if (s != CX_OK && s != CX_ERR_CUDA) return s;
   if (!bytes) return CX_ERR_INVALID;
@@ -54,7 +54,7 @@ extern "C" cx_status cx_mbs_workspace_size(const cx_mbs_desc* d, size_t* bytes) 
 
 extern "C" cx_status cx_mbs_precondition(const cx_mbs_desc* d, const void* eps, const void* src, void* prec_y,
                                          void* workspace, size_t workspace_bytes, cx_stream_t stream) {
-  MbsArgs a;
+  MbsArgs a{};  // pointers a call does not set stay null
   cx_status s = mbs_args(d, &a);
   if (s != CX_OK) return s;
   if (!eps || !src || !prec_y || !workspace || workspace_bytes < sizeof(float2) * 3 * (size_t)a.vox) {
@@ -74,7 +74,7 @@ extern "C" cx_status cx_mbs_precondition(const cx_mbs_desc* d, const void* eps, 
 extern "C" cx_status cx_mbs_iterate(const cx_mbs_desc* d, const void* eps, const void* prec_y, const void* x,
                                     void* x_new, double* acc, void* workspace, size_t workspace_bytes,
                                     cx_stream_t stream) {
-  MbsArgs a;
+  MbsArgs a{};  // pointers a call does not set stay null
   cx_status s = mbs_args(d, &a);
   if (s != CX_OK) return s;
   if (!eps || !prec_y || !x || !x_new || !acc || !workspace ||
@@ -97,7 +97,7 @@ extern "C" cx_status cx_mbs_iterate(const cx_mbs_desc* d, const void* eps, const
 
 extern "C" cx_status cx_mbs_forward(const cx_mbs_desc* d, const void* eps, const void* x, void* out, void* workspace,
                                     size_t workspace_bytes, cx_stream_t stream) {
-  MbsArgs a;
+  MbsArgs a{};  // pointers a call does not set stay null
   cx_status s = mbs_args(d, &a);
   if (s != CX_OK) return s;
   if (!eps || !x || !out || !workspace || workspace_bytes < sizeof(float2) * 3 * (size_t)a.vox || x == out) {
