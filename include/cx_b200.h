@@ -19,7 +19,10 @@
  *    the matching *_workspace_size call.  No entry point allocates device
  *    memory, synchronises the stream, or traps: errors come back as a
  *    cx_status and a thread-local message (cx_last_error).
- *  - Every call is asynchronous on the given stream.
+ *  - Every call is asynchronous on the given stream.  Two entry points fork
+ *    work onto a second stream and join it back with events created per call:
+ *    cx_psf_4f_to_host (the caller's copy stream) and cx_multislice_backward
+ *    (a stream the library creates once per device).
  */
 #ifndef CX_B200_H
 #define CX_B200_H
