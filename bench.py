@@ -730,6 +730,24 @@ def asm_arm(args):
             res[key] = {"ms": round(ms, 4), "Mpx_s": round(B * 1024 * 1024 / (ms * 1e-3) / 1e6, 1),
                                        "achieved_GBs": round(alg / (ms * 1e-3) / 1e9, 1),
                                        "frac": round(alg / (ms * 1e-3) / 1e9 / hbm, 4)}
+            if B == 1 and form == "accurate":
+                # the same call captured once in a CUDA graph and replayed: a lone field's
+                # three passes without the host's per-call work (a graph-replaying caller)
+                step()
+                torch.cuda.synchronize(dev)
+                graph = torch.cuda.CUDAGraph()
+                side = torch.cuda.Stream(dev)
+                side.wait_stream(torch.cuda.current_stream(dev))
+                with torch.cuda.stream(side):
+                    with torch.cuda.graph(graph, stream=side):
+                        step()
+                torch.cuda.current_stream(dev).wait_stream(side)
+                gms = _device_timer(torch, dev, args.steps, args.warmup)(graph.replay)
+                res[key + "/graph_replay"] = {"ms": round(gms, 4),
+                                              "Mpx_s": round(1024 * 1024 / (gms * 1e-3) / 1e6, 1),
+                                              "achieved_GBs": round(alg / (gms * 1e-3) / 1e9, 1),
+                                              "frac": round(alg / (gms * 1e-3) / 1e9 / hbm, 4)}
+                del graph
             if not args.no_accuracy:
                 # outside the timed region: field 0 of the batch against the FP64 oracle
                 out0 = step().u.reshape(B, 1024, 1024)[0].cpu().numpy()
